@@ -1,0 +1,381 @@
+"""SAXS throughput benchmark: frames/s at 100k atoms on a 256^3 supercell.
+
+Workload (one "step"): one batch of the 100-frame trajectory of the 100k-atom
+system (12 nm cubic box, H/C/O/N/S/P mix, frame k = frame 0 + N(0, 0.05 nm)
+per atom), grid 128, B-spline order 4, scale 2 (256^3 supercell), q-cut
+0.5 /A, bin 0.002 /A (reset to the supercell's reciprocal spacing), npt
+histogram in FP64 - all through the batched fused forward.
+
+  value  frames/s with the frames already in HBM (device-timed, CUDA events,
+         L2 flushed between steps)
+  e2e    frames/s through the public API from pinned host buffers: every step
+         copies its frames host->device and reads the histogram back
+
+usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+Under torchrun each rank processes its own 100 frames (weak scaling); the FP64
+histograms are summed with one NCCL all-reduce at the end of every step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO))
+
+NATOMS = 100_000
+BOX = 120.0
+GRID = 128
+SCALE = 2.0
+QCUT = 0.5
+BIN = 0.002
+FRAMES = 100
+JITTER = 0.5
+METRIC = "SAXS frames/s @100k atoms, 256^3 supercell (batched fused forward)"
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--batch", type=int, default=FRAMES)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi SM clocks and throttle reasons, sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world <= 1:
+        return 0, 1, None
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return dist.get_rank(), world, dist
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+def max_over_ranks(v: float, dist) -> float:
+    if dist is None:
+        return v
+    import torch
+
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def bench_ours(args):
+    import torch
+
+    from pycusaxs_b200 import SaxsEngine
+    from pycusaxs_b200.synthetic import cubic_system
+
+    rank, world, dist = dist_setup(args)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    system = cubic_system(NATOMS, BOX, seed=1000 + rank, jitter=JITTER, nframes=FRAMES)
+    frames = system.frames(0, FRAMES)                       # (100, N, 3) float32 host
+    boxes = np.stack([system.box] * FRAMES)
+    B = min(args.batch, FRAMES)
+    eng = SaxsEngine((GRID,) * 3, system.atom_index(), system.natoms, system.box,
+                     scale_factor=SCALE, bin_size=BIN, qcut=QCUT, max_frames=B)
+    st = eng.stream
+    x_dev = torch.from_numpy(frames).to(dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    hist_buf = torch.zeros(2 * eng.info.num_bins, dtype=torch.float64, device=dev)
+
+    def step_device():
+        eng.forward(x_dev, boxes)
+
+    def reduce_hist():
+        if dist is not None:
+            h, n = eng.histogram()
+            hist_buf.copy_(torch.from_numpy(np.concatenate([h, n])))
+            dist.all_reduce(hist_buf)
+
+    # warm-up
+    for _ in range(args.warmup):
+        step_device()
+    st.synchronize()
+    eng.reset()
+    # timed device-resident steps: L2 flush on the engine stream, then events around the step
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    eng.profile_enable(True)
+    clocks = ClockSampler(dev.index)
+    clocks.start()
+    barrier(dist)
+    torch.cuda.synchronize()
+    for k in range(args.steps):
+        with torch.cuda.stream(st):
+            flush.zero_()
+        ev[k][0].record(st)
+        step_device()
+        ev[k][1].record(st)
+    torch.cuda.synchronize()
+    barrier(dist)
+    ck = clocks.stop()
+    eng.profile_enable(False)
+    stages = eng.profile_read()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    total_s = max_over_ranks(sum(step_ms) / 1e3, dist)
+    reduce_hist()
+    value = world * FRAMES * args.steps / total_s
+
+    # per-kernel roofline for the dominant stage
+    prof = {k: v for k, v in stages.items()}
+    dom = max(prof, key=lambda k: prof[k][0])
+    info = eng.info
+    nkx, nky, nkz = info.kbox
+    T = len(eng.type_names)
+    M = system.natoms
+    ex = ey = ez = GRID
+    frames_timed = FRAMES * args.steps
+    algo_bytes = {
+        # sorted atom records in, Z half-plane out
+        "k_spread_zdft": 16 * M + 8 * T * nkz * ex * ey,
+        "k_ydft": 8 * T * nkz * ex * ey + 8 * T * nkz * nky * ex,
+        "k_xdft_post": 8 * T * nkz * nky * ex + 4 * nkz * nky * nkx,
+        "k_bin_atoms": 12 * M + 8 * M,
+        "k_scatter_atoms": 12 * M + 8 * M + 16 * M,
+        "k_hist": 4 * nkz * nky * nkx,
+        "k_scan": 8 * T * (GRID // 8) ** 2,
+    }
+    algo_flops = {
+        "k_spread_zdft": 4 * T * ex * ey * ez * nkz,          # real x complex MAC = 2 FMA
+        "k_ydft": 8 * T * nkz * ex * ey * nky,                # complex MAC = 4 FMA
+        "k_xdft_post": 8 * T * nkz * nky * ex * nkx,
+    }
+    peaks = json.loads((REPO / "MEASURED_PEAKS.json").read_text()) if (
+        REPO / "MEASURED_PEAKS.json").exists() else {}
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    dom_ms, dom_launches = prof[dom]
+    per_launch_s = dom_ms / 1e3 / max(dom_launches, 1)
+    frames_per_launch = frames_timed / max(dom_launches, 1)
+    achieved = algo_bytes.get(dom, 0) * frames_per_launch / per_launch_s / 1e9
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": hbm,
+                "unit": "GB/s", "frac": round(achieved / hbm, 4), "traffic": None,
+                "peak_source": "measured" if peaks else "fallback"}
+    if dom in algo_flops:
+        roofline["fp32_tflops"] = round(algo_flops[dom] * frames_per_launch / per_launch_s / 1e12, 2)
+    stage_share = {k: round(v[0] / max(sum(x[0] for x in prof.values()), 1e-9), 4)
+                   for k, v in prof.items()}
+
+    # e2e through the public API from pinned host memory
+    host = torch.from_numpy(frames).pin_memory()
+    eng.reset()
+    for _ in range(max(1, args.warmup)):
+        eng.forward_host(host.numpy(), boxes)
+        eng.histogram()
+    barrier(dist)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        eng.forward_host(host.numpy(), boxes)
+        h, n = eng.histogram()
+    e2e_s = max_over_ranks(time.perf_counter() - t0, dist)
+    e2e = {"value": round(world * FRAMES * args.steps / e2e_s, 1), "unit": "frames/s",
+           "h2d_bytes_per_step": int(frames.nbytes), "d2h_bytes_per_step": int(h.nbytes + n.nbytes)}
+
+    # the plain per-frame path (one frame per call), same frames, device resident
+    plain = None
+    if not args.no_plain:
+        eng1 = SaxsEngine((GRID,) * 3, system.atom_index(), system.natoms, system.box,
+                          scale_factor=SCALE, bin_size=BIN, qcut=QCUT, max_frames=1)
+        for k in range(5):
+            eng1.forward(x_dev[k], boxes[k])
+        eng1.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(eng1.stream)
+        for k in range(FRAMES):
+            eng1.forward(x_dev[k], boxes[k])
+        b.record(eng1.stream)
+        b.synchronize()
+        plain = FRAMES / (a.elapsed_time(b) / 1e3)
+        eng1.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(system)
+
+    launches = sum(v[1] for v in prof.values())
+    out = {
+        "metric": METRIC, "value": round(value, 1), "unit": "frames/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(total_s * 1e3 / args.steps, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 histogram)",
+        "data": "synthetic (seeded uniform atoms, Gaussian-jittered frames)",
+        "config": {"workload": "100k atoms, 12 nm cubic box, grid 128, order 4, scale 2 "
+                               "(256^3 supercell), qcut 0.5/A, 100 frames per step, npt",
+                   "frames_per_step_per_gpu": FRAMES, "batch": B, "l2": "flushed between steps",
+                   "kbox": [nkx, nky, nkz], "plain_path_frames_per_s": round(plain, 1) if plain else None,
+                   "stage_share": stage_share, "parallelism": f"frames sharded over {world} GPU(s)"},
+        "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": ck,
+        "gpu_launches": int(launches),
+    }
+    eng.close()
+    if rank == 0:
+        print(json.dumps(out))
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def cpu_baseline(system) -> dict:
+    """The FP64 oracle on one frame of the same workload, on this host's cores."""
+    from oracle import saxs_oracle as O
+
+    names = sorted({str(e) for e in system.elements})
+    ff = O.load_form_factors()
+    plan = O.OraclePlan(grid=(GRID,) * 3, types=names, coeffs=np.stack([ff[n] for n in names]),
+                        box0=system.box, sigma=SCALE, bin_size=BIN, qcut=QCUT)
+    toa = system.type_of_atom(names)
+    t0 = time.perf_counter()
+    O.run_frames(plan, [(system.frame(0), system.box)], toa)
+    dt = time.perf_counter() - t0
+    return {"value": round(1.0 / dt, 4), "unit": "frames/s", "cores": 1, "kind": "port",
+            "sample": f"1 frame of the workload through the FP64 NumPy oracle ({dt:.1f} s)"}
+
+
+def bench_reference(args):
+    rank, world, dist = (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+                         None)
+    if rank != 0:
+        return
+    refdir = REPO / "oracle" / "_ref"
+    if not any(refdir.glob("pycusaxs_cuda*.so")):
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "reference build oracle/_ref missing (run oracle/build_ref.sh)"}))
+        return
+    sys.path.insert(0, str(refdir))
+    import pycusaxs_cuda  # the reference cudaSAXS, built from its own sources
+
+    from pycusaxs_b200.synthetic import SyntheticTopology, cubic_system
+
+    system = cubic_system(NATOMS, BOX, seed=1000, jitter=JITTER, nframes=FRAMES)
+    topo = SyntheticTopology(system)
+    sample = 10
+
+    def run(nframes):
+        devnull = os.open(os.devnull, os.O_WRONLY)
+        saved = os.dup(1)
+        os.dup2(devnull, 1)
+        try:
+            t0 = time.perf_counter()
+            pycusaxs_cuda.run(topo, "synthetic.tpr", "synthetic.xtc", [GRID], begin=0,
+                              end=nframes - 1, stride=1, output="/tmp/ref_bench.dat",
+                              scale_factor=SCALE, bin_size=BIN, qcut=QCUT)
+            return time.perf_counter() - t0
+        finally:
+            os.dup2(saved, 1)
+            os.close(devnull)
+            os.close(saved)
+
+    for _ in range(max(1, args.warmup)):
+        run(2)
+    per_frame = []
+    for _ in range(args.steps):
+        t_small = run(2)
+        t_big = run(2 + sample)
+        per_frame.append((t_big - t_small) / sample)
+    value = 1.0 / statistics.median(per_frame)
+    out = {"metric": METRIC, "value": round(value, 2), "unit": "frames/s", "n_gpus": 1,
+           "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": round(statistics.median(per_frame) * 1e3 * sample, 3),
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+           "data": "synthetic", "impl": "reference",
+           "config": {"workload": "100k atoms, 12 nm cubic box, grid 128, order 4, scale 2 "
+                                  "(256^3 supercell), qcut 0.5/A, npt",
+                      "method": "per-frame slope: (run of 12 frames - run of 2 frames) / 10"},
+           "cpu_baseline": {"value": round(value, 2), "unit": "frames/s", "cores": 1,
+                            "kind": "reference",
+                            "sample": f"{sample} frames per step through the reference's own "
+                                      "pycusaxs_cuda.run (its CUDA build, oracle/_ref; the "
+                                      "reference has no CPU path)"},
+           "e2e": {"value": round(value, 2), "unit": "frames/s", "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        bench_reference(args)
+    else:
+        bench_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,169 @@
+/*
+ * pycusaxs_b200 — C ABI of the B200-native per-frame SAXS path.
+ *
+ * The reference exposes this path only through its pybind11 module
+ * (`pycusaxs_cuda.run`, cpp-src/pybind/cuda_bindings.cpp:172-196) which drives
+ * RunSaxs::Run (cpp-src/Exec/RunSaxs.cu:94-271) and saxsKernel
+ * (cpp-src/Saxs/saxsKernel.h:30-114).  This header is the plain-C boundary
+ * underneath the new drop-in: plain pointers and sizes, status codes instead of
+ * exceptions, caller-owned device buffers for per-frame data, an explicit CUDA
+ * stream.  Each entry point names the reference code it replaces.
+ *
+ * Units follow the reference: positions and boxes in Angstrom, q in 1/Angstrom.
+ * Arrays are row-major; boxes are 3x3 with the cell vectors as rows (the
+ * MDAnalysis `triclinic_dimensions` layout, pycusaxs/topology.py:565-577).
+ *
+ * Every function returns SAXS_OK (0) or a negative SAXS_E* code; the message of
+ * the last failure on the calling thread is available from saxs_last_error().
+ */
+#ifndef PYCUSAXS_B200_H
+#define PYCUSAXS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define SAXS_OK 0
+#define SAXS_E_INVALID (-1)   /* bad argument (the reference raises ValueError) */
+#define SAXS_E_CUDA (-2)      /* CUDA runtime or cuFFT failure */
+#define SAXS_E_NOMEM (-3)     /* device allocation refused (saxsKernel.cu:301-314) */
+#define SAXS_E_RANGE (-4)     /* a frame left the planned k-box or capacity */
+#define SAXS_E_DEVICE (-5)    /* a kernel reported an error through its status word */
+
+/* ensembles (cpp-src/Exec/Options.cpp:16, cudaSAXS.cu:84-87) */
+#define SAXS_NPT 0 /* one histogram per frame, summed over frames (saxsKernel.cu:190-196) */
+#define SAXS_NVT 1 /* intensities summed over frames, binned once (saxsKernel.cu:184-189, 17-39) */
+
+typedef struct SaxsPlan SaxsPlan;
+
+/* Run parameters: the fields of CudaSaxsConfig (cpp-src/include/CudaSaxsInterface.h:10-28)
+ * that reach the numerics, plus the topology's per-type atom lists. */
+typedef struct SaxsParams {
+  int grid[3];          /* nx, ny, nz                                              */
+  int scaled_grid[3];   /* nnx, nny, nnz; all 0 = derive from scale_factor          */
+  int order;            /* B-spline order 1..8 (only 4 is meaningful, as upstream)  */
+  float scale_factor;   /* sigma                                                   */
+  float bin_size;       /* requested Delta-q (1/A), reset upward (saxsKernel.cu:489-526) */
+  float qcut;           /* requested q cut-off (1/A), reset downward                */
+  int ensemble;         /* SAXS_NPT or SAXS_NVT                                    */
+  int ntypes;           /* number of element types                                 */
+  const float *form_factors; /* ntypes x 9 (a1..a4, b1..b4, c), host memory         */
+  int natoms;           /* rows of the per-frame position array                    */
+  int nentries;         /* length of entry_atom / entry_type (sum of type lists)   */
+  const int32_t *entry_atom; /* host: position row spread by each entry            */
+  const int32_t *entry_type; /* host: type index 0..ntypes-1 of each entry         */
+  float box0[9];        /* first-frame box: fixes Delta-q, q-cut and the k-box     */
+  int max_frames;       /* frames per saxs_forward call (batch capacity)           */
+  float box_margin;     /* relative box shrink the k-box tolerates (e.g. 0.05)     */
+} SaxsParams;
+
+/* Sizes derived at plan creation. */
+typedef struct SaxsPlanInfo {
+  int grid[3];
+  int scaled_grid[3];   /* the supercell actually used                             */
+  float bin_size;       /* effective Delta-q                                       */
+  float qcut;           /* effective q cut-off                                     */
+  int num_bins;         /* int(qcut/bin_size)+1 (saxsKernel.cu:247)                */
+  int kbox[3];          /* k-points evaluated per axis (x, y: signed range; z: 0..)*/
+  int kz_count;
+  int path;             /* 0 = pruned separable DFT                                 */
+  size_t device_bytes;  /* device memory held by the plan                          */
+  int frames_accumulated;
+} SaxsPlanInfo;
+
+/* Create a plan: grid sizing, Delta-q/q-cut reset, B-spline moduli, twiddle
+ * tables, device buffers.  Replaces saxsKernel::{scaledCell,
+ * resetHistogramParameters, createMemory, setcufftPlan}
+ * (saxsKernel.cu:470-488, 489-526, 240-366; saxsKernel.h:55-58) and the setup
+ * half of RunSaxs::Run (RunSaxs.cu:107-133).  The current CUDA device is used. */
+int saxs_plan_create(const SaxsParams *params, SaxsPlan **plan);
+
+/* Release every resource of the plan (saxsKernel::~saxsKernel, saxsKernel.cu:546-553). */
+void saxs_plan_destroy(SaxsPlan *plan);
+
+int saxs_plan_info(const SaxsPlan *plan, SaxsPlanInfo *info);
+
+/* Process `nframes` frames (<= max_frames).  Frame f's positions are
+ * xyz_dev[f*frame_stride .. +3*natoms) (float32, device memory); its box is
+ * boxes_host[9*f .. +9] (host memory).  npt: the frames' histograms are added
+ * to the plan's FP64 accumulators; nvt: their intensities are added to the
+ * plan's FP64 intensity sum.  Enqueued on `stream`; returns without waiting.
+ * Replaces saxsKernel::runPKernel (saxsKernel.cu:59-209) and the per-frame body
+ * of RunSaxs::Run (RunSaxs.cu:171-203). */
+int saxs_forward(SaxsPlan *plan, const float *xyz_dev, int64_t frame_stride, int nframes,
+                 const float *boxes_host, void *stream);
+
+/* Finish the run: for nvt bin the summed intensities with the first-frame box
+ * (saxsKernel::getHistogram, saxsKernel.cu:17-39); then copy the FP64
+ * histogram and counts (num_bins each) to host memory and wait for them
+ * (saxsKernel::getSaxs, saxsKernel.cu:210-225).  The accumulators are kept. */
+int saxs_histogram(SaxsPlan *plan, double *hist_host, double *nhist_host, void *stream);
+
+/* Zero the accumulators so the plan can serve another run. */
+int saxs_reset(SaxsPlan *plan, void *stream);
+
+/* Intensities |sum_t f_t F_t|^2 * M of the last frame processed by
+ * saxs_forward, over the plan's k-box (kz, ky, kx order, float32), for tests
+ * and diagnostics.  `out_host` holds kbox[0]*kbox[1]*kz_count floats. */
+int saxs_debug_kbox_intensity(SaxsPlan *plan, float *out_host, void *stream);
+
+/* Per-type FP64 z-border sums of the last frame (saxsDeviceKernels.cu:446-465). */
+int saxs_debug_border_sums(SaxsPlan *plan, double *out_host, void *stream);
+
+/* Reverse-mode derivative of a profile loss with respect to the positions of one
+ * frame.  Given dL/dI for each histogram bin (num_bins doubles, host; bins that
+ * the profile does not report carry 0), recompute the frame's per-type grids
+ * and write dL/dxyz (3*natoms float32, device, overwritten) for the frame's
+ * positions xyz_dev with box box_host.  npt semantics of a single frame
+ * (I_bin = hist/nhist).  No reference counterpart: the reference has no
+ * derivative. */
+int saxs_backward(SaxsPlan *plan, const float *xyz_dev, const float *box_host,
+                  const double *dl_dprofile_host, float *grad_xyz_dev, void *stream);
+
+/* ---- per-kernel timing (diagnostics; no reference counterpart: the reference
+ * times only whole frames with one event pair, saxsKernel.cu:64-67,197-208) ---- */
+
+/* Number of timed kernel stages and the name of stage i. */
+int saxs_profile_stages(void);
+const char *saxs_profile_stage_name(int i);
+
+/* Enable (1) or disable (0) CUDA-event timing around every kernel that
+ * saxs_forward launches, on the stream it launches on. */
+int saxs_profile_enable(SaxsPlan *plan, int enable);
+
+/* Wait for the timed work, then add each stage's milliseconds since the last
+ * read into ms_out[0..saxs_profile_stages()), and its launch count into
+ * launches_out (may be NULL).  Clears the pending records. */
+int saxs_profile_read(SaxsPlan *plan, double *ms_out, int *launches_out);
+
+/* ---- setup numerics, exposed so that tests can pin them against the reference ---- */
+
+/* Nearest 2^a 3^b 5^c 7^d to round(n*sigma), ties to the smaller
+ * (saxsKernel::findClosestProduct, saxsKernel.cu:449-469). */
+int64_t saxs_closest_product(int n, float sigma);
+
+/* oc from the upper triangle of a 3x3 box (Cell::calculateMatrices, Cell.cpp:111-126). */
+int saxs_cell_oc(const float box[9], float oc_out[9]);
+
+/* Effective Delta-q, q-cut and bin count (saxsKernel.cu:489-526, :247). */
+int saxs_histogram_parameters(const int nn[3], const float oc[9], float sigma, float bin_size,
+                              float qcut, float *bin_out, float *qcut_out, int *num_bins_out);
+
+/* Inverse B-spline moduli of one axis of length n (BSpmod, BSpmod.cpp:45-129). */
+int saxs_bspline_moduli(int n, int ndim, float *out);
+
+/* Message of the last failure on the calling thread ("" if none). */
+const char *saxs_last_error(void);
+
+/* Library version string. */
+const char *saxs_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PYCUSAXS_B200_H */

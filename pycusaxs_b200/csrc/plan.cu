@@ -1,0 +1,1304 @@
+// pycusaxs_b200: B200-native per-frame SAXS path.
+//
+// Pipeline of one batch of frames (all kernels hand-written for sm_100a):
+//
+//   k_bin_atoms     atoms -> float32 grid coordinates (the reference's float
+//                   steps, saxsDeviceKernels.cu:355-368), home-tile bin + rank
+//                   (counting sort), per-type FP64 z-border sums for the
+//                   padding mean (saxsDeviceKernels.cu:446-465 evaluated per
+//                   atom instead of per voxel).
+//   k_scan          per-frame exclusive scan of the bin counts.
+//   k_scatter_atoms atoms -> records sorted by (type, home tile).
+//   k_spread_zdft   one CTA per (frame, type, 8x8 column tile): B-spline
+//                   spreading into a shared-memory column tile (no global
+//                   atomics), mean padding folded in as "subtract the mean",
+//                   then the z-axis DFT of every column restricted to the
+//                   kz values the q-cut can reach.
+//   k_ydft          y-axis DFT restricted to the ky range (complex GEMM-shaped
+//                   tiles in shared memory, FP32 FMA).
+//   k_xdft_post     x-axis DFT restricted to the kx range, then per k-point:
+//                   form factor f_t(|q|), complex sum over types, |F|^2 times
+//                   the B-spline moduli (saxsDeviceKernels.cu:142-216).
+//   k_hist          mirror-weighted radial histogram with the reference's
+//                   float32 bin rule (saxsDeviceKernels.cu:67-125), FP64
+//                   shared-memory bins, one global flush per CTA.
+//
+// Why no full FFT: the reference zero-pads (mean-pads) the nx^3 grid into an
+// nn^3 supercell and runs a full R2C FFT, but only k-points with |q| <= qcut
+// ever reach the histogram, and qcut is clamped so that these form a small
+// ellipsoid around the origin (|m| <= ~20 of 256 at 100k atoms / 256^3).  The
+// padded transform is F = DFT(g - mean over the corner block) + mean*nn^3 at
+// k = 0, evaluated exactly by three pruned DFT passes that never touch the
+// zero region.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "pycusaxs_b200.h"
+#include "setup.h"
+
+namespace {
+
+constexpr int kTile = 8;                  // spread tile edge (columns per axis)
+constexpr int kCols = kTile * kTile;      // columns per tile
+constexpr int kThreads = 256;
+constexpr int kGeom = 24;                 // floats of per-frame geometry: oc[9], ocs[9]
+constexpr int kRing = 4;                  // pinned geometry slots in flight
+constexpr int kKzGroup = 10;              // kz outputs per warp in k_spread_zdft
+constexpr int kKzPass = 2 * kKzGroup;     // kz outputs per pass (two warp groups)
+constexpr int kKyGroup = 10;              // ky outputs per warp in k_ydft
+constexpr int kKyPass = 8 * kKyGroup;     // ky outputs per pass (eight warps)
+constexpr int kYChunk = 32;               // y values staged per step in k_ydft
+constexpr int kYRows = 64;                // x rows per CTA in k_ydft
+constexpr int kYStride = kYRows + 2;      // padded shared row (float2), 16-byte aligned
+constexpr int kXRows = 4;                 // ky rows per CTA in k_xdft_post
+constexpr int kMaxSmem = 227 * 1024;
+constexpr int kHistSmemBins = 2048;       // bins held in shared memory by k_hist
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string &msg) {
+  g_err = msg;
+  return code;
+}
+
+#define CUDA_TRY(x)                                                                   \
+  do {                                                                                \
+    cudaError_t e_ = (x);                                                             \
+    if (e_ != cudaSuccess)                                                            \
+      return fail(SAXS_E_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_));      \
+  } while (0)
+
+inline int round_up(int v, int m) { return (v + m - 1) / m * m; }
+
+// Everything a kernel needs, passed by value.
+struct DevArgs {
+  int n[3], nn[3], ext[3];
+  int order, ntaps;
+  int T, M;
+  int tiles[2], stiles[2], nbins;
+  int kx_lo, nkx, ky_lo, nky, nkz, nkzp, nkxp, nkyp;
+  int nf[3];
+  int dz;
+  float dq, qcut;
+  int num_bins;
+  double border_count;
+  double nn3;
+  int64_t frame_stride;
+  const float *xyz;
+  const int32_t *entry_atom;
+  const int32_t *entry_type;
+  const float *geom;
+  const float2 *twz;  // [ez][nkzp]
+  const float2 *twy;  // [ey][nkyp]
+  const float2 *twx;  // [ex][nkxp]
+  const float *modx, *mody, *modz;
+  const float *ff;    // [T][9]
+  int2 *key;
+  int *counts;
+  int *offsets;
+  float4 *rec;
+  double *border;
+  float2 *Z;
+  float2 *Y;
+  float *ibox;
+  double *hist, *nhist;
+  double *iacc;
+  int *status;
+};
+
+// ---------------------------------------------------------------------------
+// device helpers
+// ---------------------------------------------------------------------------
+
+// Grid coordinate r = n * frac(oc_row . x), written as the reference writes it
+// (saxsDeviceKernels.cu:355-361) so that nvcc evaluates it the same way.
+__device__ __forceinline__ float grid_coord(const float *oc, float x0, float y0, float z0, int n) {
+  float x1 = oc[0] * x0 + oc[1] * y0 + oc[2] * z0;
+  return static_cast<float>(n * (x1 - rint(x1 - 0.5)));
+}
+
+// |q| of the k-point with signed indices (ia, ja, ka), in the reference's
+// float32 form (saxsDeviceKernels.cu:85-92): the dot products in float, the
+// 2*pi factor applied in double, then sqrtf of the sum of squares.
+__device__ __forceinline__ float kpoint_q(const float *oc, int ia, int ja, int ka) {
+  float mw1, mw2, mw3, mw;
+  mw1 = oc[0] * ia + oc[1] * ja + oc[2] * ka;
+  mw1 = 2.0 * M_PI * mw1;
+  mw2 = oc[3] * ia + oc[4] * ja + oc[5] * ka;
+  mw2 = 2.0 * M_PI * mw2;
+  mw3 = oc[6] * ia + oc[7] * ja + oc[8] * ka;
+  mw3 = 2.0 * M_PI * mw3;
+  mw = sqrtf(mw1 * mw1 + mw2 * mw2 + mw3 * mw3);
+  return mw;
+}
+
+// Cubic (order-4) cardinal B-spline weights of the four taps at fractional
+// offset u in [0, 1]: tap 0 is the farthest-left grid point.
+__device__ __forceinline__ void cubic_weights(float u, float w[4]) {
+  const float v = 1.0f - u;
+  const float u2 = u * u, u3 = u2 * u;
+  const float s = 1.0f / 6.0f;
+  w[0] = v * v * v * s;
+  w[1] = (3.0f * u3 - 6.0f * u2 + 4.0f) * s;
+  w[2] = (-3.0f * u3 + 3.0f * u2 + 3.0f * u + 1.0f) * s;
+  w[3] = u3 * s;
+}
+
+// Form factor sum_i a_i exp(-b_i s2) + c at s2 = (q/4pi)^2 (opsfact.cu:30-35).
+__device__ __forceinline__ float form_factor(const float *c, float q2) {
+  return c[0] * expf(-c[4] * q2) + c[1] * expf(-c[5] * q2) + c[2] * expf(-c[6] * q2) +
+         c[3] * expf(-c[7] * q2) + c[8];
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ __forceinline__ int signed_k(int k, int nn, int nf) { return k < nf ? k : k - nn; }
+
+// ---------------------------------------------------------------------------
+// kernels
+// ---------------------------------------------------------------------------
+
+// grid (ceil(M/256), frames).  Dynamic shared memory: (warps x T) doubles.
+__global__ void __launch_bounds__(kThreads) k_bin_atoms(DevArgs a) {
+  extern __shared__ double sh_part[];
+  __shared__ float oc[9];
+  const int f = blockIdx.y;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (threadIdx.x < 9) oc[threadIdx.x] = a.geom[f * kGeom + threadIdx.x];
+  __syncthreads();
+  int t = -1;
+  double contrib = 0.0;
+  if (e < a.M) {
+    const int at = a.entry_atom[e];
+    t = a.entry_type[e];
+    const float *p = a.xyz + f * a.frame_stride + 3ll * at;
+    const float x0 = p[0], y0 = p[1], z0 = p[2];
+    float r[3];
+    int m[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      r[d] = grid_coord(oc + 3 * d, x0, y0, z0, a.n[d]);
+      m[d] = static_cast<int>(r[d]);
+    }
+    int xf = m[0] - a.order;
+    if (xf < 0) xf += a.n[0];
+    int yf = m[1] - a.order;
+    if (yf < 0) yf += a.n[1];
+    const int bin = (t * a.tiles[1] + yf / kTile) * a.tiles[0] + xf / kTile;
+    const int rank = atomicAdd(&a.counts[f * a.nbins + bin], 1);
+    a.key[static_cast<int64_t>(f) * a.M + e] = make_int2(bin, rank);
+    // Contribution of this atom to the z-border planes of its type's grid:
+    // (sum of x weights) * (sum of y weights) * (sum of z weights on border planes).
+    float wx[4], wy[4], wz[4];
+    cubic_weights(r[0] - static_cast<float>(m[0]), wx);
+    cubic_weights(r[1] - static_cast<float>(m[1]), wy);
+    cubic_weights(r[2] - static_cast<float>(m[2]), wz);
+    float sx = 0.f, sy = 0.f, sz = 0.f;
+#pragma unroll
+    for (int o = 0; o < 4; ++o) {
+      if (o < a.ntaps) {
+        sx += wx[o];
+        sy += wy[o];
+        int z = m[2] - a.order + o;
+        if (z < 0) z += a.n[2];
+        if (z <= a.dz || z >= a.n[2] - a.dz) sz += wz[o];
+      }
+    }
+    contrib = static_cast<double>(sx) * static_cast<double>(sy) * static_cast<double>(sz);
+  }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nw = blockDim.x >> 5;
+  for (int tt = 0; tt < a.T; ++tt) {
+    const unsigned any = __ballot_sync(0xffffffffu, t == tt);
+    double v = 0.0;
+    if (any) v = warp_sum(t == tt ? contrib : 0.0);
+    if (lane == 0) sh_part[warp * a.T + tt] = v;
+  }
+  __syncthreads();
+  for (int tt = threadIdx.x; tt < a.T; tt += blockDim.x) {
+    double s = 0.0;
+    for (int w = 0; w < nw; ++w) s += sh_part[w * a.T + tt];
+    if (s != 0.0) atomicAdd(&a.border[f * a.T + tt], s);
+  }
+}
+
+// grid (frames), block 1024: exclusive scan of counts -> offsets[0..nbins].
+__global__ void __launch_bounds__(1024) k_scan(DevArgs a) {
+  __shared__ int sums[1024];
+  const int f = blockIdx.x;
+  const int nb = a.nbins;
+  const int *c = a.counts + static_cast<int64_t>(f) * nb;
+  int *o = a.offsets + static_cast<int64_t>(f) * (nb + 1);
+  const int per = (nb + blockDim.x - 1) / blockDim.x;
+  const int s0 = threadIdx.x * per;
+  int local = 0;
+  for (int i = 0; i < per; ++i)
+    if (s0 + i < nb) local += c[s0 + i];
+  sums[threadIdx.x] = local;
+  __syncthreads();
+  for (int off = 1; off < blockDim.x; off <<= 1) {
+    const int v = threadIdx.x >= off ? sums[threadIdx.x - off] : 0;
+    __syncthreads();
+    sums[threadIdx.x] += v;
+    __syncthreads();
+  }
+  int run = sums[threadIdx.x] - local;
+  for (int i = 0; i < per; ++i) {
+    if (s0 + i < nb) {
+      o[s0 + i] = run;
+      run += c[s0 + i];
+    }
+  }
+  if (threadIdx.x == blockDim.x - 1) o[nb] = sums[threadIdx.x];
+}
+
+// grid (ceil(M/256), frames): records sorted by (type, home tile).
+__global__ void __launch_bounds__(kThreads) k_scatter_atoms(DevArgs a) {
+  __shared__ float oc[9];
+  const int f = blockIdx.y;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (threadIdx.x < 9) oc[threadIdx.x] = a.geom[f * kGeom + threadIdx.x];
+  __syncthreads();
+  if (e >= a.M) return;
+  const int at = a.entry_atom[e];
+  const float *p = a.xyz + f * a.frame_stride + 3ll * at;
+  const float x0 = p[0], y0 = p[1], z0 = p[2];
+  const float r0 = grid_coord(oc + 0, x0, y0, z0, a.n[0]);
+  const float r1 = grid_coord(oc + 3, x0, y0, z0, a.n[1]);
+  const float r2 = grid_coord(oc + 6, x0, y0, z0, a.n[2]);
+  const int2 k = a.key[static_cast<int64_t>(f) * a.M + e];
+  const int pos = a.offsets[static_cast<int64_t>(f) * (a.nbins + 1) + k.x] + k.y;
+  a.rec[static_cast<int64_t>(f) * a.M + pos] = make_float4(r0, r1, r2, __int_as_float(e));
+}
+
+// Distinct home tiles whose atoms can reach columns [c0, c0+cw) along an axis
+// of length n with `order`-tap stencils starting at the home position.
+__device__ __forceinline__ int home_tiles(int c0, int cw, int order, int n, int *out) {
+  int cnt = 0;
+  for (int d = 0; d < cw + order - 1; ++d) {
+    int x = (c0 - order + 1 + d) % n;
+    if (x < 0) x += n;
+    const int h = x / kTile;
+    bool seen = false;
+    for (int k = 0; k < cnt; ++k) seen |= (out[k] == h);
+    if (!seen && cnt < 4) out[cnt++] = h;
+  }
+  return cnt;
+}
+
+// grid (stiles_x*stiles_y, T, frames), block 256.
+// Dynamic shared memory: tile nz*64 floats | twiddles ez*nkzp float2 | reduction 20*64 float2.
+__global__ void __launch_bounds__(kThreads) k_spread_zdft(DevArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int nz = a.n[2], ez = a.ext[2];
+  float *tile = reinterpret_cast<float *>(smem);
+  float2 *tws = reinterpret_cast<float2 *>(tile + static_cast<size_t>(nz) * kCols);
+  float2 *red = tws + static_cast<size_t>(ez) * a.nkzp;
+  const int f = blockIdx.z, t = blockIdx.y;
+  const int TX = blockIdx.x % a.stiles[0], TY = blockIdx.x / a.stiles[0];
+  const int x0 = TX * kTile, y0 = TY * kTile;
+  const int cw = min(kTile, a.ext[0] - x0), ch = min(kTile, a.ext[1] - y0);
+  const int tid = threadIdx.x;
+
+  for (int i = tid; i < nz * kCols; i += blockDim.x) tile[i] = 0.0f;
+  {
+    const float4 *src = reinterpret_cast<const float4 *>(a.twz);
+    float4 *dst = reinterpret_cast<float4 *>(tws);
+    const int n4 = ez * a.nkzp / 2;
+    for (int i = tid; i < n4; i += blockDim.x) dst[i] = src[i];
+  }
+  int hx[4], hy[4];
+  const int nhx = home_tiles(x0, cw, a.order, a.n[0], hx);
+  const int nhy = home_tiles(y0, ch, a.order, a.n[1], hy);
+  __syncthreads();
+
+  // --- spreading into the shared column tile ---
+  const int *off = a.offsets + static_cast<int64_t>(f) * (a.nbins + 1);
+  const float4 *rec = a.rec + static_cast<int64_t>(f) * a.M;
+  const int P = a.order, nt = a.ntaps;
+  for (int ix = 0; ix < nhx; ++ix) {
+    for (int iy = 0; iy < nhy; ++iy) {
+      const int bin = (t * a.tiles[1] + hy[iy]) * a.tiles[0] + hx[ix];
+      const int s = off[bin], e = off[bin + 1];
+      for (int i = s + tid; i < e; i += blockDim.x) {
+        const float4 q = rec[i];
+        const int m0 = static_cast<int>(q.x), m1 = static_cast<int>(q.y),
+                  m2 = static_cast<int>(q.z);
+        float wx[4], wy[4], wz[4];
+        cubic_weights(q.x - static_cast<float>(m0), wx);
+        cubic_weights(q.y - static_cast<float>(m1), wy);
+        cubic_weights(q.z - static_cast<float>(m2), wz);
+        int zs[4];
+#pragma unroll
+        for (int o = 0; o < 4; ++o) {
+          int z = m2 - P + o;
+          if (z < 0) z += nz;
+          zs[o] = z;
+        }
+#pragma unroll
+        for (int o = 0; o < 4; ++o) {
+          if (o >= nt) break;
+          int x = m0 - P + o;
+          if (x < 0) x += a.n[0];
+          const int lx = x - x0;
+          if (static_cast<unsigned>(lx) >= static_cast<unsigned>(cw)) continue;
+#pragma unroll
+          for (int p = 0; p < 4; ++p) {
+            if (p >= nt) break;
+            int y = m1 - P + p;
+            if (y < 0) y += a.n[1];
+            const int ly = y - y0;
+            if (static_cast<unsigned>(ly) >= static_cast<unsigned>(ch)) continue;
+            const float wxy = wx[o] * wy[p];
+            float *col = tile + lx * kTile + ly;
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+              if (r >= nt) break;
+              atomicAdd(col + zs[r] * kCols, wxy * wz[r]);
+            }
+          }
+        }
+      }
+    }
+  }
+  __syncthreads();
+
+  // --- mean padding: the supercell is g on the corner block and the border
+  // mean elsewhere, i.e. (g - mean) on the corner plus a constant whose
+  // transform lives at k = 0 only ---
+  const float mean =
+      static_cast<float>(a.border[static_cast<int64_t>(f) * a.T + t] / a.border_count);
+  for (int i = tid; i < ez * kCols; i += blockDim.x) {
+    const int col = i % kCols;
+    if ((col / kTile) < cw && (col % kTile) < ch) tile[i] -= mean;
+  }
+  __syncthreads();
+
+  // --- z-axis DFT of the 64 columns restricted to kz in [0, nkz) ---
+  const int warp = tid >> 5, lane = tid & 31;
+  const int ngroups = (a.nkz + kKzGroup - 1) / kKzGroup;
+  const int gpp = ngroups >= 2 ? 2 : 1;
+  const int zsplit = (kThreads / 32) / gpp;
+  const int kg = warp % gpp, zsi = warp / gpp;
+  const int zlo = zsi * ez / zsplit, zhi = (zsi + 1) * ez / zsplit;
+  const float2 *tile2 = reinterpret_cast<const float2 *>(tile);
+  const int ex = a.ext[0], ey = a.ext[1];
+  const int64_t zplane = static_cast<int64_t>(ex) * ey;
+  float2 *Zft = a.Z + (static_cast<int64_t>(f) * a.T + t) * a.nkz * zplane;
+  for (int kpass = 0; kpass * gpp * kKzGroup < a.nkz; ++kpass) {
+    const int kbase = (kpass * gpp + kg) * kKzGroup;
+    float2 acc0[kKzGroup], acc1[kKzGroup];
+#pragma unroll
+    for (int j = 0; j < kKzGroup; ++j) acc0[j] = acc1[j] = make_float2(0.f, 0.f);
+    if (kbase < a.nkz) {
+      for (int z = zlo; z < zhi; ++z) {
+        const float2 g = tile2[z * (kCols / 2) + lane];
+        const float4 *w4 = reinterpret_cast<const float4 *>(tws + static_cast<size_t>(z) * a.nkzp + kbase);
+#pragma unroll
+        for (int j = 0; j < kKzGroup / 2; ++j) {
+          const float4 w = w4[j];
+          acc0[2 * j].x = fmaf(g.x, w.x, acc0[2 * j].x);
+          acc0[2 * j].y = fmaf(g.x, w.y, acc0[2 * j].y);
+          acc1[2 * j].x = fmaf(g.y, w.x, acc1[2 * j].x);
+          acc1[2 * j].y = fmaf(g.y, w.y, acc1[2 * j].y);
+          acc0[2 * j + 1].x = fmaf(g.x, w.z, acc0[2 * j + 1].x);
+          acc0[2 * j + 1].y = fmaf(g.x, w.w, acc0[2 * j + 1].y);
+          acc1[2 * j + 1].x = fmaf(g.y, w.z, acc1[2 * j + 1].x);
+          acc1[2 * j + 1].y = fmaf(g.y, w.w, acc1[2 * j + 1].y);
+        }
+      }
+    }
+    // reduce the z splits: red[kz_local][col]
+    const int kzl_n = gpp * kKzGroup;
+    for (int i = tid; i < kzl_n * kCols; i += blockDim.x) red[i] = make_float2(0.f, 0.f);
+    __syncthreads();
+    for (int s = 0; s < zsplit; ++s) {
+      if (zsi == s && kbase < a.nkz) {
+#pragma unroll
+        for (int j = 0; j < kKzGroup; ++j) {
+          float4 *dst = reinterpret_cast<float4 *>(red + (kg * kKzGroup + j) * kCols + 2 * lane);
+          float4 v = *dst;
+          v.x += acc0[j].x;
+          v.y += acc0[j].y;
+          v.z += acc1[j].x;
+          v.w += acc1[j].y;
+          *dst = v;
+        }
+      }
+      __syncthreads();
+    }
+    for (int i = tid; i < kzl_n * kCols; i += blockDim.x) {
+      const int kzl = i / kCols, col = i % kCols;
+      const int kz = kpass * kzl_n + kzl;
+      const int lx = col / kTile, ly = col % kTile;
+      if (kz < a.nkz && lx < cw && ly < ch)
+        Zft[kz * zplane + static_cast<int64_t>(x0 + lx) * ey + (y0 + ly)] = red[i];
+    }
+    __syncthreads();
+  }
+}
+
+// grid (ceil(ex/64), nkz, frames*T), block 256: y-axis DFT.
+// Y[f,t,kz][ky][x] = sum_y Z[f,t,kz][x][y] * exp(-2 pi i ja y / nny).
+__global__ void __launch_bounds__(kThreads) k_ydft(DevArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  float2 *zs = reinterpret_cast<float2 *>(smem);        // [kYChunk][kYStride]
+  float2 *tys = zs + kYChunk * kYStride;                // [kYChunk][nkyp]
+  const int ft = blockIdx.z, kz = blockIdx.y;
+  const int xb = blockIdx.x * kYRows;
+  const int ex = a.ext[0], ey = a.ext[1];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const float2 *Zp = a.Z + (static_cast<int64_t>(ft) * a.nkz + kz) * ex * ey;
+  float2 *Yp = a.Y + (static_cast<int64_t>(ft) * a.nkz + kz) * a.nky * ex;
+  const int xr0 = xb + 2 * lane;
+  for (int kp = 0; kp * kKyPass < a.nky; ++kp) {
+    const int kbase = kp * kKyPass + warp * kKyGroup;
+    float2 acc0[kKyGroup], acc1[kKyGroup];
+#pragma unroll
+    for (int j = 0; j < kKyGroup; ++j) acc0[j] = acc1[j] = make_float2(0.f, 0.f);
+    for (int y0 = 0; y0 < ey; y0 += kYChunk) {
+      const int yn = min(kYChunk, ey - y0);
+      for (int i = tid; i < kYRows * kYChunk; i += blockDim.x) {
+        const int row = i / kYChunk, yy = i % kYChunk;
+        const int x = xb + row, y = y0 + yy;
+        zs[yy * kYStride + row] =
+            (x < ex && yy < yn) ? Zp[static_cast<int64_t>(x) * ey + y] : make_float2(0.f, 0.f);
+      }
+      {
+        const float4 *src = reinterpret_cast<const float4 *>(a.twy + static_cast<size_t>(y0) * a.nkyp);
+        float4 *dst = reinterpret_cast<float4 *>(tys);
+        const int n4 = yn * a.nkyp / 2;
+        for (int i = tid; i < n4; i += blockDim.x) dst[i] = src[i];
+      }
+      __syncthreads();
+      if (kbase < a.nky) {
+        for (int yy = 0; yy < yn; ++yy) {
+          const float4 z2 = *reinterpret_cast<const float4 *>(zs + yy * kYStride + 2 * lane);
+          const float4 *w4 = reinterpret_cast<const float4 *>(tys + yy * a.nkyp + kbase);
+#pragma unroll
+          for (int j = 0; j < kKyGroup / 2; ++j) {
+            const float4 w = w4[j];
+            // (z.x + i z.y)(w.x + i w.y)
+            acc0[2 * j].x = fmaf(z2.x, w.x, fmaf(-z2.y, w.y, acc0[2 * j].x));
+            acc0[2 * j].y = fmaf(z2.x, w.y, fmaf(z2.y, w.x, acc0[2 * j].y));
+            acc1[2 * j].x = fmaf(z2.z, w.x, fmaf(-z2.w, w.y, acc1[2 * j].x));
+            acc1[2 * j].y = fmaf(z2.z, w.y, fmaf(z2.w, w.x, acc1[2 * j].y));
+            acc0[2 * j + 1].x = fmaf(z2.x, w.z, fmaf(-z2.y, w.w, acc0[2 * j + 1].x));
+            acc0[2 * j + 1].y = fmaf(z2.x, w.w, fmaf(z2.y, w.z, acc0[2 * j + 1].y));
+            acc1[2 * j + 1].x = fmaf(z2.z, w.z, fmaf(-z2.w, w.w, acc1[2 * j + 1].x));
+            acc1[2 * j + 1].y = fmaf(z2.z, w.w, fmaf(z2.w, w.z, acc1[2 * j + 1].y));
+          }
+        }
+      }
+      __syncthreads();
+    }
+    if (kbase < a.nky) {
+#pragma unroll
+      for (int j = 0; j < kKyGroup; ++j) {
+        const int ky = kbase + j;
+        if (ky < a.nky) {
+          if (xr0 < ex) Yp[static_cast<int64_t>(ky) * ex + xr0] = acc0[j];
+          if (xr0 + 1 < ex) Yp[static_cast<int64_t>(ky) * ex + xr0 + 1] = acc1[j];
+        }
+      }
+    }
+  }
+}
+
+// grid (ceil(nky/4), nkz, frames), block 256: x-axis DFT, form factors, type
+// sum, modulus.  Dynamic shared memory: twx ex*nkxp | Y rows T*ex | F T*nkxp (float2).
+__global__ void __launch_bounds__(kThreads) k_xdft_post(DevArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int ex = a.ext[0];
+  float2 *txs = reinterpret_cast<float2 *>(smem);
+  float2 *ys = txs + static_cast<size_t>(ex) * a.nkxp;
+  float2 *fs = ys + static_cast<size_t>(a.T) * ex;
+  __shared__ float ocs[9];
+  __shared__ float means[64];
+  const int f = blockIdx.z, kz = blockIdx.y;
+  const int tid = threadIdx.x;
+  if (tid < 9) ocs[tid] = a.geom[f * kGeom + 9 + tid];
+  for (int t = tid; t < a.T && t < 64; t += blockDim.x)
+    means[t] = static_cast<float>(a.border[static_cast<int64_t>(f) * a.T + t] / a.border_count);
+  {
+    const float4 *src = reinterpret_cast<const float4 *>(a.twx);
+    float4 *dst = reinterpret_cast<float4 *>(txs);
+    const int n4 = ex * a.nkxp / 2;
+    for (int i = tid; i < n4; i += blockDim.x) dst[i] = src[i];
+  }
+  const int ka = signed_k(kz, a.nn[2], a.nf[2]);
+  for (int r = 0; r < kXRows; ++r) {
+    const int ky = blockIdx.x * kXRows + r;
+    if (ky >= a.nky) break;
+    const int ja = a.ky_lo + ky;
+    __syncthreads();
+    for (int i = tid; i < a.T * ex; i += blockDim.x) {
+      const int t = i / ex, x = i % ex;
+      ys[i] = a.Y[((static_cast<int64_t>(f) * a.T + t) * a.nkz + kz) * a.nky * ex +
+                  static_cast<int64_t>(ky) * ex + x];
+    }
+    __syncthreads();
+    for (int i = tid; i < a.T * a.nkx; i += blockDim.x) {
+      const int t = i / a.nkx, kx = i % a.nkx;
+      const float2 *yr = ys + t * ex;
+      float2 acc = make_float2(0.f, 0.f);
+      for (int x = 0; x < ex; ++x) {
+        const float2 v = yr[x];
+        const float2 w = txs[x * a.nkxp + kx];
+        acc.x = fmaf(v.x, w.x, fmaf(-v.y, w.y, acc.x));
+        acc.y = fmaf(v.x, w.y, fmaf(v.y, w.x, acc.y));
+      }
+      if (ka == 0 && ja == 0 && a.kx_lo + kx == 0)
+        acc.x += static_cast<float>(static_cast<double>(means[t < 64 ? t : 63]) * a.nn3);
+      fs[t * a.nkxp + kx] = acc;
+    }
+    __syncthreads();
+    for (int kx = tid; kx < a.nkx; kx += blockDim.x) {
+      const int ia = a.kx_lo + kx;
+      const float mw = kpoint_q(ocs, ia, ja, ka);
+      float I = 0.0f;
+      if (!(mw > a.qcut)) {
+        const float q = mw / (4.0 * M_PI);
+        const float q2 = q * q;
+        float2 A = make_float2(0.f, 0.f);
+        for (int t = 0; t < a.T; ++t) {
+          const float ft = form_factor(a.ff + 9 * t, q2);
+          const float2 F = fs[t * a.nkxp + kx];
+          A.x = fmaf(ft, F.x, A.x);
+          A.y = fmaf(ft, F.y, A.y);
+        }
+        const int i = ia < 0 ? ia + a.nn[0] : ia;
+        const int j = ja < 0 ? ja + a.nn[1] : ja;
+        const float bsp = a.modx[i] * a.mody[j] * a.modz[kz];
+        I = (A.x * A.x + A.y * A.y) * bsp;
+      }
+      a.ibox[((static_cast<int64_t>(f) * a.nkz + kz) * a.nky + ky) * a.nkx + kx] = I;
+    }
+  }
+}
+
+// grid (nkz, planes), block 256: mirror-weighted histogram of one kz plane.
+// `vals` holds nkz*nky*nkx values per plane; `geom` the frame geometry.
+template <typename V>
+__global__ void __launch_bounds__(kThreads)
+    k_hist(DevArgs a, const V *vals, const float *geom, int geom_stride, double fact,
+           double *hist, double *nhist) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int npts = a.nky * a.nkx;
+  const bool in_smem = a.num_bins <= kHistSmemBins;
+  double *sh = reinterpret_cast<double *>(smem);
+  double *sn = sh + (in_smem ? a.num_bins : 0);
+  V *pl = reinterpret_cast<V *>(sn + (in_smem ? a.num_bins : 0));
+  __shared__ float ocs[9];
+  const int kz = blockIdx.x, f = blockIdx.y;
+  const int tid = threadIdx.x;
+  if (tid < 9) ocs[tid] = geom[f * geom_stride + 9 + tid];
+  if (in_smem)
+    for (int b = tid; b < 2 * a.num_bins; b += blockDim.x) sh[b] = 0.0;
+  const V *src = vals + (static_cast<int64_t>(f) * a.nkz + kz) * npts;
+  for (int p = tid; p < npts; p += blockDim.x) pl[p] = src[p];
+  __syncthreads();
+  const int ka = signed_k(kz, a.nn[2], a.nf[2]);
+  const int kx_hi = a.kx_lo + a.nkx - 1, ky_hi = a.ky_lo + a.nky - 1;
+  double *dh = in_smem ? sh : hist;
+  double *dn = in_smem ? sn : nhist;
+  for (int p = tid; p < npts; p += blockDim.x) {
+    const int ky = p / a.nkx, kx = p % a.nkx;
+    const int ia = a.kx_lo + kx, ja = a.ky_lo + ky;
+    const float mw = kpoint_q(ocs, ia, ja, ka);
+    if (mw > a.qcut) continue;
+    if (a.dq <= 0.0f) continue;
+    const int h0 = static_cast<int>(mw / a.dq);
+    if (h0 < 0 || h0 >= a.num_bins) continue;
+    double v, c;
+    if (ia == 0 && ja == 0 && ka == 0) {
+      v = static_cast<double>(pl[p]) * fact;
+      c = 1.0;
+    } else {
+      int ib = -ia, jb = -ja;
+      if (ib > kx_hi) ib = ia;
+      if (jb > ky_hi) jb = ja;
+      const int pm = (jb - a.ky_lo) * a.nkx + (ib - a.kx_lo);
+      if (sizeof(V) == 4)
+        v = static_cast<double>(static_cast<float>(pl[p]) + static_cast<float>(pl[pm])) * fact;
+      else
+        v = (static_cast<double>(pl[p]) + static_cast<double>(pl[pm])) * fact;
+      c = 2.0;
+    }
+    atomicAdd(dh + h0, v);
+    atomicAdd(dn + h0, c);
+  }
+  if (in_smem) {
+    __syncthreads();
+    for (int b = tid; b < a.num_bins; b += blockDim.x) {
+      if (sn[b] != 0.0) {
+        atomicAdd(hist + b, sh[b]);
+        atomicAdd(nhist + b, sn[b]);
+      }
+    }
+  }
+}
+
+// grid (ceil(points/256)), block 256: nvt intensity sum over the batch's frames.
+__global__ void k_accumulate(DevArgs a, int nframes) {
+  const int64_t npl = static_cast<int64_t>(a.nkz) * a.nky * a.nkx;
+  const int64_t p = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (p >= npl) return;
+  double s = a.iacc[p];
+  for (int f = 0; f < nframes; ++f) s += static_cast<double>(a.ibox[f * npl + p]);
+  a.iacc[p] = s;
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+struct Ring {
+  float *host = nullptr;
+  cudaEvent_t ev[kRing] = {};
+  int next = 0;
+};
+
+// Timed stages of saxs_forward, in launch order.
+enum Stage { kStBin, kStScan, kStScatter, kStSpread, kStYdft, kStXdft, kStHist, kStages };
+const char *kStageNames[kStages] = {"k_bin_atoms", "k_scan", "k_scatter_atoms", "k_spread_zdft",
+                                    "k_ydft", "k_xdft_post", "k_hist"};
+
+struct StageRecord {
+  cudaEvent_t start[kStages] = {};
+  cudaEvent_t stop[kStages] = {};
+  bool used[kStages] = {};
+};
+
+}  // namespace
+
+struct SaxsPlan {
+  int device = 0;
+  SaxsParams p{};
+  std::vector<float> ff;
+  DevArgs a{};
+  int ensemble = SAXS_NPT;
+  long long half[3] = {0, 0, 0};
+  bool full_axis[3] = {false, false, false};
+  float sigma_scale = 1.0f;  // nx / nnx
+  int frames = 0;            // frames accumulated
+  int last_frame_batch = 0;  // frames in the last forward batch
+  size_t bytes = 0;
+  size_t smem_spread = 0, smem_ydft = 0, smem_xdft = 0, smem_hist = 0, smem_bin = 0;
+  std::vector<void *> allocations;
+  Ring ring;
+  float *d_geom0 = nullptr;
+  double *d_tmp_hist = nullptr;
+  bool profiling = false;
+  std::vector<StageRecord> prof_pending;
+  std::vector<cudaEvent_t> event_pool;
+};
+
+namespace {
+
+template <typename T>
+int dalloc(SaxsPlan *pl, T **ptr, size_t count) {
+  const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+  cudaError_t e = cudaMalloc(reinterpret_cast<void **>(ptr), bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    size_t fr = 0, tot = 0;
+    cudaMemGetInfo(&fr, &tot);
+    return fail(SAXS_E_NOMEM, "device allocation of " + std::to_string(bytes) +
+                                  " bytes failed (" + cudaGetErrorString(e) + "; free " +
+                                  std::to_string(fr) + " of " + std::to_string(tot) + ")");
+  }
+  pl->allocations.push_back(*ptr);
+  pl->bytes += bytes;
+  return SAXS_OK;
+}
+
+void frame_geometry(const SaxsPlan *pl, const float box[9], float g[kGeom]) {
+  float oc[9];
+  saxs::cell_oc(box, oc);
+  for (int i = 0; i < 9; ++i) {
+    g[i] = oc[i];
+    g[9 + i] = pl->sigma_scale * oc[i];
+  }
+  for (int i = 18; i < kGeom; ++i) g[i] = 0.0f;
+}
+
+int check_box(const float box[9]) {
+  for (int i = 0; i < 9; ++i)
+    if (!std::isfinite(box[i])) return fail(SAXS_E_INVALID, "box contains a non-finite value");
+  if (!(box[0] > 0.f) || !(box[4] > 0.f) || !(box[8] > 0.f))
+    return fail(SAXS_E_INVALID, "box diagonal must be positive");
+  return SAXS_OK;
+}
+
+void destroy(SaxsPlan *pl) {
+  if (!pl) return;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(pl->device);
+  for (void *p : pl->allocations) cudaFree(p);
+  for (int i = 0; i < kRing; ++i)
+    if (pl->ring.ev[i]) cudaEventDestroy(pl->ring.ev[i]);
+  for (auto &r : pl->prof_pending)
+    for (int k = 0; k < kStages; ++k) {
+      if (r.start[k]) cudaEventDestroy(r.start[k]);
+      if (r.stop[k]) cudaEventDestroy(r.stop[k]);
+    }
+  for (cudaEvent_t e : pl->event_pool) cudaEventDestroy(e);
+  if (pl->ring.host) cudaFreeHost(pl->ring.host);
+  cudaSetDevice(prev);
+  delete pl;
+}
+
+int create(const SaxsParams *prm, SaxsPlan **out) {
+  if (!prm || !out) return fail(SAXS_E_INVALID, "null argument");
+  *out = nullptr;
+  const SaxsParams &p = *prm;
+  for (int d = 0; d < 3; ++d)
+    if (p.grid[d] <= 0) return fail(SAXS_E_INVALID, "Grid dimensions must be positive");
+  if (p.order < 1 || p.order > 8)
+    return fail(SAXS_E_INVALID, "Spline order must be between 1 and 8");
+  if (p.ntypes < 1 || !p.form_factors) return fail(SAXS_E_INVALID, "at least one atom type is required");
+  if (p.natoms < 0 || p.nentries < 0) return fail(SAXS_E_INVALID, "negative atom count");
+  if (p.nentries > 0 && (!p.entry_atom || !p.entry_type))
+    return fail(SAXS_E_INVALID, "atom lists missing");
+  if (p.max_frames < 1) return fail(SAXS_E_INVALID, "max_frames must be >= 1");
+  if (p.ensemble != SAXS_NPT && p.ensemble != SAXS_NVT)
+    return fail(SAXS_E_INVALID, "ensemble must be npt or nvt");
+  if (int rc = check_box(p.box0)) return rc;
+  for (int i = 0; i < p.nentries; ++i) {
+    if (p.entry_atom[i] < 0 || p.entry_atom[i] >= p.natoms)
+      return fail(SAXS_E_INVALID, "atom index " + std::to_string(p.entry_atom[i]) +
+                                      " out of range [0, " + std::to_string(p.natoms) + ")");
+    if (p.entry_type[i] < 0 || p.entry_type[i] >= p.ntypes)
+      return fail(SAXS_E_INVALID, "type index out of range");
+  }
+  const bool scaled = p.scaled_grid[0] > 0 || p.scaled_grid[1] > 0 || p.scaled_grid[2] > 0;
+  int nn[3];
+  for (int d = 0; d < 3; ++d) {
+    if (scaled) {
+      if (p.scaled_grid[d] <= 0) return fail(SAXS_E_INVALID, "Scaled grid dimensions must be positive");
+      nn[d] = p.scaled_grid[d];
+    } else {
+      if (!(p.scale_factor > 0.0f))
+        return fail(SAXS_E_INVALID, "Scale factor must be positive when scaled grid is not provided");
+      const long long v = saxs::closest_product(p.grid[d], p.scale_factor);
+      if (v < 1 || v > (1 << 20)) return fail(SAXS_E_INVALID, "scaled grid out of range");
+      nn[d] = static_cast<int>(v);
+    }
+  }
+  const int ntaps = std::min(p.order, 4);
+  for (int d = 0; d < 3; ++d) {
+    if (p.grid[d] < p.order)
+      return fail(SAXS_E_INVALID, "grid dimension smaller than the spline order");
+    if (nn[d] < 2) return fail(SAXS_E_INVALID, "scaled grid dimension must be >= 2");
+  }
+
+  SaxsPlan *pl = new SaxsPlan();
+  cudaGetDevice(&pl->device);
+  pl->p = p;
+  pl->ensemble = p.ensemble;
+  pl->ff.assign(p.form_factors, p.form_factors + 9 * p.ntypes);
+  DevArgs &a = pl->a;
+  for (int d = 0; d < 3; ++d) {
+    a.n[d] = p.grid[d];
+    a.nn[d] = nn[d];
+    a.ext[d] = std::min(p.grid[d], nn[d]);
+    a.nf[d] = saxs::nf_of(nn[d]);
+  }
+  a.order = p.order;
+  a.ntaps = ntaps;
+  a.T = p.ntypes;
+  a.M = p.nentries;
+  a.tiles[0] = (a.n[0] + kTile - 1) / kTile;
+  a.tiles[1] = (a.n[1] + kTile - 1) / kTile;
+  a.stiles[0] = (a.ext[0] + kTile - 1) / kTile;
+  a.stiles[1] = (a.ext[1] + kTile - 1) / kTile;
+  a.nbins = a.T * a.tiles[0] * a.tiles[1];
+  a.dz = static_cast<int>(0.07f * a.n[2] / 2);  // borderBins (saxsKernel.h:107-110)
+  {
+    int planes = 0;
+    for (int z = 0; z < a.n[2]; ++z)
+      if (!(z > a.dz && z < a.n[2] - a.dz)) ++planes;
+    a.border_count = static_cast<double>(a.n[0]) * a.n[1] * planes;
+  }
+  a.nn3 = static_cast<double>(nn[0]) * nn[1] * nn[2];
+
+  float oc0[9];
+  saxs::cell_oc(p.box0, oc0);
+  saxs::histogram_parameters(nn, oc0, p.scale_factor, p.bin_size, p.qcut, &a.dq, &a.qcut,
+                             &a.num_bins);
+  if (a.num_bins < 1) a.num_bins = 1;
+  pl->sigma_scale = static_cast<float>(a.n[0]) / static_cast<float>(nn[0]);
+
+  // k-box: every integer k with |2 pi ocs k| <= qcut for the first frame and
+  // for boxes up to `box_margin` smaller.
+  float ocs0[9];
+  for (int i = 0; i < 9; ++i) ocs0[i] = pl->sigma_scale * oc0[i];
+  const double margin = std::max(0.0f, p.box_margin) + 1e-5;
+  saxs::kbox_halfwidths(ocs0, a.qcut, margin, pl->half);
+  for (int d = 0; d < 2; ++d) {
+    const long long hmax = a.nf[d] - 1;
+    if (pl->half[d] >= hmax) {
+      pl->full_axis[d] = true;
+      pl->half[d] = hmax;
+    }
+  }
+  a.kx_lo = pl->full_axis[0] ? a.nf[0] - nn[0] : -static_cast<int>(pl->half[0]);
+  a.nkx = pl->full_axis[0] ? nn[0] : 2 * static_cast<int>(pl->half[0]) + 1;
+  a.ky_lo = pl->full_axis[1] ? a.nf[1] - nn[1] : -static_cast<int>(pl->half[1]);
+  a.nky = pl->full_axis[1] ? nn[1] : 2 * static_cast<int>(pl->half[1]) + 1;
+  if (pl->half[2] >= nn[2] / 2) {
+    pl->full_axis[2] = true;
+    pl->half[2] = nn[2] / 2;
+  }
+  a.nkz = static_cast<int>(pl->half[2]) + 1;
+  a.nkzp = round_up(a.nkz, kKzPass);
+  a.nkxp = round_up(a.nkx, 2);
+  a.nkyp = round_up(a.nky, kKyGroup);
+
+  // shared-memory budgets
+  pl->smem_spread = static_cast<size_t>(a.n[2]) * kCols * sizeof(float) +
+                    static_cast<size_t>(a.ext[2]) * a.nkzp * sizeof(float2) +
+                    static_cast<size_t>(kKzPass) * kCols * sizeof(float2);
+  pl->smem_ydft = static_cast<size_t>(kYChunk) * kYStride * sizeof(float2) +
+                  static_cast<size_t>(kYChunk) * a.nkyp * sizeof(float2);
+  pl->smem_xdft = (static_cast<size_t>(a.ext[0]) * a.nkxp + static_cast<size_t>(a.T) * a.ext[0] +
+                   static_cast<size_t>(a.T) * a.nkxp) * sizeof(float2);
+  const size_t plane = static_cast<size_t>(a.nky) * a.nkx;
+  pl->smem_hist = (a.num_bins <= kHistSmemBins ? 2 * sizeof(double) * a.num_bins : 0) +
+                  plane * sizeof(double);
+  pl->smem_bin = static_cast<size_t>(kThreads / 32) * a.T * sizeof(double);
+  if (pl->smem_spread > static_cast<size_t>(kMaxSmem) || pl->smem_xdft > static_cast<size_t>(kMaxSmem) ||
+      pl->smem_hist > static_cast<size_t>(kMaxSmem) || pl->smem_bin > 48 * 1024) {
+    destroy(pl);
+    return fail(SAXS_E_INVALID,
+                "grid / q-cut combination exceeds the shared-memory budget of the pruned path (z "
+                "extent " + std::to_string(a.n[2]) + ", k-box " + std::to_string(a.nkx) + "x" +
+                    std::to_string(a.nky) + "x" + std::to_string(a.nkz) + ")");
+  }
+  if (a.T > 64) {
+    destroy(pl);
+    return fail(SAXS_E_INVALID, "at most 64 element types are supported");
+  }
+
+  const int B = p.max_frames;
+  const int ex = a.ext[0], ey = a.ext[1], ez = a.ext[2];
+  int rc = SAXS_OK;
+  int32_t *d_ea = nullptr, *d_et = nullptr;
+  float2 *d_twz = nullptr, *d_twy = nullptr, *d_twx = nullptr;
+  float *d_modx = nullptr, *d_mody = nullptr, *d_modz = nullptr, *d_ff = nullptr, *d_geom = nullptr;
+  int *d_status = nullptr;
+#define ALLOC(ptr, cnt)                       \
+  do {                                        \
+    if ((rc = dalloc(pl, &(ptr), (cnt)))) {   \
+      destroy(pl);                            \
+      return rc;                              \
+    }                                         \
+  } while (0)
+  ALLOC(d_ea, a.M);
+  ALLOC(d_et, a.M);
+  ALLOC(d_twz, static_cast<size_t>(ez) * a.nkzp);
+  ALLOC(d_twy, static_cast<size_t>(ey) * a.nkyp);
+  ALLOC(d_twx, static_cast<size_t>(ex) * a.nkxp);
+  ALLOC(d_modx, nn[0]);
+  ALLOC(d_mody, nn[1]);
+  ALLOC(d_modz, nn[2]);
+  ALLOC(d_ff, 9 * a.T);
+  ALLOC(d_geom, static_cast<size_t>(B) * kGeom);
+  ALLOC(pl->d_geom0, kGeom);
+  ALLOC(d_status, 4);
+  ALLOC(a.key, static_cast<size_t>(B) * a.M);
+  ALLOC(a.counts, static_cast<size_t>(B) * a.nbins);
+  ALLOC(a.offsets, static_cast<size_t>(B) * (a.nbins + 1));
+  ALLOC(a.rec, static_cast<size_t>(B) * a.M);
+  ALLOC(a.border, static_cast<size_t>(B) * a.T);
+  ALLOC(a.Z, static_cast<size_t>(B) * a.T * a.nkz * ex * ey);
+  ALLOC(a.Y, static_cast<size_t>(B) * a.T * a.nkz * a.nky * ex);
+  ALLOC(a.ibox, static_cast<size_t>(B) * a.nkz * a.nky * a.nkx);
+  ALLOC(a.hist, a.num_bins);
+  ALLOC(a.nhist, a.num_bins);
+  ALLOC(pl->d_tmp_hist, 2 * a.num_bins);
+  if (pl->ensemble == SAXS_NVT) ALLOC(a.iacc, static_cast<size_t>(a.nkz) * a.nky * a.nkx);
+#undef ALLOC
+  a.entry_atom = d_ea;
+  a.entry_type = d_et;
+  a.twz = d_twz;
+  a.twy = d_twy;
+  a.twx = d_twx;
+  a.modx = d_modx;
+  a.mody = d_mody;
+  a.modz = d_modz;
+  a.ff = d_ff;
+  a.geom = d_geom;
+  a.status = d_status;
+
+  // host tables
+  std::vector<float2> twz(static_cast<size_t>(ez) * a.nkzp, make_float2(0.f, 0.f));
+  for (int z = 0; z < ez; ++z)
+    for (int k = 0; k < a.nkz; ++k) saxs::twiddle(k, z, nn[2], &twz[z * a.nkzp + k].x, &twz[z * a.nkzp + k].y);
+  std::vector<float2> twy(static_cast<size_t>(ey) * a.nkyp, make_float2(0.f, 0.f));
+  for (int y = 0; y < ey; ++y)
+    for (int k = 0; k < a.nky; ++k)
+      saxs::twiddle(a.ky_lo + k, y, nn[1], &twy[y * a.nkyp + k].x, &twy[y * a.nkyp + k].y);
+  std::vector<float2> twx(static_cast<size_t>(ex) * a.nkxp, make_float2(0.f, 0.f));
+  for (int x = 0; x < ex; ++x)
+    for (int k = 0; k < a.nkx; ++k)
+      saxs::twiddle(a.kx_lo + k, x, nn[0], &twx[x * a.nkxp + k].x, &twx[x * a.nkxp + k].y);
+  const int ndim = std::max(nn[0], std::max(nn[1], nn[2]));
+  std::vector<float> mx(nn[0]), my(nn[1]), mz(nn[2]);
+  saxs::bspline_moduli(nn[0], ndim, mx.data());
+  saxs::bspline_moduli(nn[1], ndim, my.data());
+  saxs::bspline_moduli(nn[2], ndim, mz.data());
+  float g0[kGeom];
+  frame_geometry(pl, p.box0, g0);
+
+  auto up = [&](void *dst, const void *src, size_t bytes) -> int {
+    if (bytes == 0) return SAXS_OK;
+    cudaError_t e = cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return fail(SAXS_E_CUDA, std::string("upload: ") + cudaGetErrorString(e));
+    return SAXS_OK;
+  };
+  if ((rc = up(d_ea, p.entry_atom, sizeof(int32_t) * a.M)) ||
+      (rc = up(d_et, p.entry_type, sizeof(int32_t) * a.M)) ||
+      (rc = up(d_twz, twz.data(), sizeof(float2) * twz.size())) ||
+      (rc = up(d_twy, twy.data(), sizeof(float2) * twy.size())) ||
+      (rc = up(d_twx, twx.data(), sizeof(float2) * twx.size())) ||
+      (rc = up(d_modx, mx.data(), sizeof(float) * nn[0])) ||
+      (rc = up(d_mody, my.data(), sizeof(float) * nn[1])) ||
+      (rc = up(d_modz, mz.data(), sizeof(float) * nn[2])) ||
+      (rc = up(d_ff, pl->ff.data(), sizeof(float) * pl->ff.size())) ||
+      (rc = up(pl->d_geom0, g0, sizeof(g0)))) {
+    destroy(pl);
+    return rc;
+  }
+  cudaError_t e = cudaMemset(a.hist, 0, sizeof(double) * a.num_bins);
+  if (e == cudaSuccess) e = cudaMemset(a.nhist, 0, sizeof(double) * a.num_bins);
+  if (e == cudaSuccess && a.iacc)
+    e = cudaMemset(a.iacc, 0, sizeof(double) * a.nkz * a.nky * a.nkx);
+  if (e == cudaSuccess) e = cudaMemset(d_status, 0, 4 * sizeof(int));
+  if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void **>(&pl->ring.host),
+                                           sizeof(float) * kRing * B * kGeom);
+  for (int i = 0; e == cudaSuccess && i < kRing; ++i)
+    e = cudaEventCreateWithFlags(&pl->ring.ev[i], cudaEventDisableTiming);
+  // The dynamic shared-memory limit is per kernel function, not per plan, so
+  // it is raised to the device maximum once for every plan alike.
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_spread_zdft, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ydft, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_xdft_post, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_hist<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_hist<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
+  if (e != cudaSuccess) {
+    destroy(pl);
+    return fail(SAXS_E_CUDA, std::string("plan setup: ") + cudaGetErrorString(e));
+  }
+  *out = pl;
+  return SAXS_OK;
+}
+
+int launch_check(const char *what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(SAXS_E_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+  return SAXS_OK;
+}
+
+cudaEvent_t pooled_event(SaxsPlan *pl) {
+  if (!pl->event_pool.empty()) {
+    cudaEvent_t e = pl->event_pool.back();
+    pl->event_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+// Records CUDA events around one stage when profiling is on.
+struct StageTimer {
+  SaxsPlan *pl;
+  StageRecord *rec;
+  cudaStream_t st;
+  void begin(int k) {
+    if (!rec) return;
+    rec->start[k] = pooled_event(pl);
+    rec->stop[k] = pooled_event(pl);
+    rec->used[k] = true;
+    cudaEventRecord(rec->start[k], st);
+  }
+  void end(int k) {
+    if (rec) cudaEventRecord(rec->stop[k], st);
+  }
+};
+
+int forward(SaxsPlan *pl, const float *xyz, int64_t stride, int nframes, const float *boxes,
+            cudaStream_t st) {
+  if (!pl) return fail(SAXS_E_INVALID, "null plan");
+  if (nframes < 1 || nframes > pl->p.max_frames)
+    return fail(SAXS_E_INVALID, "nframes must be in [1, max_frames]");
+  if (!boxes || (!xyz && pl->a.M > 0)) return fail(SAXS_E_INVALID, "null positions or boxes");
+  if (stride < 3ll * pl->p.natoms) return fail(SAXS_E_INVALID, "frame stride smaller than 3*natoms");
+  DevArgs a = pl->a;
+  a.xyz = xyz;
+  a.frame_stride = stride;
+  // geometry of each frame, checked against the planned k-box
+  Ring &ring = pl->ring;
+  const int slot = ring.next;
+  ring.next = (ring.next + 1) % kRing;
+  CUDA_TRY(cudaEventSynchronize(ring.ev[slot]));
+  float *g = ring.host + static_cast<size_t>(slot) * pl->p.max_frames * kGeom;
+  for (int f = 0; f < nframes; ++f) {
+    const float *box = boxes + 9 * f;
+    if (int rc = check_box(box)) return rc;
+    frame_geometry(pl, box, g + f * kGeom);
+    long long h[3];
+    saxs::kbox_halfwidths(g + f * kGeom + 9, a.qcut, 1e-5, h);
+    for (int d = 0; d < 3; ++d) {
+      if (!pl->full_axis[d] && h[d] > pl->half[d])
+        return fail(SAXS_E_RANGE, "frame box shrank beyond the planned k-box margin; "
+                                  "create the plan with a larger box_margin");
+    }
+  }
+  CUDA_TRY(cudaMemcpyAsync(const_cast<float *>(a.geom), g, sizeof(float) * nframes * kGeom,
+                           cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaEventRecord(ring.ev[slot], st));
+  CUDA_TRY(cudaMemsetAsync(a.counts, 0, sizeof(int) * nframes * a.nbins, st));
+  CUDA_TRY(cudaMemsetAsync(a.border, 0, sizeof(double) * nframes * a.T, st));
+
+  StageTimer tm{pl, nullptr, st};
+  if (pl->profiling) {
+    pl->prof_pending.emplace_back();
+    tm.rec = &pl->prof_pending.back();
+  }
+  if (a.M > 0) {
+    dim3 gb((a.M + kThreads - 1) / kThreads, nframes);
+    tm.begin(kStBin);
+    k_bin_atoms<<<gb, kThreads, pl->smem_bin, st>>>(a);
+    tm.end(kStBin);
+    if (int rc = launch_check("k_bin_atoms")) return rc;
+    tm.begin(kStScan);
+    k_scan<<<nframes, 1024, 0, st>>>(a);
+    tm.end(kStScan);
+    if (int rc = launch_check("k_scan")) return rc;
+    tm.begin(kStScatter);
+    k_scatter_atoms<<<gb, kThreads, 0, st>>>(a);
+    tm.end(kStScatter);
+    if (int rc = launch_check("k_scatter_atoms")) return rc;
+  } else {
+    CUDA_TRY(cudaMemsetAsync(a.offsets, 0, sizeof(int) * nframes * (a.nbins + 1), st));
+  }
+  {
+    dim3 gs(a.stiles[0] * a.stiles[1], a.T, nframes);
+    tm.begin(kStSpread);
+    k_spread_zdft<<<gs, kThreads, pl->smem_spread, st>>>(a);
+    tm.end(kStSpread);
+    if (int rc = launch_check("k_spread_zdft")) return rc;
+  }
+  {
+    dim3 gy((a.ext[0] + kYRows - 1) / kYRows, a.nkz, nframes * a.T);
+    tm.begin(kStYdft);
+    k_ydft<<<gy, kThreads, pl->smem_ydft, st>>>(a);
+    tm.end(kStYdft);
+    if (int rc = launch_check("k_ydft")) return rc;
+  }
+  {
+    dim3 gx((a.nky + kXRows - 1) / kXRows, a.nkz, nframes);
+    tm.begin(kStXdft);
+    k_xdft_post<<<gx, kThreads, pl->smem_xdft, st>>>(a);
+    tm.end(kStXdft);
+    if (int rc = launch_check("k_xdft_post")) return rc;
+  }
+  tm.begin(kStHist);
+  if (pl->ensemble == SAXS_NPT) {
+    dim3 gh(a.nkz, nframes);
+    k_hist<float><<<gh, kThreads, pl->smem_hist, st>>>(a, a.ibox, a.geom, kGeom, 1.0, a.hist,
+                                                       a.nhist);
+  } else {
+    const int64_t npl = static_cast<int64_t>(a.nkz) * a.nky * a.nkx;
+    k_accumulate<<<static_cast<unsigned>((npl + kThreads - 1) / kThreads), kThreads, 0, st>>>(a, nframes);
+  }
+  tm.end(kStHist);
+  if (int rc = launch_check("k_hist")) return rc;
+  pl->frames += nframes;
+  pl->last_frame_batch = nframes;
+  return SAXS_OK;
+}
+
+int histogram(SaxsPlan *pl, double *hist, double *nhist, cudaStream_t st) {
+  if (!pl || !hist || !nhist) return fail(SAXS_E_INVALID, "null argument");
+  const DevArgs &a = pl->a;
+  const size_t nb = static_cast<size_t>(a.num_bins);
+  if (pl->ensemble == SAXS_NVT) {
+    double *th = pl->d_tmp_hist, *tn = pl->d_tmp_hist + nb;
+    CUDA_TRY(cudaMemsetAsync(th, 0, 2 * nb * sizeof(double), st));
+    if (pl->frames > 0) {
+      const float fact = static_cast<float>(1.0 / static_cast<float>(pl->frames));
+      dim3 gh(a.nkz, 1);
+      k_hist<double><<<gh, kThreads, pl->smem_hist, st>>>(a, a.iacc, pl->d_geom0, kGeom,
+                                                          static_cast<double>(fact), th, tn);
+      if (int rc = launch_check("k_hist(nvt)")) return rc;
+    }
+    CUDA_TRY(cudaMemcpyAsync(hist, th, nb * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaMemcpyAsync(nhist, tn, nb * sizeof(double), cudaMemcpyDeviceToHost, st));
+  } else {
+    CUDA_TRY(cudaMemcpyAsync(hist, a.hist, nb * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaMemcpyAsync(nhist, a.nhist, nb * sizeof(double), cudaMemcpyDeviceToHost, st));
+  }
+  CUDA_TRY(cudaStreamSynchronize(st));
+  return SAXS_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+int saxs_plan_create(const SaxsParams *params, SaxsPlan **plan) {
+  g_err.clear();
+  return create(params, plan);
+}
+
+void saxs_plan_destroy(SaxsPlan *plan) { destroy(plan); }
+
+int saxs_plan_info(const SaxsPlan *pl, SaxsPlanInfo *info) {
+  if (!pl || !info) return fail(SAXS_E_INVALID, "null argument");
+  const DevArgs &a = pl->a;
+  for (int d = 0; d < 3; ++d) {
+    info->grid[d] = a.n[d];
+    info->scaled_grid[d] = a.nn[d];
+  }
+  info->bin_size = a.dq;
+  info->qcut = a.qcut;
+  info->num_bins = a.num_bins;
+  info->kbox[0] = a.nkx;
+  info->kbox[1] = a.nky;
+  info->kbox[2] = a.nkz;
+  info->kz_count = a.nkz;
+  info->path = 0;
+  info->device_bytes = pl->bytes;
+  info->frames_accumulated = pl->frames;
+  return SAXS_OK;
+}
+
+int saxs_forward(SaxsPlan *plan, const float *xyz_dev, int64_t frame_stride, int nframes,
+                 const float *boxes_host, void *stream) {
+  g_err.clear();
+  int prev = 0;
+  cudaGetDevice(&prev);
+  if (plan && prev != plan->device) cudaSetDevice(plan->device);
+  const int rc = forward(plan, xyz_dev, frame_stride, nframes, boxes_host,
+                         static_cast<cudaStream_t>(stream));
+  if (plan && prev != plan->device) cudaSetDevice(prev);
+  return rc;
+}
+
+int saxs_histogram(SaxsPlan *plan, double *hist_host, double *nhist_host, void *stream) {
+  g_err.clear();
+  return histogram(plan, hist_host, nhist_host, static_cast<cudaStream_t>(stream));
+}
+
+int saxs_reset(SaxsPlan *pl, void *stream) {
+  if (!pl) return fail(SAXS_E_INVALID, "null plan");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const DevArgs &a = pl->a;
+  CUDA_TRY(cudaMemsetAsync(a.hist, 0, sizeof(double) * a.num_bins, st));
+  CUDA_TRY(cudaMemsetAsync(a.nhist, 0, sizeof(double) * a.num_bins, st));
+  if (a.iacc) CUDA_TRY(cudaMemsetAsync(a.iacc, 0, sizeof(double) * a.nkz * a.nky * a.nkx, st));
+  pl->frames = 0;
+  return SAXS_OK;
+}
+
+int saxs_debug_kbox_intensity(SaxsPlan *pl, float *out, void *stream) {
+  if (!pl || !out) return fail(SAXS_E_INVALID, "null argument");
+  if (pl->last_frame_batch < 1) return fail(SAXS_E_INVALID, "no frame processed yet");
+  const DevArgs &a = pl->a;
+  const size_t npl = static_cast<size_t>(a.nkz) * a.nky * a.nkx;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  CUDA_TRY(cudaMemcpyAsync(out, a.ibox + (pl->last_frame_batch - 1) * npl, npl * sizeof(float),
+                           cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  return SAXS_OK;
+}
+
+int saxs_debug_border_sums(SaxsPlan *pl, double *out, void *stream) {
+  if (!pl || !out) return fail(SAXS_E_INVALID, "null argument");
+  if (pl->last_frame_batch < 1) return fail(SAXS_E_INVALID, "no frame processed yet");
+  const DevArgs &a = pl->a;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  CUDA_TRY(cudaMemcpyAsync(out, a.border + static_cast<size_t>(pl->last_frame_batch - 1) * a.T,
+                           a.T * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  return SAXS_OK;
+}
+
+int saxs_backward(SaxsPlan *, const float *, const float *, const double *, float *, void *) {
+  return fail(SAXS_E_INVALID, "saxs_backward: not available in this build");
+}
+
+int saxs_profile_stages(void) { return kStages; }
+
+const char *saxs_profile_stage_name(int i) {
+  return (i >= 0 && i < kStages) ? kStageNames[i] : "";
+}
+
+int saxs_profile_enable(SaxsPlan *pl, int enable) {
+  if (!pl) return fail(SAXS_E_INVALID, "null plan");
+  pl->profiling = enable != 0;
+  return SAXS_OK;
+}
+
+int saxs_profile_read(SaxsPlan *pl, double *ms_out, int *launches_out) {
+  if (!pl || !ms_out) return fail(SAXS_E_INVALID, "null argument");
+  for (auto &r : pl->prof_pending) {
+    for (int k = 0; k < kStages; ++k) {
+      if (!r.used[k]) continue;
+      CUDA_TRY(cudaEventSynchronize(r.stop[k]));
+      float ms = 0.f;
+      CUDA_TRY(cudaEventElapsedTime(&ms, r.start[k], r.stop[k]));
+      ms_out[k] += ms;
+      if (launches_out) launches_out[k] += 1;
+      pl->event_pool.push_back(r.start[k]);
+      pl->event_pool.push_back(r.stop[k]);
+      r.start[k] = r.stop[k] = nullptr;
+    }
+  }
+  pl->prof_pending.clear();
+  return SAXS_OK;
+}
+
+int64_t saxs_closest_product(int n, float sigma) { return saxs::closest_product(n, sigma); }
+
+int saxs_cell_oc(const float box[9], float oc_out[9]) {
+  if (!box || !oc_out) return fail(SAXS_E_INVALID, "null argument");
+  saxs::cell_oc(box, oc_out);
+  return SAXS_OK;
+}
+
+int saxs_histogram_parameters(const int nn[3], const float oc[9], float sigma, float bin_size,
+                              float qcut, float *bin_out, float *qcut_out, int *num_bins_out) {
+  if (!nn || !oc || !bin_out || !qcut_out || !num_bins_out) return fail(SAXS_E_INVALID, "null argument");
+  saxs::histogram_parameters(nn, oc, sigma, bin_size, qcut, bin_out, qcut_out, num_bins_out);
+  return SAXS_OK;
+}
+
+int saxs_bspline_moduli(int n, int ndim, float *out) {
+  if (n < 1 || !out) return fail(SAXS_E_INVALID, "bad argument");
+  saxs::bspline_moduli(n, ndim, out);
+  return SAXS_OK;
+}
+
+const char *saxs_last_error(void) { return g_err.c_str(); }
+
+const char *saxs_version(void) { return "pycusaxs_b200 0.1 (sm_100a)"; }
+
+}  // extern "C"

@@ -1,0 +1,293 @@
+"""Python host layer over the C ABI: one SAXS run on one CUDA device.
+
+``SaxsEngine`` owns a native plan (grid sizing, tables, device buffers) and a
+CUDA stream.  Frames are pushed either from device memory (``forward``) or
+from host memory (``forward_host``: pinned staging, double-buffered H2D on a
+copy stream overlapping the previous frames' kernels).  ``profile()`` returns
+the I(q) rows the reference writes (saxsKernel.cu:210-225).
+
+PyTorch is used only as plumbing: device/pinned allocations and streams.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _native
+from .formfactors import form_factor_rows
+
+ENSEMBLES = {"npt": _native.SAXS_NPT, "nvt": _native.SAXS_NVT}
+
+
+def _torch():
+    import torch
+
+    if not torch.cuda.is_available():
+        raise RuntimeError("pycusaxs_b200 needs a CUDA device (no CPU fallback)")
+    return torch
+
+
+@dataclass
+class PlanInfo:
+    grid: tuple
+    scaled_grid: tuple
+    bin_size: float
+    qcut: float
+    num_bins: int
+    kbox: tuple
+    device_bytes: int
+    frames: int
+
+
+def entries_from_index(atom_index: dict, natoms: int | None = None):
+    """(type names, entry_atom, entry_type) from an element -> indices mapping.
+
+    Types are ordered like the keys of the reference's std::map (byte-wise
+    sorted, RunSaxs.cu:108-115), which fixes the order of the type sum.
+    """
+    names = sorted(atom_index.keys(), key=lambda s: s.encode())
+    atoms, types = [], []
+    for t, name in enumerate(names):
+        idx = np.asarray(list(atom_index[name]), dtype=np.int64).reshape(-1)
+        if idx.size and (idx.min() < 0 or (natoms is not None and idx.max() >= natoms)):
+            raise ValueError(f"atom index out of range for element {name!r}")
+        atoms.append(idx)
+        types.append(np.full(idx.size, t, dtype=np.int32))
+    ea = np.concatenate(atoms).astype(np.int32) if atoms else np.zeros(0, np.int32)
+    et = np.concatenate(types) if types else np.zeros(0, np.int32)
+    return names, ea, et
+
+
+class SaxsEngine:
+    """A SAXS run (npt or nvt) over frames of one topology."""
+
+    def __init__(self, grid, atom_index: dict, natoms: int, box0, *, scaled_grid=(0, 0, 0),
+                 order: int = 4, scale_factor: float = 1.0, bin_size: float = 0.0,
+                 qcut: float = 0.0, ensemble: str = "npt", max_frames: int = 1,
+                 box_margin: float = 0.05, device=None, form_factors: dict | None = None):
+        torch = _torch()
+        self._torch = torch
+        self.lib = _native.load()
+        if device is None:
+            device = torch.device("cuda", torch.cuda.current_device())
+        self.device = torch.device(device)
+        grid = tuple(int(v) for v in (grid if len(grid) == 3 else [grid[0]] * 3))
+        sg = tuple(int(v) for v in scaled_grid) if scaled_grid else (0, 0, 0)
+        if len(sg) == 1:
+            sg = sg * 3
+        self.type_names, ea, et = entries_from_index(atom_index, natoms)
+        ff = form_factor_rows(self.type_names, form_factors)
+        self._ff = np.ascontiguousarray(ff, dtype=np.float32)
+        self._ea = np.ascontiguousarray(ea, dtype=np.int32)
+        self._et = np.ascontiguousarray(et, dtype=np.int32)
+        self.natoms = int(natoms)
+        self.max_frames = int(max_frames)
+        p = _native.SaxsParams()
+        p.grid[:] = grid
+        p.scaled_grid[:] = sg
+        p.order = int(order)
+        p.scale_factor = float(scale_factor)
+        p.bin_size = float(bin_size)
+        p.qcut = float(qcut)
+        if ensemble not in ENSEMBLES:
+            raise ValueError(f"unknown ensemble {ensemble!r}")
+        self.ensemble = ensemble
+        p.ensemble = ENSEMBLES[ensemble]
+        p.ntypes = len(self.type_names)
+        p.form_factors = self._ff.ctypes.data_as(_native.c_float_p)
+        p.natoms = self.natoms
+        p.nentries = int(self._ea.size)
+        p.entry_atom = self._ea.ctypes.data_as(_native.c_int32_p)
+        p.entry_type = self._et.ctypes.data_as(_native.c_int32_p)
+        p.box0[:] = [float(v) for v in np.asarray(box0, dtype=np.float32).reshape(9)]
+        p.max_frames = self.max_frames
+        p.box_margin = float(box_margin)
+        self._params = p
+        plan = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            _native.check(self.lib.saxs_plan_create(ctypes.byref(p), ctypes.byref(plan)))
+        self._plan = plan
+        self.stream = torch.cuda.Stream(device=self.device)
+        self._copy_stream = torch.cuda.Stream(device=self.device)
+        self._staging = None
+        self.info = self._info()
+
+    # -- plan information -------------------------------------------------
+    def _info(self) -> PlanInfo:
+        i = _native.SaxsPlanInfo()
+        _native.check(self.lib.saxs_plan_info(self._plan, ctypes.byref(i)))
+        return PlanInfo(tuple(i.grid), tuple(i.scaled_grid), float(i.bin_size), float(i.qcut),
+                        int(i.num_bins), tuple(i.kbox), int(i.device_bytes),
+                        int(i.frames_accumulated))
+
+    @property
+    def frames(self) -> int:
+        return self._info().frames
+
+    # -- frames -----------------------------------------------------------
+    def forward(self, xyz, boxes) -> None:
+        """Process frames already on the device.
+
+        ``xyz``: CUDA float32 tensor (B, natoms, 3) or (natoms, 3), contiguous
+        per frame; ``boxes``: (B, 3, 3) or (3, 3) array on the host.
+        """
+        torch = self._torch
+        if xyz.dim() == 2:
+            xyz = xyz.unsqueeze(0)
+        if xyz.dtype != torch.float32 or xyz.device != self.device:
+            raise ValueError("xyz must be a float32 tensor on the plan's device")
+        if xyz.shape[1] < self.natoms or xyz.shape[2] != 3 or xyz.stride(2) != 1 or xyz.stride(1) != 3:
+            raise ValueError("xyz must have shape (B, natoms, 3) with contiguous rows")
+        b = np.ascontiguousarray(np.asarray(boxes, dtype=np.float32).reshape(-1, 9))
+        nf = xyz.shape[0]
+        if b.shape[0] != nf:
+            raise ValueError("one box per frame is required")
+        for s in range(0, nf, self.max_frames):
+            e = min(nf, s + self.max_frames)
+            _native.check(self.lib.saxs_forward(
+                self._plan, ctypes.c_void_p(xyz[s].data_ptr()), ctypes.c_int64(xyz.stride(0)),
+                e - s, b[s:e].ctypes.data_as(_native.c_float_p),
+                ctypes.c_void_p(self.stream.cuda_stream)))
+
+    def forward_host(self, xyz, boxes) -> None:
+        """Process frames held in host memory (numpy, (B, natoms, 3) or (natoms, 3)).
+
+        Frames go through a pinned staging buffer and are copied to the device
+        on a copy stream, double-buffered against the compute stream.
+        """
+        torch = self._torch
+        x = np.asarray(xyz, dtype=np.float32)
+        if x.ndim == 2:
+            x = x[None]
+        b = np.asarray(boxes, dtype=np.float32).reshape(-1, 9)
+        nf = x.shape[0]
+        if b.shape[0] != nf:
+            raise ValueError("one box per frame is required")
+        if x.shape[1] < self.natoms or x.shape[2] != 3:
+            raise ValueError("positions must have shape (B, natoms, 3)")
+        st = self._staging_buffers(x.shape[1])
+        B = self.max_frames
+        for s in range(0, nf, B):
+            e = min(nf, s + B)
+            slot = st["next"]
+            st["next"] ^= 1
+            host, dev = st["host"][slot], st["dev"][slot]
+            st["copied"][slot].synchronize()              # staging slot free again
+            np.copyto(host.numpy()[: e - s], x[s:e])
+            with torch.cuda.stream(self._copy_stream):
+                self._copy_stream.wait_event(st["used"][slot])  # device slot free again
+                dev[: e - s].copy_(host[: e - s], non_blocking=True)
+                st["copied"][slot].record(self._copy_stream)
+            self.stream.wait_event(st["copied"][slot])
+            _native.check(self.lib.saxs_forward(
+                self._plan, ctypes.c_void_p(dev.data_ptr()), ctypes.c_int64(dev.stride(0)),
+                e - s, np.ascontiguousarray(b[s:e]).ctypes.data_as(_native.c_float_p),
+                ctypes.c_void_p(self.stream.cuda_stream)))
+            st["used"][slot].record(self.stream)
+
+    def _staging_buffers(self, rows: int):
+        torch = self._torch
+        if self._staging is None or self._staging["rows"] != rows:
+            if self._staging is not None:  # buffers may still be in use by queued work
+                self._copy_stream.synchronize()
+                self.stream.synchronize()
+            shape = (self.max_frames, rows, 3)
+            self._staging = {
+                "rows": rows,
+                "host": [torch.empty(shape, dtype=torch.float32, pin_memory=True) for _ in range(2)],
+                "dev": [torch.empty(shape, dtype=torch.float32, device=self.device) for _ in range(2)],
+                "copied": [torch.cuda.Event() for _ in range(2)],
+                "used": [torch.cuda.Event() for _ in range(2)],
+                "next": 0,
+            }
+            for ev in self._staging["copied"] + self._staging["used"]:
+                ev.record(self.stream)
+        return self._staging
+
+    # -- results ----------------------------------------------------------
+    def histogram(self):
+        """FP64 (hist, nhist) accumulated so far (waits for the device)."""
+        nb = self.info.num_bins
+        h = np.zeros(nb, dtype=np.float64)
+        n = np.zeros(nb, dtype=np.float64)
+        _native.check(self.lib.saxs_histogram(self._plan, h.ctypes.data_as(_native.c_double_p),
+                                              n.ctypes.data_as(_native.c_double_p),
+                                              ctypes.c_void_p(self.stream.cuda_stream)))
+        return h, n
+
+    def profile(self):
+        """I(q) rows (q, I) for bins o >= 1 with nhist != 0 (saxsKernel.cu:210-225)."""
+        h, n = self.histogram()
+        return profile_rows(h, n, self.info.bin_size)
+
+    def kbox_intensity(self) -> np.ndarray:
+        """Intensities of the last frame over the k-box, shape (nkz, nky, nkx)."""
+        nkx, nky, nkz = self.info.kbox
+        out = np.zeros(nkz * nky * nkx, dtype=np.float32)
+        _native.check(self.lib.saxs_debug_kbox_intensity(
+            self._plan, out.ctypes.data_as(_native.c_float_p),
+            ctypes.c_void_p(self.stream.cuda_stream)))
+        return out.reshape(nkz, nky, nkx)
+
+    def border_sums(self) -> np.ndarray:
+        out = np.zeros(len(self.type_names), dtype=np.float64)
+        _native.check(self.lib.saxs_debug_border_sums(
+            self._plan, out.ctypes.data_as(_native.c_double_p),
+            ctypes.c_void_p(self.stream.cuda_stream)))
+        return out
+
+    def profile_enable(self, on: bool = True) -> None:
+        """Time every kernel of ``forward`` with CUDA events on the engine stream."""
+        _native.check(self.lib.saxs_profile_enable(self._plan, int(bool(on))))
+
+    def profile_read(self) -> dict:
+        """{stage: (milliseconds, launches)} since the last read (waits for the device)."""
+        n = self.lib.saxs_profile_stages()
+        ms = np.zeros(n, dtype=np.float64)
+        cnt = np.zeros(n, dtype=np.int32)
+        _native.check(self.lib.saxs_profile_read(self._plan, ms.ctypes.data_as(_native.c_double_p),
+                                                 cnt.ctypes.data_as(_native.c_int_p)))
+        return {self.lib.saxs_profile_stage_name(i).decode(): (float(ms[i]), int(cnt[i]))
+                for i in range(n)}
+
+    def reset(self) -> None:
+        _native.check(self.lib.saxs_reset(self._plan, ctypes.c_void_p(self.stream.cuda_stream)))
+
+    def synchronize(self) -> None:
+        self.stream.synchronize()
+
+    def close(self) -> None:
+        if getattr(self, "_plan", None):
+            self.stream.synchronize()
+            self._copy_stream.synchronize()
+            self.lib.saxs_plan_destroy(self._plan)
+            self._plan = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def profile_rows(hist, nhist, bin_size):
+    """(q, I) rows: q = o*bin_size in float32, I = hist/nhist (saxsKernel.cu:210-225)."""
+    rows = []
+    b = np.float32(bin_size)
+    for o in range(1, len(hist)):
+        if nhist[o] != 0.0:
+            rows.append((float(np.float32(o) * b), float(hist[o] / nhist[o])))
+    return rows
+
+
+def format_profile(rows) -> str:
+    """Text of the profile file (RunSaxs.cu:224-228: setw(10) fixed 5, setw(12) scientific 5)."""
+    return "".join(f"{q:10.5f}{i:12.5e}\n" for q, i in rows)
