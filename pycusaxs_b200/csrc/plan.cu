@@ -57,7 +57,6 @@ constexpr int kYChunk = 32;               // y values staged per step in k_ydft
 constexpr int kYRows = 64;                // x rows per CTA in k_ydft
 constexpr int kYStride = kYRows + 2;      // padded shared row (float2), 16-byte aligned
 constexpr int kXRows = 4;                 // ky rows per CTA in k_xdft_post
-constexpr int kMaxSmem = 227 * 1024;
 constexpr int kHistSmemBins = 2048;       // bins held in shared memory by k_hist
 
 thread_local std::string g_err;
@@ -705,6 +704,32 @@ struct SaxsPlan {
 
 namespace {
 
+int optin_smem() {
+  int dev = 0, v = 0;
+  cudaGetDevice(&dev);
+  if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) {
+    cudaGetLastError();
+    return 48 * 1024;
+  }
+  return v;
+}
+
+template <typename K>
+size_t static_smem(K kernel) {
+  cudaFuncAttributes fa{};
+  if (cudaFuncGetAttributes(&fa, kernel) != cudaSuccess) {
+    cudaGetLastError();
+    return 1024;
+  }
+  return fa.sharedSizeBytes;
+}
+
+template <typename K>
+cudaError_t raise_smem_limit(K kernel) {
+  const int lim = optin_smem() - static_cast<int>(static_smem(kernel));
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+}
+
 template <typename T>
 int dalloc(SaxsPlan *pl, T **ptr, size_t count) {
   const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
@@ -878,8 +903,11 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
   pl->smem_hist = (a.num_bins <= kHistSmemBins ? 2 * sizeof(double) * a.num_bins : 0) +
                   plane * sizeof(double);
   pl->smem_bin = static_cast<size_t>(kThreads / 32) * a.T * sizeof(double);
-  if (pl->smem_spread > static_cast<size_t>(kMaxSmem) || pl->smem_xdft > static_cast<size_t>(kMaxSmem) ||
-      pl->smem_hist > static_cast<size_t>(kMaxSmem) || pl->smem_bin > 48 * 1024) {
+  const size_t optin = static_cast<size_t>(optin_smem());
+  if (pl->smem_spread + static_smem(k_spread_zdft) > optin ||
+      pl->smem_ydft + static_smem(k_ydft) > optin ||
+      pl->smem_xdft + static_smem(k_xdft_post) > optin ||
+      pl->smem_hist + static_smem(k_hist<double>) > optin || pl->smem_bin > 40 * 1024) {
     destroy(pl);
     return fail(SAXS_E_INVALID,
                 "grid / q-cut combination exceeds the shared-memory budget of the pruned path (z "
@@ -991,12 +1019,13 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
   for (int i = 0; e == cudaSuccess && i < kRing; ++i)
     e = cudaEventCreateWithFlags(&pl->ring.ev[i], cudaEventDisableTiming);
   // The dynamic shared-memory limit is per kernel function, not per plan, so
-  // it is raised to the device maximum once for every plan alike.
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_spread_zdft, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ydft, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_xdft_post, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_hist<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_hist<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
+  // it is raised once to the largest value each kernel allows (the opt-in
+  // per-block limit minus the kernel's static shared memory).
+  if (e == cudaSuccess) e = raise_smem_limit(k_spread_zdft);
+  if (e == cudaSuccess) e = raise_smem_limit(k_ydft);
+  if (e == cudaSuccess) e = raise_smem_limit(k_xdft_post);
+  if (e == cudaSuccess) e = raise_smem_limit(k_hist<float>);
+  if (e == cudaSuccess) e = raise_smem_limit(k_hist<double>);
   if (e != cudaSuccess) {
     destroy(pl);
     return fail(SAXS_E_CUDA, std::string("plan setup: ") + cudaGetErrorString(e));

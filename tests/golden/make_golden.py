@@ -21,6 +21,7 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 REPO = HERE.parents[1]
+sys.path.insert(0, str(REPO))
 
 CASES = {
     "cubic32_npt2": dict(kind="cubic", natoms=4000, box=40.0, seed=31, jitter=0.4, frames=2,
@@ -41,7 +42,6 @@ CASES = {
 
 
 def build_system(c):
-    sys.path.insert(0, str(REPO))
     from pycusaxs_b200 import synthetic as S
 
     if c["kind"] == "cubic":

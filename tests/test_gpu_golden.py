@@ -1,0 +1,33 @@
+"""The drop-in run() against the reference's own output files (GPU).
+
+Same seeded inputs as tests/golden/make_golden.py fed to the reference
+cudaSAXS; the profile files must agree row by row: identical q text and
+intensities within GOLDEN_RTOL (the reference's FP32 noise and 6 printed
+significant digits on both sides).
+"""
+import numpy as np
+import pytest
+
+from golden.make_golden import CASES, build_system
+from test_golden import GOLDEN_RTOL, golden
+from pycusaxs_b200 import pycusaxs_cuda
+from pycusaxs_b200.synthetic import SyntheticTopology
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_dropin_file_matches_reference_file(cuda, tmp_path, name):
+    c = CASES[name]
+    out = tmp_path / f"{name}.dat"
+    pycusaxs_cuda.run(SyntheticTopology(build_system(c)), "synthetic.tpr", "synthetic.xtc",
+                      c["grid"], scaled_grid=c.get("scaled", []), begin=0, end=c["frames"] - 1,
+                      stride=1, output=str(out), order=c.get("order", 4), scale_factor=c["sigma"],
+                      bin_size=c["bin_size"], qcut=c["qcut"], simulation=c.get("simulation", ""))
+    got = [(line[:10], float(line[10:])) for line in open(out)]
+    ref = golden()[name]["rows"]
+    assert [g[0] for g in got] == [r[0] for r in ref]
+    gi = np.array([g[1] for g in got])
+    ri = np.array([float(r[1]) for r in ref])
+    err = np.abs(gi - ri) / np.abs(ri)
+    assert err.max() <= GOLDEN_RTOL, err
