@@ -239,12 +239,12 @@ def bench_ours(args):
     host = torch.from_numpy(frames).pin_memory()
     eng.reset()
     for _ in range(max(1, args.warmup)):
-        eng.forward_host(host.numpy(), boxes)
+        eng.forward_host(host, boxes)
         eng.histogram()
     barrier(dist)
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        eng.forward_host(host.numpy(), boxes)
+        eng.forward_host(host, boxes)
         h, n = eng.histogram()
     e2e_s = max_over_ranks(time.perf_counter() - t0, dist)
     e2e = {"value": round(world * FRAMES * args.steps / e2e_s, 1), "unit": "frames/s",

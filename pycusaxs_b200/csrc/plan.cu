@@ -49,8 +49,7 @@ constexpr int kCols = kTile * kTile;      // columns per tile
 constexpr int kThreads = 256;
 constexpr int kGeom = 24;                 // floats of per-frame geometry: oc[9], ocs[9]
 constexpr int kRing = 4;                  // pinned geometry slots in flight
-constexpr int kKzGroup = 10;              // kz outputs per warp in k_spread_zdft
-constexpr int kKzPass = 2 * kKzGroup;     // kz outputs per pass (two warp groups)
+constexpr int kKzThread = 6;              // kz outputs (complex) per thread in k_spread_zdft
 constexpr int kKyGroup = 10;              // ky outputs per warp in k_ydft
 constexpr int kKyPass = 8 * kKyGroup;     // ky outputs per pass (eight warps)
 constexpr int kYChunk = 32;               // y values staged per step in k_ydft
@@ -93,11 +92,14 @@ struct DevArgs {
   const int32_t *entry_atom;
   const int32_t *entry_type;
   const float *geom;
-  const float2 *twz;  // [ez][nkzp]
+  const float2 *twz;  // [ez][nkzp], nkzp a multiple of kKzThread
   const float2 *twy;  // [ey][nkyp]
   const float2 *twx;  // [ex][nkxp]
   const float *modx, *mody, *modz;
   const float *ff;    // [T][9]
+  const float *twz_sum; // [2*nkzp]: sum over z < ez of the z twiddles (re, im)
+  const int4 *home_x; // per spread tile along x: home tiles whose atoms reach it (-1 padded)
+  const int4 *home_y;
   int2 *key;
   int *counts;
   int *offsets;
@@ -280,56 +282,48 @@ __global__ void __launch_bounds__(kThreads) k_scatter_atoms(DevArgs a) {
   a.rec[static_cast<int64_t>(f) * a.M + pos] = make_float4(r0, r1, r2, __int_as_float(e));
 }
 
-// Distinct home tiles whose atoms can reach columns [c0, c0+cw) along an axis
-// of length n with `order`-tap stencils starting at the home position.
-__device__ __forceinline__ int home_tiles(int c0, int cw, int order, int n, int *out) {
-  int cnt = 0;
-  for (int d = 0; d < cw + order - 1; ++d) {
-    int x = (c0 - order + 1 + d) % n;
-    if (x < 0) x += n;
-    const int h = x / kTile;
-    bool seen = false;
-    for (int k = 0; k < cnt; ++k) seen |= (out[k] == h);
-    if (!seen && cnt < 4) out[cnt++] = h;
+// The atoms of up to 16 home bins of one tile, as one flat range: bin j holds
+// records [start[j], start[j] + cum[j+1] - cum[j]).  Filled by threads 0..15.
+struct TileAtoms {
+  int start[16];
+  int cum[17];
+  int nb;
+};
+
+__device__ __forceinline__ void tile_atom_ranges(const DevArgs &a, TileAtoms &ta, int f, int t,
+                                                 int x0, int y0) {
+  if (threadIdx.x == 0) {
+    const int4 hxv = a.home_x[x0 / kTile], hyv = a.home_y[y0 / kTile];
+    const int hx[4] = {hxv.x, hxv.y, hxv.z, hxv.w}, hy[4] = {hyv.x, hyv.y, hyv.z, hyv.w};
+    const int *off = a.offsets + static_cast<int64_t>(f) * (a.nbins + 1);
+    int nb = 0;
+    ta.cum[0] = 0;
+    for (int ix = 0; ix < 4; ++ix) {
+      for (int iy = 0; iy < 4; ++iy) {
+        if (hx[ix] >= 0 && hy[iy] >= 0) {
+          const int bin = (t * a.tiles[1] + hy[iy]) * a.tiles[0] + hx[ix];
+          const int s0 = off[bin];
+          ta.start[nb] = s0;
+          ta.cum[nb + 1] = ta.cum[nb] + (off[bin + 1] - s0);
+          ++nb;
+        }
+      }
+    }
+    ta.nb = nb;
   }
-  return cnt;
 }
 
-// grid (stiles_x*stiles_y, T, frames), block 256.
-// Dynamic shared memory: tile nz*64 floats | twiddles ez*nkzp float2 | reduction 20*64 float2.
-__global__ void __launch_bounds__(kThreads) k_spread_zdft(DevArgs a) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  const int nz = a.n[2], ez = a.ext[2];
-  float *tile = reinterpret_cast<float *>(smem);
-  float2 *tws = reinterpret_cast<float2 *>(tile + static_cast<size_t>(nz) * kCols);
-  float2 *red = tws + static_cast<size_t>(ez) * a.nkzp;
-  const int f = blockIdx.z, t = blockIdx.y;
-  const int TX = blockIdx.x % a.stiles[0], TY = blockIdx.x / a.stiles[0];
-  const int x0 = TX * kTile, y0 = TY * kTile;
-  const int cw = min(kTile, a.ext[0] - x0), ch = min(kTile, a.ext[1] - y0);
-  const int tid = threadIdx.x;
-
-  for (int i = tid; i < nz * kCols; i += blockDim.x) tile[i] = 0.0f;
-  {
-    const float4 *src = reinterpret_cast<const float4 *>(a.twz);
-    float4 *dst = reinterpret_cast<float4 *>(tws);
-    const int n4 = ez * a.nkzp / 2;
-    for (int i = tid; i < n4; i += blockDim.x) dst[i] = src[i];
-  }
-  int hx[4], hy[4];
-  const int nhx = home_tiles(x0, cw, a.order, a.n[0], hx);
-  const int nhy = home_tiles(y0, ch, a.order, a.n[1], hy);
-  __syncthreads();
-
-  // --- spreading into the shared column tile ---
-  const int *off = a.offsets + static_cast<int64_t>(f) * (a.nbins + 1);
+// Spreading of one column tile into shared memory (float atomics on the tile).
+__device__ __forceinline__ void spread_tile(const DevArgs &a, const TileAtoms &ta, float *tile,
+                                            int f, int x0, int y0, int cw, int ch) {
   const float4 *rec = a.rec + static_cast<int64_t>(f) * a.M;
-  const int P = a.order, nt = a.ntaps;
-  for (int ix = 0; ix < nhx; ++ix) {
-    for (int iy = 0; iy < nhy; ++iy) {
-      const int bin = (t * a.tiles[1] + hy[iy]) * a.tiles[0] + hx[ix];
-      const int s = off[bin], e = off[bin + 1];
-      for (int i = s + tid; i < e; i += blockDim.x) {
+  const int P = a.order, nt = a.ntaps, nz = a.n[2];
+  const int total = ta.cum[ta.nb];
+  {
+    for (int k = threadIdx.x; k < total; k += blockDim.x) {
+      int j = 0;
+      while (k >= ta.cum[j + 1]) ++j;
+      const int i = ta.start[j] + (k - ta.cum[j]);
         const float4 q = rec[i];
         const int m0 = static_cast<int>(q.x), m1 = static_cast<int>(q.y),
                   m2 = static_cast<int>(q.z);
@@ -342,7 +336,7 @@ __global__ void __launch_bounds__(kThreads) k_spread_zdft(DevArgs a) {
         for (int o = 0; o < 4; ++o) {
           int z = m2 - P + o;
           if (z < 0) z += nz;
-          zs[o] = z;
+          zs[o] = z * kCols;
         }
 #pragma unroll
         for (int o = 0; o < 4; ++o) {
@@ -363,85 +357,122 @@ __global__ void __launch_bounds__(kThreads) k_spread_zdft(DevArgs a) {
 #pragma unroll
             for (int r = 0; r < 4; ++r) {
               if (r >= nt) break;
-              atomicAdd(col + zs[r] * kCols, wxy * wz[r]);
+              atomicAdd(col + zs[r], wxy * wz[r]);
             }
           }
         }
       }
     }
-  }
-  __syncthreads();
+}
 
-  // --- mean padding: the supercell is g on the corner block and the border
-  // mean elsewhere, i.e. (g - mean) on the corner plus a constant whose
-  // transform lives at k = 0 only ---
-  const float mean =
-      static_cast<float>(a.border[static_cast<int64_t>(f) * a.T + t] / a.border_count);
-  for (int i = tid; i < ez * kCols; i += blockDim.x) {
-    const int col = i % kCols;
-    if ((col / kTile) < cw && (col % kTile) < ch) tile[i] -= mean;
+// Persistent: grid = min(work items, resident CTAs); block 256.  A work item is
+// one (frame, type, 8x8 column tile).  Dynamic shared memory:
+//   twiddles  ez x NP floats   (NP = 2*nkzq; row z holds exp(-2 pi i kz z/nnz) as re,im)
+//   tile      max(nz*64, 64*NP) floats (z-major: 64 columns contiguous per z)
+// The z-axis DFT of the 64 columns is a small GEMM  out[c][n] = sum_z g[z][c] tw[z][n]
+// done with 4 columns x 6 kz (12 floats) per thread and the z range split
+// `ks` ways across the block, reduced deterministically in shared memory.
+__global__ void __launch_bounds__(kThreads, 2) k_spread_zdft(DevArgs a, int items) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int nz = a.n[2], ez = a.ext[2];
+  const int NP = 2 * a.nkzp;
+  float *tws = reinterpret_cast<float *>(smem);
+  float *tile = tws + static_cast<size_t>(ez) * NP;
+  const int tid = threadIdx.x;
+  {
+    const float4 *src = reinterpret_cast<const float4 *>(a.twz);
+    float4 *dst = reinterpret_cast<float4 *>(tws);
+    const int n4 = ez * NP / 4;
+    for (int i = tid; i < n4; i += blockDim.x) dst[i] = src[i];
   }
-  __syncthreads();
-
-  // --- z-axis DFT of the 64 columns restricted to kz in [0, nkz) ---
-  const int warp = tid >> 5, lane = tid & 31;
-  const int ngroups = (a.nkz + kKzGroup - 1) / kKzGroup;
-  const int gpp = ngroups >= 2 ? 2 : 1;
-  const int zsplit = (kThreads / 32) / gpp;
-  const int kg = warp % gpp, zsi = warp / gpp;
-  const int zlo = zsi * ez / zsplit, zhi = (zsi + 1) * ez / zsplit;
-  const float2 *tile2 = reinterpret_cast<const float2 *>(tile);
+  const int ngroups = a.nkzp / kKzThread;      // kz groups of kKzThread
+  const int tps = (kCols / 4) * ngroups;       // tasks per z split
+  const int ks = max(1, min(8, static_cast<int>(blockDim.x) / tps));
+  const int split = tid / tps, task = tid % tps;
+  const int cg = task % (kCols / 4), kg = task / (kCols / 4);
+  const bool worker = split < ks;
+  const int zlo = split * ez / ks, zhi = (split + 1) * ez / ks;
+  const int st = a.stiles[0] * a.stiles[1];
   const int ex = a.ext[0], ey = a.ext[1];
   const int64_t zplane = static_cast<int64_t>(ex) * ey;
-  float2 *Zft = a.Z + (static_cast<int64_t>(f) * a.T + t) * a.nkz * zplane;
-  for (int kpass = 0; kpass * gpp * kKzGroup < a.nkz; ++kpass) {
-    const int kbase = (kpass * gpp + kg) * kKzGroup;
-    float2 acc0[kKzGroup], acc1[kKzGroup];
+  const int tile_floats = max(nz * kCols, kCols * NP);
+
+  __shared__ TileAtoms ta;
+  for (int w = blockIdx.x; w < items; w += gridDim.x) {
+    const int f = w / (a.T * st);
+    const int t = (w / st) % a.T;
+    const int tl = w % st;
+    const int x0 = (tl % a.stiles[0]) * kTile, y0 = (tl / a.stiles[0]) * kTile;
+    const int cw = min(kTile, ex - x0), ch = min(kTile, ey - y0);
+    {
+      float4 *t4 = reinterpret_cast<float4 *>(tile);
+      for (int i = tid; i < tile_floats / 4; i += blockDim.x) t4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    tile_atom_ranges(a, ta, f, t, x0, y0);
+    __syncthreads();
+    spread_tile(a, ta, tile, f, x0, y0, cw, ch);
+    __syncthreads();
+    // mean padding: the supercell is g on the corner block and the border mean
+    // elsewhere = (g - mean) on the corner + a constant whose transform is k = 0
+    // only.  The column DFT of -mean over z < ez is -mean * sum_z tw[z][n].
+    const float mean =
+        static_cast<float>(a.border[static_cast<int64_t>(f) * a.T + t] / a.border_count);
+    float acc[4][2 * kKzThread];
 #pragma unroll
-    for (int j = 0; j < kKzGroup; ++j) acc0[j] = acc1[j] = make_float2(0.f, 0.f);
-    if (kbase < a.nkz) {
+    for (int c = 0; c < 4; ++c)
+#pragma unroll
+      for (int n = 0; n < 2 * kKzThread; ++n) acc[c][n] = 0.f;
+    if (worker) {
+      const float4 *g4 = reinterpret_cast<const float4 *>(tile) + cg;
+      const float *twr = tws + kg * 2 * kKzThread;
       for (int z = zlo; z < zhi; ++z) {
-        const float2 g = tile2[z * (kCols / 2) + lane];
-        const float4 *w4 = reinterpret_cast<const float4 *>(tws + static_cast<size_t>(z) * a.nkzp + kbase);
+        const float4 g = g4[z * (kCols / 4)];
+        const float4 *w4 = reinterpret_cast<const float4 *>(twr + z * NP);
+        const float4 w0 = w4[0], w1 = w4[1], w2 = w4[2];
+        const float wv[12] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w, w2.x, w2.y, w2.z, w2.w};
+        const float gv[4] = {g.x, g.y, g.z, g.w};
 #pragma unroll
-        for (int j = 0; j < kKzGroup / 2; ++j) {
-          const float4 w = w4[j];
-          acc0[2 * j].x = fmaf(g.x, w.x, acc0[2 * j].x);
-          acc0[2 * j].y = fmaf(g.x, w.y, acc0[2 * j].y);
-          acc1[2 * j].x = fmaf(g.y, w.x, acc1[2 * j].x);
-          acc1[2 * j].y = fmaf(g.y, w.y, acc1[2 * j].y);
-          acc0[2 * j + 1].x = fmaf(g.x, w.z, acc0[2 * j + 1].x);
-          acc0[2 * j + 1].y = fmaf(g.x, w.w, acc0[2 * j + 1].y);
-          acc1[2 * j + 1].x = fmaf(g.y, w.z, acc1[2 * j + 1].x);
-          acc1[2 * j + 1].y = fmaf(g.y, w.w, acc1[2 * j + 1].y);
+        for (int c = 0; c < 4; ++c)
+#pragma unroll
+          for (int n = 0; n < 12; ++n) acc[c][n] = fmaf(gv[c], wv[n], acc[c][n]);
+      }
+      if (split == 0) {
+#pragma unroll
+        for (int n = 0; n < 2 * kKzThread; ++n) {
+          const float d = a.twz_sum[kg * 2 * kKzThread + n];
+#pragma unroll
+          for (int c = 0; c < 4; ++c) acc[c][n] = fmaf(-mean, d, acc[c][n]);
         }
       }
     }
-    // reduce the z splits: red[kz_local][col]
-    const int kzl_n = gpp * kKzGroup;
-    for (int i = tid; i < kzl_n * kCols; i += blockDim.x) red[i] = make_float2(0.f, 0.f);
-    __syncthreads();
-    for (int s = 0; s < zsplit; ++s) {
-      if (zsi == s && kbase < a.nkz) {
+    __syncthreads();  // tile contents are dead: reuse the region as out[NP][64]
+    float *out = tile;
+    for (int r = 0; r < ks; ++r) {
+      if (worker && split == r) {
 #pragma unroll
-        for (int j = 0; j < kKzGroup; ++j) {
-          float4 *dst = reinterpret_cast<float4 *>(red + (kg * kKzGroup + j) * kCols + 2 * lane);
-          float4 v = *dst;
-          v.x += acc0[j].x;
-          v.y += acc0[j].y;
-          v.z += acc1[j].x;
-          v.w += acc1[j].y;
-          *dst = v;
+        for (int n = 0; n < 2 * kKzThread; ++n) {
+          float4 *o = reinterpret_cast<float4 *>(out + (kg * 2 * kKzThread + n) * kCols) + cg;
+          float4 v = make_float4(acc[0][n], acc[1][n], acc[2][n], acc[3][n]);
+          if (r > 0) {
+            const float4 u = *o;
+            v.x += u.x;
+            v.y += u.y;
+            v.z += u.z;
+            v.w += u.w;
+          }
+          *o = v;
         }
       }
       __syncthreads();
     }
-    for (int i = tid; i < kzl_n * kCols; i += blockDim.x) {
-      const int kzl = i / kCols, col = i % kCols;
-      const int kz = kpass * kzl_n + kzl;
+    float2 *Zft = a.Z + (static_cast<int64_t>(f) * a.T + t) * a.nkz * zplane;
+    for (int i = tid; i < a.nkz * kCols; i += blockDim.x) {
+      const int kz = i / kCols, col = i % kCols;
       const int lx = col / kTile, ly = col % kTile;
-      if (kz < a.nkz && lx < cw && ly < ch)
-        Zft[kz * zplane + static_cast<int64_t>(x0 + lx) * ey + (y0 + ly)] = red[i];
+      if (lx < cw && ly < ch) {
+        const float2 v = make_float2(out[(2 * kz) * kCols + col], out[(2 * kz + 1) * kCols + col]);
+        Zft[kz * zplane + static_cast<int64_t>(x0 + lx) * ey + (y0 + ly)] = v;
+      }
     }
     __syncthreads();
   }
@@ -697,6 +728,7 @@ struct SaxsPlan {
   Ring ring;
   float *d_geom0 = nullptr;
   double *d_tmp_hist = nullptr;
+  int spread_ctas = 1;  // resident CTAs of the persistent spreading kernel
   bool profiling = false;
   std::vector<StageRecord> prof_pending;
   std::vector<cudaEvent_t> event_pool;
@@ -745,6 +777,26 @@ int dalloc(SaxsPlan *pl, T **ptr, size_t count) {
   pl->allocations.push_back(*ptr);
   pl->bytes += bytes;
   return SAXS_OK;
+}
+
+// Distinct home tiles whose atoms can reach columns [c0, c0+cw) along an axis
+// of length n, for stencils of `order` taps that start at an atom's home column.
+std::vector<int4> home_tile_table(int ext, int n, int order) {
+  std::vector<int4> out;
+  for (int c0 = 0; c0 < ext; c0 += kTile) {
+    const int cw = std::min(kTile, ext - c0);
+    int h[4] = {-1, -1, -1, -1}, cnt = 0;
+    for (int d = 0; d < cw + order - 1; ++d) {
+      int x = (c0 - order + 1 + d) % n;
+      if (x < 0) x += n;
+      const int t = x / kTile;
+      bool seen = false;
+      for (int k = 0; k < cnt; ++k) seen |= (h[k] == t);
+      if (!seen && cnt < 4) h[cnt++] = t;
+    }
+    out.push_back(make_int4(h[0], h[1], h[2], h[3]));
+  }
+  return out;
 }
 
 void frame_geometry(const SaxsPlan *pl, const float box[9], float g[kGeom]) {
@@ -887,14 +939,14 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
     pl->half[2] = nn[2] / 2;
   }
   a.nkz = static_cast<int>(pl->half[2]) + 1;
-  a.nkzp = round_up(a.nkz, kKzPass);
+  a.nkzp = round_up(a.nkz, kKzThread);
   a.nkxp = round_up(a.nkx, 2);
   a.nkyp = round_up(a.nky, kKyGroup);
 
   // shared-memory budgets
-  pl->smem_spread = static_cast<size_t>(a.n[2]) * kCols * sizeof(float) +
-                    static_cast<size_t>(a.ext[2]) * a.nkzp * sizeof(float2) +
-                    static_cast<size_t>(kKzPass) * kCols * sizeof(float2);
+  pl->smem_spread = (static_cast<size_t>(a.ext[2]) * 2 * a.nkzp +
+                     std::max<size_t>(static_cast<size_t>(a.n[2]) * kCols,
+                                      static_cast<size_t>(kCols) * 2 * a.nkzp)) * sizeof(float);
   pl->smem_ydft = static_cast<size_t>(kYChunk) * kYStride * sizeof(float2) +
                   static_cast<size_t>(kYChunk) * a.nkyp * sizeof(float2);
   pl->smem_xdft = (static_cast<size_t>(a.ext[0]) * a.nkxp + static_cast<size_t>(a.T) * a.ext[0] +
@@ -942,6 +994,11 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
   ALLOC(d_mody, nn[1]);
   ALLOC(d_modz, nn[2]);
   ALLOC(d_ff, 9 * a.T);
+  int4 *d_hx = nullptr, *d_hy = nullptr;
+  float *d_twzs = nullptr;
+  ALLOC(d_twzs, 2 * a.nkzp);
+  ALLOC(d_hx, a.stiles[0]);
+  ALLOC(d_hy, a.stiles[1]);
   ALLOC(d_geom, static_cast<size_t>(B) * kGeom);
   ALLOC(pl->d_geom0, kGeom);
   ALLOC(d_status, 4);
@@ -967,6 +1024,9 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
   a.mody = d_mody;
   a.modz = d_modz;
   a.ff = d_ff;
+  a.twz_sum = d_twzs;
+  a.home_x = d_hx;
+  a.home_y = d_hy;
   a.geom = d_geom;
   a.status = d_status;
 
@@ -974,6 +1034,18 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
   std::vector<float2> twz(static_cast<size_t>(ez) * a.nkzp, make_float2(0.f, 0.f));
   for (int z = 0; z < ez; ++z)
     for (int k = 0; k < a.nkz; ++k) saxs::twiddle(k, z, nn[2], &twz[z * a.nkzp + k].x, &twz[z * a.nkzp + k].y);
+  std::vector<float> twzs(2 * a.nkzp, 0.0f);
+  for (int k = 0; k < a.nkz; ++k) {
+    double re = 0.0, im = 0.0;
+    for (int z = 0; z < ez; ++z) {
+      long long r = (static_cast<long long>(k) * z) % nn[2];
+      const double ang = -2.0 * M_PI * static_cast<double>(r) / nn[2];
+      re += std::cos(ang);
+      im += std::sin(ang);
+    }
+    twzs[2 * k] = static_cast<float>(re);
+    twzs[2 * k + 1] = static_cast<float>(im);
+  }
   std::vector<float2> twy(static_cast<size_t>(ey) * a.nkyp, make_float2(0.f, 0.f));
   for (int y = 0; y < ey; ++y)
     for (int k = 0; k < a.nky; ++k)
@@ -989,6 +1061,8 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
   saxs::bspline_moduli(nn[2], ndim, mz.data());
   float g0[kGeom];
   frame_geometry(pl, p.box0, g0);
+  const std::vector<int4> hxt = home_tile_table(ex, a.n[0], a.order);
+  const std::vector<int4> hyt = home_tile_table(ey, a.n[1], a.order);
 
   auto up = [&](void *dst, const void *src, size_t bytes) -> int {
     if (bytes == 0) return SAXS_OK;
@@ -1005,6 +1079,9 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
       (rc = up(d_mody, my.data(), sizeof(float) * nn[1])) ||
       (rc = up(d_modz, mz.data(), sizeof(float) * nn[2])) ||
       (rc = up(d_ff, pl->ff.data(), sizeof(float) * pl->ff.size())) ||
+      (rc = up(d_hx, hxt.data(), sizeof(int4) * hxt.size())) ||
+      (rc = up(d_twzs, twzs.data(), sizeof(float) * twzs.size())) ||
+      (rc = up(d_hy, hyt.data(), sizeof(int4) * hyt.size())) ||
       (rc = up(pl->d_geom0, g0, sizeof(g0)))) {
     destroy(pl);
     return rc;
@@ -1026,6 +1103,13 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
   if (e == cudaSuccess) e = raise_smem_limit(k_xdft_post);
   if (e == cudaSuccess) e = raise_smem_limit(k_hist<float>);
   if (e == cudaSuccess) e = raise_smem_limit(k_hist<double>);
+  if (e == cudaSuccess) {
+    int per_sm = 0, sms = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_spread_zdft, kThreads,
+                                                      pl->smem_spread);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, pl->device);
+    pl->spread_ctas = std::max(1, per_sm) * std::max(1, sms);
+  }
   if (e != cudaSuccess) {
     destroy(pl);
     return fail(SAXS_E_CUDA, std::string("plan setup: ") + cudaGetErrorString(e));
@@ -1125,9 +1209,10 @@ int forward(SaxsPlan *pl, const float *xyz, int64_t stride, int nframes, const f
     CUDA_TRY(cudaMemsetAsync(a.offsets, 0, sizeof(int) * nframes * (a.nbins + 1), st));
   }
   {
-    dim3 gs(a.stiles[0] * a.stiles[1], a.T, nframes);
+    const int items = a.stiles[0] * a.stiles[1] * a.T * nframes;
+    const int grid = std::max(1, std::min(items, pl->spread_ctas));
     tm.begin(kStSpread);
-    k_spread_zdft<<<gs, kThreads, pl->smem_spread, st>>>(a);
+    k_spread_zdft<<<grid, kThreads, pl->smem_spread, st>>>(a, items);
     tm.end(kStSpread);
     if (int rc = launch_check("k_spread_zdft")) return rc;
   }

@@ -152,15 +152,26 @@ class SaxsEngine:
                 ctypes.c_void_p(self.stream.cuda_stream)))
 
     def forward_host(self, xyz, boxes) -> None:
-        """Process frames held in host memory (numpy, (B, natoms, 3) or (natoms, 3)).
+        """Process frames held in host memory, (B, natoms, 3) or (natoms, 3).
 
-        Frames go through a pinned staging buffer and are copied to the device
-        on a copy stream, double-buffered against the compute stream.
+        ``xyz`` is a numpy array or a CPU torch tensor.  A pinned tensor is
+        copied straight to the device; anything else goes through a pinned
+        staging buffer first.  Host-to-device copies run on a copy stream,
+        double-buffered against the compute stream.
         """
         torch = self._torch
-        x = np.asarray(xyz, dtype=np.float32)
-        if x.ndim == 2:
-            x = x[None]
+        pinned = isinstance(xyz, torch.Tensor) and xyz.device.type == "cpu" and xyz.is_pinned()
+        if isinstance(xyz, torch.Tensor) and not pinned:
+            xyz = xyz.detach().cpu().numpy()
+        if pinned:
+            x = xyz if xyz.dtype == torch.float32 else xyz.float()
+            if x.dim() == 2:
+                x = x.unsqueeze(0)
+            x = x.contiguous()
+        else:
+            x = np.asarray(xyz, dtype=np.float32)
+            if x.ndim == 2:
+                x = x[None]
         b = np.asarray(boxes, dtype=np.float32).reshape(-1, 9)
         nf = x.shape[0]
         if b.shape[0] != nf:
@@ -173,12 +184,17 @@ class SaxsEngine:
             e = min(nf, s + B)
             slot = st["next"]
             st["next"] ^= 1
-            host, dev = st["host"][slot], st["dev"][slot]
-            st["copied"][slot].synchronize()              # staging slot free again
-            np.copyto(host.numpy()[: e - s], x[s:e])
+            dev = st["dev"][slot]
+            if pinned:
+                src = x[s:e]
+            else:
+                host = st["host"][slot]
+                st["copied"][slot].synchronize()              # staging slot free again
+                np.copyto(host.numpy()[: e - s], x[s:e])
+                src = host[: e - s]
             with torch.cuda.stream(self._copy_stream):
                 self._copy_stream.wait_event(st["used"][slot])  # device slot free again
-                dev[: e - s].copy_(host[: e - s], non_blocking=True)
+                dev[: e - s].copy_(src, non_blocking=True)
                 st["copied"][slot].record(self._copy_stream)
             self.stream.wait_event(st["copied"][slot])
             _native.check(self.lib.saxs_forward(
