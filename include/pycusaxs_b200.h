@@ -124,6 +124,25 @@ int saxs_debug_border_sums(SaxsPlan *plan, double *out_host, void *stream);
 int saxs_backward(SaxsPlan *plan, const float *xyz_dev, const float *box_host,
                   const double *dl_dprofile_host, float *grad_xyz_dev, void *stream);
 
+/* ---- allocation-free single frame (no counterpart in the reference) ----
+ *
+ * For hosts that cannot let the library allocate device memory while they run
+ * (an MD engine or application that owns all device memory through its own
+ * pool, or a per-step loop that must not stall on, or fail in, the allocator).
+ * Runs one frame of `plan` - positions xyz_dev (natoms x 3 float32, device),
+ * box box_host (3x3, host) - and writes that frame's histogram to hist_dev and
+ * nhist_dev (num_bins doubles each, device; overwritten).  The plan's own
+ * accumulators are left alone.  Every temporary comes from one fixed device
+ * array of SAXS_NOALLOC_SCRATCH_BYTES held by every GPU that loads the library
+ * until exit; plans needing more per frame get SAXS_E_RANGE.  Calls share that
+ * array, so calls that overlap on the GPU must be serialised by the caller.  The
+ * first call on a device looks the array up (cudaGetSymbolAddress) and should
+ * come before any stream capture.  Allocates nothing; the plan is created,
+ * with allocation, beforehand by saxs_plan_create. */
+#define SAXS_NOALLOC_SCRATCH_BYTES ((size_t)32 << 20)
+int saxs_forward_noalloc(SaxsPlan *plan, const float *xyz_dev, const float *box_host,
+                         double *hist_dev, double *nhist_dev, void *stream);
+
 /* ---- per-kernel timing (diagnostics; no reference counterpart: the reference
  * times only whole frames with one event pair, saxsKernel.cu:64-67,197-208) ---- */
 

@@ -17,6 +17,7 @@ SAXS_E_CUDA = -2
 SAXS_E_NOMEM = -3
 SAXS_E_RANGE = -4
 SAXS_E_DEVICE = -5
+SAXS_NOALLOC_SCRATCH_BYTES = 32 << 20
 SAXS_NPT = 0
 SAXS_NVT = 1
 
@@ -24,7 +25,7 @@ SAXS_NVT = 1
 EXPORTED = (
     "saxs_plan_create", "saxs_plan_destroy", "saxs_plan_info", "saxs_forward", "saxs_histogram",
     "saxs_reset", "saxs_debug_kbox_intensity", "saxs_debug_border_sums", "saxs_backward",
-    "saxs_profile_stages", "saxs_profile_stage_name", "saxs_profile_enable", "saxs_profile_read",
+    "saxs_forward_noalloc", "saxs_profile_stages", "saxs_profile_stage_name", "saxs_profile_enable", "saxs_profile_read",
     "saxs_closest_product", "saxs_cell_oc", "saxs_histogram_parameters", "saxs_bspline_moduli",
     "saxs_last_error", "saxs_version",
 )
@@ -112,6 +113,8 @@ def load(path: os.PathLike | str | None = None) -> ctypes.CDLL:
     lib.saxs_debug_border_sums.restype = ctypes.c_int
     lib.saxs_backward.argtypes = [vp, vp, c_float_p, c_double_p, vp, vp]
     lib.saxs_backward.restype = ctypes.c_int
+    lib.saxs_forward_noalloc.argtypes = [vp, vp, c_float_p, vp, vp, vp]
+    lib.saxs_forward_noalloc.restype = ctypes.c_int
     lib.saxs_profile_stages.argtypes = []
     lib.saxs_profile_stages.restype = ctypes.c_int
     lib.saxs_profile_stage_name.argtypes = [ctypes.c_int]

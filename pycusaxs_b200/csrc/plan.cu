@@ -40,6 +40,7 @@
 #include <vector>
 
 #include "pycusaxs_b200.h"
+#include "scratch_forward.h"
 #include "setup.h"
 
 namespace {
@@ -1271,6 +1272,121 @@ int histogram(SaxsPlan *pl, double *hist, double *nhist, cudaStream_t st) {
 }
 
 }  // namespace
+
+// ---------------------------------------------------------------------------
+// single frame into caller scratch (used by the allocation-free entry point)
+// ---------------------------------------------------------------------------
+namespace saxs {
+
+namespace {
+
+// Byte offsets of the per-frame buffers inside one scratch block.
+struct ScratchLayout {
+  size_t geom, key, counts, offsets, rec, border, Z, Y, ibox, total;
+};
+
+ScratchLayout scratch_layout(const DevArgs &a) {
+  auto up = [](size_t v) { return (v + 255) / 256 * 256; };
+  ScratchLayout L{};
+  size_t o = 0;
+  L.geom = o;
+  o = up(o + sizeof(float) * kGeom);
+  L.key = o;
+  o = up(o + sizeof(int2) * static_cast<size_t>(a.M));
+  L.counts = o;
+  o = up(o + sizeof(int) * static_cast<size_t>(a.nbins));
+  L.offsets = o;
+  o = up(o + sizeof(int) * (static_cast<size_t>(a.nbins) + 1));
+  L.rec = o;
+  o = up(o + sizeof(float4) * static_cast<size_t>(a.M));
+  L.border = o;
+  o = up(o + sizeof(double) * static_cast<size_t>(a.T));
+  L.Z = o;
+  o = up(o + sizeof(float2) * static_cast<size_t>(a.T) * a.nkz * a.ext[0] * a.ext[1]);
+  L.Y = o;
+  o = up(o + sizeof(float2) * static_cast<size_t>(a.T) * a.nkz * a.nky * a.ext[0]);
+  L.ibox = o;
+  o = up(o + sizeof(float) * static_cast<size_t>(a.nkz) * a.nky * a.nkx);
+  L.total = o;
+  return L;
+}
+
+}  // namespace
+
+int plan_device(const SaxsPlan *plan) { return plan->device; }
+
+size_t single_frame_scratch_bytes(const SaxsPlan *plan) { return scratch_layout(plan->a).total; }
+
+int record_error(int code, const char *msg) { return fail(code, msg); }
+
+int forward_into_scratch(SaxsPlan *pl, const float *xyz, const float *box, unsigned char *scratch,
+                         size_t scratch_bytes, double *hist, double *nhist, cudaStream_t st) {
+  if (!pl || !box || !scratch || !hist || !nhist || (!xyz && pl->a.M > 0))
+    return fail(SAXS_E_INVALID, "null argument");
+  if (int rc = check_box(box)) return rc;
+  DevArgs a = pl->a;
+  const ScratchLayout L = scratch_layout(a);
+  if (L.total > scratch_bytes) return fail(SAXS_E_RANGE, "scratch too small for this plan");
+  a.xyz = xyz;
+  a.frame_stride = 3ll * pl->p.natoms;
+  a.geom = reinterpret_cast<const float *>(scratch + L.geom);
+  a.key = reinterpret_cast<int2 *>(scratch + L.key);
+  a.counts = reinterpret_cast<int *>(scratch + L.counts);
+  a.offsets = reinterpret_cast<int *>(scratch + L.offsets);
+  a.rec = reinterpret_cast<float4 *>(scratch + L.rec);
+  a.border = reinterpret_cast<double *>(scratch + L.border);
+  a.Z = reinterpret_cast<float2 *>(scratch + L.Z);
+  a.Y = reinterpret_cast<float2 *>(scratch + L.Y);
+  a.ibox = reinterpret_cast<float *>(scratch + L.ibox);
+  a.hist = hist;
+  a.nhist = nhist;
+  // frame geometry, checked against the k-box, staged through the plan's pinned ring
+  Ring &ring = pl->ring;
+  const int slot = ring.next;
+  ring.next = (ring.next + 1) % kRing;
+  CUDA_TRY(cudaEventSynchronize(ring.ev[slot]));
+  float *g = ring.host + static_cast<size_t>(slot) * pl->p.max_frames * kGeom;
+  frame_geometry(pl, box, g);
+  long long h[3];
+  kbox_halfwidths(g + 9, a.qcut, 1e-5, h);
+  for (int d = 0; d < 3; ++d)
+    if (!pl->full_axis[d] && h[d] > pl->half[d])
+      return fail(SAXS_E_RANGE, "frame box shrank beyond the planned k-box margin");
+  CUDA_TRY(cudaMemcpyAsync(const_cast<float *>(a.geom), g, sizeof(float) * kGeom,
+                           cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaEventRecord(ring.ev[slot], st));
+  // the block keeps the previous call's contents: clear what accumulates
+  CUDA_TRY(cudaMemsetAsync(a.counts, 0, sizeof(int) * a.nbins, st));
+  CUDA_TRY(cudaMemsetAsync(a.border, 0, sizeof(double) * a.T, st));
+  CUDA_TRY(cudaMemsetAsync(hist, 0, sizeof(double) * a.num_bins, st));
+  CUDA_TRY(cudaMemsetAsync(nhist, 0, sizeof(double) * a.num_bins, st));
+  if (a.M > 0) {
+    dim3 gb((a.M + kThreads - 1) / kThreads, 1);
+    k_bin_atoms<<<gb, kThreads, pl->smem_bin, st>>>(a);
+    if (int rc = launch_check("k_bin_atoms")) return rc;
+    k_scan<<<1, 1024, 0, st>>>(a);
+    if (int rc = launch_check("k_scan")) return rc;
+    k_scatter_atoms<<<gb, kThreads, 0, st>>>(a);
+    if (int rc = launch_check("k_scatter_atoms")) return rc;
+  } else {
+    CUDA_TRY(cudaMemsetAsync(a.offsets, 0, sizeof(int) * (a.nbins + 1), st));
+  }
+  const int items = a.stiles[0] * a.stiles[1] * a.T;
+  k_spread_zdft<<<std::max(1, std::min(items, pl->spread_ctas)), kThreads, pl->smem_spread, st>>>(
+      a, items);
+  if (int rc = launch_check("k_spread_zdft")) return rc;
+  dim3 gy((a.ext[0] + kYRows - 1) / kYRows, a.nkz, a.T);
+  k_ydft<<<gy, kThreads, pl->smem_ydft, st>>>(a);
+  if (int rc = launch_check("k_ydft")) return rc;
+  dim3 gx((a.nky + kXRows - 1) / kXRows, a.nkz, 1);
+  k_xdft_post<<<gx, kThreads, pl->smem_xdft, st>>>(a);
+  if (int rc = launch_check("k_xdft_post")) return rc;
+  dim3 gh(a.nkz, 1);
+  k_hist<float><<<gh, kThreads, pl->smem_hist, st>>>(a, a.ibox, a.geom, kGeom, 1.0, hist, nhist);
+  return launch_check("k_hist");
+}
+
+}  // namespace saxs
 
 // ---------------------------------------------------------------------------
 // C ABI
