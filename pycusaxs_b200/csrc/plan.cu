@@ -82,6 +82,7 @@ struct DevArgs {
   int T, M;
   int tiles[2], stiles[2], nbins;
   int kx_lo, nkx, ky_lo, nky, nkz, nkzp, nkxp, nkyp;
+  int zc;  // z rows of twiddles k_spread_zdft holds in shared memory at once
   int nf[3];
   int dz;
   float dq, qcut;
@@ -378,9 +379,10 @@ __global__ void __launch_bounds__(kThreads, 2) k_spread_zdft(DevArgs a, int item
   const int nz = a.n[2], ez = a.ext[2];
   const int NP = 2 * a.nkzp;
   float *tws = reinterpret_cast<float *>(smem);
-  float *tile = tws + static_cast<size_t>(ez) * NP;
+  float *tile = tws + static_cast<size_t>(a.zc) * NP;
   const int tid = threadIdx.x;
-  {
+  const bool all_rows = a.zc >= ez;
+  if (all_rows) {
     const float4 *src = reinterpret_cast<const float4 *>(a.twz);
     float4 *dst = reinterpret_cast<float4 *>(tws);
     const int n4 = ez * NP / 4;
@@ -388,11 +390,11 @@ __global__ void __launch_bounds__(kThreads, 2) k_spread_zdft(DevArgs a, int item
   }
   const int ngroups = a.nkzp / kKzThread;      // kz groups of kKzThread
   const int tps = (kCols / 4) * ngroups;       // tasks per z split
+  // Small k-boxes: every task runs once and the z range is split `ks` ways.
+  // Large k-boxes (tps > block): ks = 1 and the block walks the tasks in rounds.
   const int ks = max(1, min(8, static_cast<int>(blockDim.x) / tps));
-  const int split = tid / tps, task = tid % tps;
-  const int cg = task % (kCols / 4), kg = task / (kCols / 4);
-  const bool worker = split < ks;
-  const int zlo = split * ez / ks, zhi = (split + 1) * ez / ks;
+  const int rounds = (tps + blockDim.x - 1) / blockDim.x;
+  const int split = rounds > 1 ? 0 : tid / tps;
   const int st = a.stiles[0] * a.stiles[1];
   const int ex = a.ext[0], ey = a.ext[1];
   const int64_t zplane = static_cast<int64_t>(ex) * ey;
@@ -418,26 +420,44 @@ __global__ void __launch_bounds__(kThreads, 2) k_spread_zdft(DevArgs a, int item
     // only.  The column DFT of -mean over z < ez is -mean * sum_z tw[z][n].
     const float mean =
         static_cast<float>(a.border[static_cast<int64_t>(f) * a.T + t] / a.border_count);
-    float acc[4][2 * kKzThread];
+    float2 *Zft = a.Z + (static_cast<int64_t>(f) * a.T + t) * a.nkz * zplane;
+    for (int rd = 0; rd < rounds; ++rd) {
+      const int task = rounds > 1 ? rd * blockDim.x + tid : tid % tps;
+      const bool worker = rounds > 1 ? task < tps : split < ks;
+      const int cg = task % (kCols / 4), kg = task / (kCols / 4);
+      float acc[4][2 * kKzThread];
 #pragma unroll
-    for (int c = 0; c < 4; ++c)
+      for (int c = 0; c < 4; ++c)
 #pragma unroll
-      for (int n = 0; n < 2 * kKzThread; ++n) acc[c][n] = 0.f;
-    if (worker) {
-      const float4 *g4 = reinterpret_cast<const float4 *>(tile) + cg;
-      const float *twr = tws + kg * 2 * kKzThread;
-      for (int z = zlo; z < zhi; ++z) {
-        const float4 g = g4[z * (kCols / 4)];
-        const float4 *w4 = reinterpret_cast<const float4 *>(twr + z * NP);
-        const float4 w0 = w4[0], w1 = w4[1], w2 = w4[2];
-        const float wv[12] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w, w2.x, w2.y, w2.z, w2.w};
-        const float gv[4] = {g.x, g.y, g.z, g.w};
+        for (int n = 0; n < 2 * kKzThread; ++n) acc[c][n] = 0.f;
+      for (int z0 = 0; z0 < ez; z0 += a.zc) {
+        const int zn = min(a.zc, ez - z0);
+        if (!all_rows) {
+          __syncthreads();
+          const float4 *src = reinterpret_cast<const float4 *>(a.twz) + static_cast<size_t>(z0) * NP / 4;
+          float4 *dst = reinterpret_cast<float4 *>(tws);
+          const int n4 = zn * NP / 4;
+          for (int i = tid; i < n4; i += blockDim.x) dst[i] = src[i];
+          __syncthreads();
+        }
+        if (worker) {
+          const float4 *g4 = reinterpret_cast<const float4 *>(tile) + cg;
+          const float *twr = tws + kg * 2 * kKzThread;
+          const int zlo = z0 + split * zn / ks, zhi = z0 + (split + 1) * zn / ks;
+          for (int z = zlo; z < zhi; ++z) {
+            const float4 g = g4[z * (kCols / 4)];
+            const float4 *w4 = reinterpret_cast<const float4 *>(twr + (z - z0) * NP);
+            const float4 w0 = w4[0], w1 = w4[1], w2 = w4[2];
+            const float wv[12] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w, w2.x, w2.y, w2.z, w2.w};
+            const float gv[4] = {g.x, g.y, g.z, g.w};
 #pragma unroll
-        for (int c = 0; c < 4; ++c)
+            for (int c = 0; c < 4; ++c)
 #pragma unroll
-          for (int n = 0; n < 12; ++n) acc[c][n] = fmaf(gv[c], wv[n], acc[c][n]);
+              for (int n = 0; n < 12; ++n) acc[c][n] = fmaf(gv[c], wv[n], acc[c][n]);
+          }
+        }
       }
-      if (split == 0) {
+      if (worker && split == 0) {
 #pragma unroll
         for (int n = 0; n < 2 * kKzThread; ++n) {
           const float d = a.twz_sum[kg * 2 * kKzThread + n];
@@ -445,39 +465,57 @@ __global__ void __launch_bounds__(kThreads, 2) k_spread_zdft(DevArgs a, int item
           for (int c = 0; c < 4; ++c) acc[c][n] = fmaf(-mean, d, acc[c][n]);
         }
       }
-    }
-    __syncthreads();  // tile contents are dead: reuse the region as out[NP][64]
-    float *out = tile;
-    for (int r = 0; r < ks; ++r) {
-      if (worker && split == r) {
+      if (rounds > 1) {
+        // the tile is still read by later rounds: results go straight to Z
+        if (worker) {
 #pragma unroll
-        for (int n = 0; n < 2 * kKzThread; ++n) {
-          float4 *o = reinterpret_cast<float4 *>(out + (kg * 2 * kKzThread + n) * kCols) + cg;
-          float4 v = make_float4(acc[0][n], acc[1][n], acc[2][n], acc[3][n]);
-          if (r > 0) {
-            const float4 u = *o;
-            v.x += u.x;
-            v.y += u.y;
-            v.z += u.z;
-            v.w += u.w;
+          for (int c = 0; c < 4; ++c) {
+            const int col = 4 * cg + c, lx = col / kTile, ly = col % kTile;
+            if (lx >= cw || ly >= ch) continue;
+#pragma unroll
+            for (int j = 0; j < kKzThread; ++j) {
+              const int kz = kg * kKzThread + j;
+              if (kz < a.nkz)
+                Zft[kz * zplane + static_cast<int64_t>(x0 + lx) * ey + (y0 + ly)] =
+                    make_float2(acc[c][2 * j], acc[c][2 * j + 1]);
+            }
           }
-          *o = v;
         }
+        continue;
       }
-      __syncthreads();
-    }
-    float2 *Zft = a.Z + (static_cast<int64_t>(f) * a.T + t) * a.nkz * zplane;
-    for (int i = tid; i < a.nkz * kCols; i += blockDim.x) {
-      const int kz = i / kCols, col = i % kCols;
-      const int lx = col / kTile, ly = col % kTile;
-      if (lx < cw && ly < ch) {
-        const float2 v = make_float2(out[(2 * kz) * kCols + col], out[(2 * kz + 1) * kCols + col]);
-        Zft[kz * zplane + static_cast<int64_t>(x0 + lx) * ey + (y0 + ly)] = v;
+      __syncthreads();  // tile contents are dead: reuse the region as out[NP][64]
+      float *out = tile;
+      for (int r = 0; r < ks; ++r) {
+        if (worker && split == r) {
+#pragma unroll
+          for (int n = 0; n < 2 * kKzThread; ++n) {
+            float4 *o = reinterpret_cast<float4 *>(out + (kg * 2 * kKzThread + n) * kCols) + cg;
+            float4 v = make_float4(acc[0][n], acc[1][n], acc[2][n], acc[3][n]);
+            if (r > 0) {
+              const float4 u = *o;
+              v.x += u.x;
+              v.y += u.y;
+              v.z += u.z;
+              v.w += u.w;
+            }
+            *o = v;
+          }
+        }
+        __syncthreads();
+      }
+      for (int i = tid; i < a.nkz * kCols; i += blockDim.x) {
+        const int kz = i / kCols, col = i % kCols;
+        const int lx = col / kTile, ly = col % kTile;
+        if (lx < cw && ly < ch) {
+          const float2 v = make_float2(out[(2 * kz) * kCols + col], out[(2 * kz + 1) * kCols + col]);
+          Zft[kz * zplane + static_cast<int64_t>(x0 + lx) * ey + (y0 + ly)] = v;
+        }
       }
     }
     __syncthreads();
   }
 }
+
 
 // grid (ceil(ex/64), nkz, frames*T), block 256: y-axis DFT.
 // Y[f,t,kz][ky][x] = sum_y Z[f,t,kz][x][y] * exp(-2 pi i ja y / nny).
@@ -547,13 +585,14 @@ __global__ void __launch_bounds__(kThreads) k_ydft(DevArgs a) {
 }
 
 // grid (ceil(nky/4), nkz, frames), block 256: x-axis DFT, form factors, type
-// sum, modulus.  Dynamic shared memory: twx ex*nkxp | Y rows T*ex | F T*nkxp (float2).
-__global__ void __launch_bounds__(kThreads) k_xdft_post(DevArgs a) {
+// sum, modulus.  Dynamic shared memory, for an x chunk of `xc` values:
+// twx xc*nkxp | Y rows T*xc | F T*nkxp (all float2).
+__global__ void __launch_bounds__(kThreads) k_xdft_post(DevArgs a, int xc) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int ex = a.ext[0];
   float2 *txs = reinterpret_cast<float2 *>(smem);
-  float2 *ys = txs + static_cast<size_t>(ex) * a.nkxp;
-  float2 *fs = ys + static_cast<size_t>(a.T) * ex;
+  float2 *ys = txs + static_cast<size_t>(xc) * a.nkxp;
+  float2 *fs = ys + static_cast<size_t>(a.T) * xc;
   __shared__ float ocs[9];
   __shared__ float means[64];
   const int f = blockIdx.z, kz = blockIdx.y;
@@ -561,37 +600,53 @@ __global__ void __launch_bounds__(kThreads) k_xdft_post(DevArgs a) {
   if (tid < 9) ocs[tid] = a.geom[f * kGeom + 9 + tid];
   for (int t = tid; t < a.T && t < 64; t += blockDim.x)
     means[t] = static_cast<float>(a.border[static_cast<int64_t>(f) * a.T + t] / a.border_count);
-  {
+  const bool one_chunk = xc >= ex;
+  if (one_chunk) {
     const float4 *src = reinterpret_cast<const float4 *>(a.twx);
     float4 *dst = reinterpret_cast<float4 *>(txs);
     const int n4 = ex * a.nkxp / 2;
     for (int i = tid; i < n4; i += blockDim.x) dst[i] = src[i];
   }
   const int ka = signed_k(kz, a.nn[2], a.nf[2]);
+  const int npairs = a.T * a.nkx;
   for (int r = 0; r < kXRows; ++r) {
     const int ky = blockIdx.x * kXRows + r;
     if (ky >= a.nky) break;
     const int ja = a.ky_lo + ky;
-    __syncthreads();
-    for (int i = tid; i < a.T * ex; i += blockDim.x) {
-      const int t = i / ex, x = i % ex;
-      ys[i] = a.Y[((static_cast<int64_t>(f) * a.T + t) * a.nkz + kz) * a.nky * ex +
-                  static_cast<int64_t>(ky) * ex + x];
-    }
-    __syncthreads();
-    for (int i = tid; i < a.T * a.nkx; i += blockDim.x) {
+    for (int p0 = 0; p0 < npairs; p0 += blockDim.x) {
+      const int i = p0 + tid;
       const int t = i / a.nkx, kx = i % a.nkx;
-      const float2 *yr = ys + t * ex;
       float2 acc = make_float2(0.f, 0.f);
-      for (int x = 0; x < ex; ++x) {
-        const float2 v = yr[x];
-        const float2 w = txs[x * a.nkxp + kx];
-        acc.x = fmaf(v.x, w.x, fmaf(-v.y, w.y, acc.x));
-        acc.y = fmaf(v.x, w.y, fmaf(v.y, w.x, acc.y));
+      for (int x0 = 0; x0 < ex; x0 += xc) {
+        const int xn = min(xc, ex - x0);
+        __syncthreads();
+        for (int j = tid; j < a.T * xn; j += blockDim.x) {
+          const int tt = j / xn, x = j % xn;
+          ys[tt * xc + x] = a.Y[((static_cast<int64_t>(f) * a.T + tt) * a.nkz + kz) * a.nky * ex +
+                                static_cast<int64_t>(ky) * ex + x0 + x];
+        }
+        if (!one_chunk) {
+          const float4 *src = reinterpret_cast<const float4 *>(a.twx + static_cast<size_t>(x0) * a.nkxp);
+          float4 *dst = reinterpret_cast<float4 *>(txs);
+          const int n4 = xn * a.nkxp / 2;
+          for (int j = tid; j < n4; j += blockDim.x) dst[j] = src[j];
+        }
+        __syncthreads();
+        if (i < npairs) {
+          const float2 *yr = ys + t * xc;
+          for (int x = 0; x < xn; ++x) {
+            const float2 v = yr[x];
+            const float2 w = txs[x * a.nkxp + kx];
+            acc.x = fmaf(v.x, w.x, fmaf(-v.y, w.y, acc.x));
+            acc.y = fmaf(v.x, w.y, fmaf(v.y, w.x, acc.y));
+          }
+        }
       }
-      if (ka == 0 && ja == 0 && a.kx_lo + kx == 0)
-        acc.x += static_cast<float>(static_cast<double>(means[t < 64 ? t : 63]) * a.nn3);
-      fs[t * a.nkxp + kx] = acc;
+      if (i < npairs) {
+        if (ka == 0 && ja == 0 && a.kx_lo + kx == 0)
+          acc.x += static_cast<float>(static_cast<double>(means[t < 64 ? t : 63]) * a.nn3);
+        fs[t * a.nkxp + kx] = acc;
+      }
     }
     __syncthreads();
     for (int kx = tid; kx < a.nkx; kx += blockDim.x) {
@@ -629,15 +684,13 @@ __global__ void __launch_bounds__(kThreads)
   const bool in_smem = a.num_bins <= kHistSmemBins;
   double *sh = reinterpret_cast<double *>(smem);
   double *sn = sh + (in_smem ? a.num_bins : 0);
-  V *pl = reinterpret_cast<V *>(sn + (in_smem ? a.num_bins : 0));
   __shared__ float ocs[9];
   const int kz = blockIdx.x, f = blockIdx.y;
   const int tid = threadIdx.x;
   if (tid < 9) ocs[tid] = geom[f * geom_stride + 9 + tid];
   if (in_smem)
     for (int b = tid; b < 2 * a.num_bins; b += blockDim.x) sh[b] = 0.0;
-  const V *src = vals + (static_cast<int64_t>(f) * a.nkz + kz) * npts;
-  for (int p = tid; p < npts; p += blockDim.x) pl[p] = src[p];
+  const V *pl = vals + (static_cast<int64_t>(f) * a.nkz + kz) * npts;
   __syncthreads();
   const int ka = signed_k(kz, a.nn[2], a.nf[2]);
   const int kx_hi = a.kx_lo + a.nkx - 1, ky_hi = a.ky_lo + a.nky - 1;
@@ -730,6 +783,7 @@ struct SaxsPlan {
   float *d_geom0 = nullptr;
   double *d_tmp_hist = nullptr;
   int spread_ctas = 1;  // resident CTAs of the persistent spreading kernel
+  int xc = 1;           // x values per shared-memory chunk in k_xdft_post
   bool profiling = false;
   std::vector<StageRecord> prof_pending;
   std::vector<cudaEvent_t> event_pool;
@@ -944,27 +998,39 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
   a.nkxp = round_up(a.nkx, 2);
   a.nkyp = round_up(a.nky, kKyGroup);
 
-  // shared-memory budgets
-  pl->smem_spread = (static_cast<size_t>(a.ext[2]) * 2 * a.nkzp +
-                     std::max<size_t>(static_cast<size_t>(a.n[2]) * kCols,
-                                      static_cast<size_t>(kCols) * 2 * a.nkzp)) * sizeof(float);
+  // shared-memory budgets (rows of twiddles / x chunks shrink to fit)
+  const size_t optin = static_cast<size_t>(optin_smem());
+  {
+    const size_t NP = 2 * static_cast<size_t>(a.nkzp);
+    const size_t tile = std::max<size_t>(static_cast<size_t>(a.n[2]) * kCols, kCols * NP) * sizeof(float);
+    const size_t avail = optin - static_smem(k_spread_zdft);
+    size_t zc = a.ext[2];
+    while (zc > 8 && zc * NP * sizeof(float) + tile > avail) zc = (zc > 16) ? zc / 2 : 8;
+    a.zc = static_cast<int>(zc);
+    pl->smem_spread = zc * NP * sizeof(float) + tile;
+  }
   pl->smem_ydft = static_cast<size_t>(kYChunk) * kYStride * sizeof(float2) +
                   static_cast<size_t>(kYChunk) * a.nkyp * sizeof(float2);
-  pl->smem_xdft = (static_cast<size_t>(a.ext[0]) * a.nkxp + static_cast<size_t>(a.T) * a.ext[0] +
-                   static_cast<size_t>(a.T) * a.nkxp) * sizeof(float2);
-  const size_t plane = static_cast<size_t>(a.nky) * a.nkx;
-  pl->smem_hist = (a.num_bins <= kHistSmemBins ? 2 * sizeof(double) * a.num_bins : 0) +
-                  plane * sizeof(double);
+  {
+    const size_t avail = optin - static_smem(k_xdft_post);
+    const size_t fixed = static_cast<size_t>(a.T) * a.nkxp * sizeof(float2);
+    const size_t per_x = (static_cast<size_t>(a.nkxp) + a.T) * sizeof(float2);
+    size_t xc = a.ext[0];
+    if (fixed + xc * per_x > avail) xc = avail > fixed + 2 * per_x ? (avail - fixed) / per_x : 2;
+    xc = std::max<size_t>(2, xc & ~static_cast<size_t>(1));
+    pl->xc = static_cast<int>(std::min<size_t>(xc, a.ext[0]));
+    pl->smem_xdft = fixed + static_cast<size_t>(pl->xc) * per_x;
+  }
+  pl->smem_hist = a.num_bins <= kHistSmemBins ? 2 * sizeof(double) * a.num_bins : 0;
   pl->smem_bin = static_cast<size_t>(kThreads / 32) * a.T * sizeof(double);
-  const size_t optin = static_cast<size_t>(optin_smem());
   if (pl->smem_spread + static_smem(k_spread_zdft) > optin ||
       pl->smem_ydft + static_smem(k_ydft) > optin ||
       pl->smem_xdft + static_smem(k_xdft_post) > optin ||
       pl->smem_hist + static_smem(k_hist<double>) > optin || pl->smem_bin > 40 * 1024) {
     destroy(pl);
     return fail(SAXS_E_INVALID,
-                "grid / q-cut combination exceeds the shared-memory budget of the pruned path (z "
-                "extent " + std::to_string(a.n[2]) + ", k-box " + std::to_string(a.nkx) + "x" +
+                "grid / q-cut combination exceeds the shared-memory budget (z extent " +
+                    std::to_string(a.n[2]) + ", k-box " + std::to_string(a.nkx) + "x" +
                     std::to_string(a.nky) + "x" + std::to_string(a.nkz) + ")");
   }
   if (a.T > 64) {
@@ -1227,7 +1293,7 @@ int forward(SaxsPlan *pl, const float *xyz, int64_t stride, int nframes, const f
   {
     dim3 gx((a.nky + kXRows - 1) / kXRows, a.nkz, nframes);
     tm.begin(kStXdft);
-    k_xdft_post<<<gx, kThreads, pl->smem_xdft, st>>>(a);
+    k_xdft_post<<<gx, kThreads, pl->smem_xdft, st>>>(a, pl->xc);
     tm.end(kStXdft);
     if (int rc = launch_check("k_xdft_post")) return rc;
   }
@@ -1379,7 +1445,7 @@ int forward_into_scratch(SaxsPlan *pl, const float *xyz, const float *box, unsig
   k_ydft<<<gy, kThreads, pl->smem_ydft, st>>>(a);
   if (int rc = launch_check("k_ydft")) return rc;
   dim3 gx((a.nky + kXRows - 1) / kXRows, a.nkz, 1);
-  k_xdft_post<<<gx, kThreads, pl->smem_xdft, st>>>(a);
+  k_xdft_post<<<gx, kThreads, pl->smem_xdft, st>>>(a, pl->xc);
   if (int rc = launch_check("k_xdft_post")) return rc;
   dim3 gh(a.nkz, 1);
   k_hist<float><<<gh, kThreads, pl->smem_hist, st>>>(a, a.ibox, a.geom, kGeom, 1.0, hist, nhist);

@@ -138,3 +138,54 @@ def test_border_sums_match_oracle_grid(cuda):
         g = O.spread(r[sel], (32, 32, 32), 4)
         assert got[t] == pytest.approx(g[:, :, mask].sum(), rel=1e-6)
     eng.close()
+
+
+def _two_element(n, lengths, seed):
+    rng = np.random.default_rng(seed)
+    L = np.asarray(lengths, np.float64)
+    pos = (rng.uniform(0, 1, (n, 3)) * L).astype(np.float32)
+    el = np.array(["C", "O"], dtype=object)[rng.choice(2, n)]
+    return System(el, pos, np.diag(L).astype(np.float32))
+
+
+def test_long_z_axis_full_spectrum_chunks_z_twiddles(cuda):
+    # 16 x 16 x 256 grid, 512 supercell along z, q-cut above Nyquist: the z
+    # twiddle table (256 rows x 258 kz) cannot sit in shared memory at once
+    s = _two_element(1500, (20.0, 20.0, 320.0), seed=31)
+    _run(s, (16, 16, 256), [s.positions], sigma=2.0, qcut=50.0)
+
+
+def test_long_x_axis_full_spectrum_chunks_x(cuda):
+    # 256 x 16 x 16 grid, full kx range of 512: k_xdft_post walks x in chunks
+    s = _two_element(1500, (320.0, 20.0, 20.0), seed=32)
+    _run(s, (256, 16, 16), [s.positions], sigma=2.0, qcut=50.0)
+
+
+def test_cli_default_parameters(cuda):
+    # the CLI defaults: scale 2.5, bin 0.01 /A, q-cut 2.0 /A (pycusaxs/saxs_defaults.py)
+    s = cubic_system(8000, 60.0, seed=33)
+    _run(s, (64, 64, 64), [s.positions], sigma=2.5, bin_size=0.01, qcut=2.0)
+
+
+def test_kbox_intensity_matches_direct_sum_on_isolated_cluster(cuda):
+    """CUDA k-box intensities vs the exact direct sum (the physics check on the GPU)."""
+    from test_physics import NAMES, cluster, direct_intensity
+    from oracle import saxs_oracle as O
+
+    pos, toa, box = cluster()
+    s = System(np.array(NAMES, dtype=object)[toa], pos, box)
+    h, n, eng = engine_hist(s, (64, 64, 64), [pos], sigma=2.0, qcut=0.6)
+    ib = eng.kbox_intensity()                       # (nkz, nky, nkx)
+    nkx, nky, nkz = eng.info.kbox
+    kz, ky, kx = np.meshgrid(np.arange(nkz), np.arange(nky), np.arange(nkx), indexing="ij")
+    m = np.stack([kx - (nkx // 2), ky - (nky // 2), kz], axis=-1).reshape(-1, 3).astype(np.float64)
+    ocs = (np.float32(64) / np.float32(128) * O.cell_matrices(box)[1]).astype(np.float64)
+    qvec = 2 * np.pi * (m @ ocs.T)
+    ff = O.load_form_factors()
+    i_dir, qa, _ = direct_intensity(qvec, pos, toa, np.stack([ff[k] for k in NAMES]))
+    i_gpu = ib.reshape(-1).astype(np.float64)
+    keep = (i_gpu > 0) & (qa > 0)
+    rel = np.abs(i_gpu[keep] - i_dir[keep]) / i_dir[keep]
+    assert keep.sum() > 3000
+    assert np.median(rel) < 1e-4 and np.quantile(rel, 0.99) < 2e-3 and rel.max() < 1e-2
+    eng.close()
