@@ -53,6 +53,7 @@ def parse():
     ap.add_argument("--batch", type=int, default=FRAMES)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
     return ap.parse_args()
 
 
@@ -270,6 +271,9 @@ def bench_ours(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(system)
+    adj = None
+    if rank == 0 and world == 1 and not args.no_adjoint:
+        adj = refinement()
 
     launches = sum(v[1] for v in prof.values())
     out = {
@@ -282,7 +286,8 @@ def bench_ours(args):
                                "(256^3 supercell), qcut 0.5/A, 100 frames per step, npt",
                    "frames_per_step_per_gpu": FRAMES, "batch": B, "l2": "flushed between steps",
                    "kbox": [nkx, nky, nkz], "plain_path_frames_per_s": round(plain, 1) if plain else None,
-                   "stage_share": stage_share, "parallelism": f"frames sharded over {world} GPU(s)"},
+                   "stage_share": stage_share, "parallelism": f"frames sharded over {world} GPU(s)",
+                   "adjoint": adj},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": ck,
         "gpu_launches": int(launches),
     }
@@ -291,6 +296,74 @@ def bench_ours(args):
         print(json.dumps(out))
     if dist is not None:
         dist.destroy_process_group()
+
+
+def refinement(steps: int = 100) -> dict:
+    """50k atoms, 10 nm box, grid 128 (256^3): forward vs forward+adjoint, and Adam refinement.
+
+    Target: the same system after a seeded 1 A Gaussian displacement of 5% of
+    the atoms; loss = sum over reported bins of (log I - log I_target)^2.
+    """
+    import torch
+
+    from pycusaxs_b200 import SaxsEngine
+    from pycusaxs_b200.autograd import saxs_profile
+    from pycusaxs_b200.synthetic import cubic_system
+
+    s = cubic_system(50_000, 100.0, seed=77)
+    rng = np.random.default_rng(78)
+    moved = s.positions.copy()
+    idx = rng.choice(s.natoms, s.natoms // 20, replace=False)
+    moved[idx] += rng.normal(0.0, 1.0, (idx.size, 3)).astype(np.float32)
+    eng = SaxsEngine((128,) * 3, s.atom_index(), s.natoms, s.box, scale_factor=2.0, bin_size=0.002,
+                     qcut=0.5, box_margin=0.05)
+    dev = eng.device
+    with torch.no_grad():
+        target = saxs_profile(torch.tensor(moved, device=dev), eng, s.box)
+    sel = target > 0
+    x = torch.tensor(s.positions, device=dev, requires_grad=True)
+
+    def loss_fn():
+        prof = saxs_profile(x, eng, s.box)
+        return ((torch.log(prof[sel]) - torch.log(target[sel])) ** 2).sum()
+
+    def timed(fn, n):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(n):
+            fn()
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t0) * 1e3 / n
+
+    def fwd():
+        with torch.no_grad():
+            loss_fn()
+
+    def fwd_bwd():
+        x.grad = None
+        loss_fn().backward()
+
+    fwd_ms = timed(fwd, 10)
+    fb_ms = timed(fwd_bwd, 10)
+    opt = torch.optim.Adam([x], lr=0.01)
+    l0 = float(loss_fn().detach())
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        opt.zero_grad()
+        loss = loss_fn()
+        loss.backward()
+        opt.step()
+    torch.cuda.synchronize()
+    adam_s = time.perf_counter() - t0
+    l1 = float(loss_fn().detach())
+    eng.close()
+    return {"workload": "50k atoms, 10 nm box, grid 128, scale 2 (256^3), log-profile loss",
+            "forward_ms": round(fwd_ms, 3), "forward_adjoint_ms": round(fb_ms, 3),
+            "adjoint_over_forward": round(fb_ms / fwd_ms, 2),
+            "adam_steps": steps, "adam_s": round(adam_s, 3), "loss_start": l0, "loss_end": l1}
 
 
 def cpu_baseline(system) -> dict:

@@ -733,6 +733,296 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
+// ---------------------------------------------------------------------------
+// adjoint (reverse mode) kernels: dL/dI(bin) -> dL/dxyz for one frame
+// ---------------------------------------------------------------------------
+
+// Extra device buffers of the adjoint, allocated on first use.
+struct AdjArgs {
+  const double *dl;   // [num_bins] dL/d profile
+  const double *nh;   // [num_bins] the frame's bin counts
+  float2 *G;          // [T][nkz][nky][nkx] dL/dF_t (Re + i Im)
+  float2 *H1;         // [T][nkz][ex][nky]
+  float2 *H2;         // [T][ex][ey][nkz]
+  float *dg;          // [T][ex][ey][ez] dL/dg' on the corner block
+  double *S;          // [T] sum of dg over the corner block
+  float *dcg;         // [T] nn^3 * Re G_t(k = 0)
+  float *grad;        // [natoms * 3] output
+};
+
+__device__ __forceinline__ double bin_weight(const DevArgs &a, const AdjArgs &j, const float *ocs,
+                                             int ia, int ja, int ka) {
+  const float mw = kpoint_q(ocs, ia, ja, ka);
+  if (mw > a.qcut || a.dq <= 0.0f) return 0.0;
+  const int h0 = static_cast<int>(mw / a.dq);
+  if (h0 < 0 || h0 >= a.num_bins) return 0.0;
+  const double n = j.nh[h0];
+  return n != 0.0 ? j.dl[h0] / n : 0.0;
+}
+
+// grid (ceil(nky/4), nkz), block 256: x-axis DFT of the recomputed Y rows, then
+// G_t(p) = 2 w(p) M(p) f_t(p) A(p) with w(p) = g[bin(p)] + g[bin(mirror(p))].
+__global__ void __launch_bounds__(kThreads) k_xdft_grad(DevArgs a, AdjArgs j, int xc) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int ex = a.ext[0];
+  float2 *txs = reinterpret_cast<float2 *>(smem);
+  float2 *ys = txs + static_cast<size_t>(xc) * a.nkxp;
+  float2 *fs = ys + static_cast<size_t>(a.T) * xc;
+  __shared__ float ocs[9];
+  __shared__ float means[64];
+  const int kz = blockIdx.y;
+  const int tid = threadIdx.x;
+  if (tid < 9) ocs[tid] = a.geom[9 + tid];
+  for (int t = tid; t < a.T && t < 64; t += blockDim.x)
+    means[t] = static_cast<float>(a.border[t] / a.border_count);
+  const int ka = signed_k(kz, a.nn[2], a.nf[2]);
+  const int npairs = a.T * a.nkx;
+  const int kx_hi = a.kx_lo + a.nkx - 1, ky_hi = a.ky_lo + a.nky - 1;
+  for (int r = 0; r < kXRows; ++r) {
+    const int ky = blockIdx.x * kXRows + r;
+    if (ky >= a.nky) break;
+    const int ja = a.ky_lo + ky;
+    for (int p0 = 0; p0 < npairs; p0 += blockDim.x) {
+      const int i = p0 + tid;
+      const int t = i / a.nkx, kx = i % a.nkx;
+      float2 acc = make_float2(0.f, 0.f);
+      for (int x0 = 0; x0 < ex; x0 += xc) {
+        const int xn = min(xc, ex - x0);
+        __syncthreads();
+        for (int q = tid; q < a.T * xn; q += blockDim.x) {
+          const int tt = q / xn, x = q % xn;
+          ys[tt * xc + x] = a.Y[(static_cast<int64_t>(tt) * a.nkz + kz) * a.nky * ex +
+                                static_cast<int64_t>(ky) * ex + x0 + x];
+        }
+        {
+          const float4 *src = reinterpret_cast<const float4 *>(a.twx + static_cast<size_t>(x0) * a.nkxp);
+          float4 *dst = reinterpret_cast<float4 *>(txs);
+          const int n4 = xn * a.nkxp / 2;
+          for (int q = tid; q < n4; q += blockDim.x) dst[q] = src[q];
+        }
+        __syncthreads();
+        if (i < npairs) {
+          const float2 *yr = ys + t * xc;
+          for (int x = 0; x < xn; ++x) {
+            const float2 v = yr[x];
+            const float2 w = txs[x * a.nkxp + kx];
+            acc.x = fmaf(v.x, w.x, fmaf(-v.y, w.y, acc.x));
+            acc.y = fmaf(v.x, w.y, fmaf(v.y, w.x, acc.y));
+          }
+        }
+      }
+      if (i < npairs) {
+        if (ka == 0 && ja == 0 && a.kx_lo + kx == 0)
+          acc.x += static_cast<float>(static_cast<double>(means[t < 64 ? t : 63]) * a.nn3);
+        fs[t * a.nkxp + kx] = acc;
+      }
+    }
+    __syncthreads();
+    for (int kx = tid; kx < a.nkx; kx += blockDim.x) {
+      const int ia = a.kx_lo + kx;
+      const float mw = kpoint_q(ocs, ia, ja, ka);
+      double w = 0.0;
+      float q2 = 0.f;
+      if (!(mw > a.qcut)) {
+        const float q = mw / (4.0 * M_PI);
+        q2 = q * q;
+        w = bin_weight(a, j, ocs, ia, ja, ka);
+        if (!(ia == 0 && ja == 0 && ka == 0)) {
+          int ib = -ia, jb = -ja;
+          if (ib > kx_hi) ib = ia;
+          if (jb > ky_hi) jb = ja;
+          w += bin_weight(a, j, ocs, ib, jb, ka);
+        }
+      }
+      float2 A = make_float2(0.f, 0.f);
+      if (w != 0.0) {
+        for (int t = 0; t < a.T; ++t) {
+          const float ft = form_factor(a.ff + 9 * t, q2);
+          const float2 F = fs[t * a.nkxp + kx];
+          A.x = fmaf(ft, F.x, A.x);
+          A.y = fmaf(ft, F.y, A.y);
+        }
+      }
+      const int ii = ia < 0 ? ia + a.nn[0] : ia;
+      const int jj = ja < 0 ? ja + a.nn[1] : ja;
+      const float bsp = a.modx[ii] * a.mody[jj] * a.modz[kz];
+      const float s = static_cast<float>(2.0 * w) * bsp;
+      for (int t = 0; t < a.T; ++t) {
+        float2 g = make_float2(0.f, 0.f);
+        if (w != 0.0) {
+          const float ft = form_factor(a.ff + 9 * t, q2);
+          g = make_float2(s * ft * A.x, s * ft * A.y);
+        }
+        j.G[((static_cast<int64_t>(t) * a.nkz + kz) * a.nky + ky) * a.nkx + kx] = g;
+        if (ka == 0 && ja == 0 && ia == 0) j.dcg[t] = static_cast<float>(g.x * a.nn3);
+      }
+    }
+  }
+}
+
+// H1[t][kz][x][ky] = sum_kx G[t][kz][ky][kx] conj(exp(-2 pi i kx x / nnx)); thread per output.
+__global__ void k_xadj(DevArgs a, AdjArgs j) {
+  const int ex = a.ext[0];
+  const int64_t total = static_cast<int64_t>(a.T) * a.nkz * ex * a.nky;
+  const int64_t o = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (o >= total) return;
+  const int ky = o % a.nky;
+  const int x = (o / a.nky) % ex;
+  const int64_t tk = o / (static_cast<int64_t>(a.nky) * ex);
+  const float2 *g = j.G + (tk * a.nky + ky) * a.nkx;
+  const float2 *w = a.twx + static_cast<size_t>(x) * a.nkxp;
+  float2 acc = make_float2(0.f, 0.f);
+  for (int kx = 0; kx < a.nkx; ++kx) {
+    const float2 v = g[kx], c = w[kx];        // v * conj(c)
+    acc.x = fmaf(v.x, c.x, fmaf(v.y, c.y, acc.x));
+    acc.y = fmaf(v.y, c.x, fmaf(-v.x, c.y, acc.y));
+  }
+  j.H1[o] = acc;
+}
+
+// H2[t][x][y][kz] = sum_ky H1[t][kz][x][ky] conj(exp(-2 pi i ky y / nny)); thread per output.
+__global__ void k_yadj(DevArgs a, AdjArgs j) {
+  const int ex = a.ext[0], ey = a.ext[1];
+  const int64_t total = static_cast<int64_t>(a.T) * ex * ey * a.nkz;
+  const int64_t o = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (o >= total) return;
+  const int kz = o % a.nkz;
+  const int y = (o / a.nkz) % ey;
+  const int x = (o / (static_cast<int64_t>(a.nkz) * ey)) % ex;
+  const int t = static_cast<int>(o / (static_cast<int64_t>(a.nkz) * ey * ex));
+  const float2 *h = j.H1 + ((static_cast<int64_t>(t) * a.nkz + kz) * ex + x) * a.nky;
+  const float2 *w = a.twy + static_cast<size_t>(y) * a.nkyp;
+  float2 acc = make_float2(0.f, 0.f);
+  for (int ky = 0; ky < a.nky; ++ky) {
+    const float2 v = h[ky], c = w[ky];
+    acc.x = fmaf(v.x, c.x, fmaf(v.y, c.y, acc.x));
+    acc.y = fmaf(v.y, c.x, fmaf(-v.x, c.y, acc.y));
+  }
+  j.H2[o] = acc;
+}
+
+// dg[t][x][y][z] = Re sum_kz H2[t][x][y][kz] conj(exp(-2 pi i kz z / nnz)); thread per output.
+__global__ void k_zadj(DevArgs a, AdjArgs j) {
+  const int ex = a.ext[0], ey = a.ext[1], ez = a.ext[2];
+  const int64_t total = static_cast<int64_t>(a.T) * ex * ey * ez;
+  const int64_t o = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (o >= total) return;
+  const int z = o % ez;
+  const int64_t col = o / ez;  // (t, x, y)
+  const float2 *h = j.H2 + col * a.nkz;
+  const float2 *w = a.twz + static_cast<size_t>(z) * a.nkzp;
+  float acc = 0.f;
+  for (int kz = 0; kz < a.nkz; ++kz) {
+    const float2 v = h[kz], c = w[kz];
+    acc = fmaf(v.x, c.x, fmaf(v.y, c.y, acc));
+  }
+  j.dg[o] = acc;
+}
+
+// grid (blocks, T), block 256: S_t = sum of dg_t over the corner block (FP64).
+__global__ void __launch_bounds__(kThreads) k_sum_dg(DevArgs a, AdjArgs j) {
+  __shared__ double red[kThreads / 32];
+  const int t = blockIdx.y;
+  const int64_t per = static_cast<int64_t>(a.ext[0]) * a.ext[1] * a.ext[2];
+  const float *d = j.dg + t * per;
+  double s = 0.0;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < per;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    s += d[i];
+  s = warp_sum(s);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double tot = 0.0;
+    for (int w = 0; w < kThreads / 32; ++w) tot += red[w];
+    atomicAdd(j.S + t, tot);
+  }
+}
+
+// One thread per entry: B-spline derivative gather of dL/dg, then dL/dx.
+__global__ void __launch_bounds__(kThreads) k_gather(DevArgs a, AdjArgs j) {
+  __shared__ float oc[9];
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (threadIdx.x < 9) oc[threadIdx.x] = a.geom[threadIdx.x];
+  __syncthreads();
+  if (e >= a.M) return;
+  const int at = a.entry_atom[e];
+  const int t = a.entry_type[e];
+  const float *p = a.xyz + 3ll * at;
+  const float x0 = p[0], y0 = p[1], z0 = p[2];
+  float r[3], w[3][4], dw[3][4];
+  int m[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    r[d] = grid_coord(oc + 3 * d, x0, y0, z0, a.n[d]);
+    m[d] = static_cast<int>(r[d]);
+    const float u = r[d] - static_cast<float>(m[d]);
+    cubic_weights(u, w[d]);
+    const float v = 1.0f - u;
+    dw[d][0] = -0.5f * v * v;
+    dw[d][1] = 1.5f * u * u - 2.0f * u;
+    dw[d][2] = -1.5f * u * u + u + 0.5f;
+    dw[d][3] = 0.5f * u * u;
+  }
+  const int P = a.order, nt = a.ntaps;
+  const int ex = a.ext[0], ey = a.ext[1], ez = a.ext[2];
+  const float *dgt = j.dg + static_cast<int64_t>(t) * ex * ey * ez;
+  float gr[3] = {0.f, 0.f, 0.f};
+  // taps on the corner block
+#pragma unroll
+  for (int o = 0; o < 4; ++o) {
+    if (o >= nt) break;
+    int x = m[0] - P + o;
+    if (x < 0) x += a.n[0];
+    if (x >= ex) continue;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      if (q >= nt) break;
+      int y = m[1] - P + q;
+      if (y < 0) y += a.n[1];
+      if (y >= ey) continue;
+#pragma unroll
+      for (int s = 0; s < 4; ++s) {
+        if (s >= nt) break;
+        int z = m[2] - P + s;
+        if (z < 0) z += a.n[2];
+        if (z >= ez) continue;
+        const float v = dgt[(static_cast<int64_t>(x) * ey + y) * ez + z];
+        gr[0] = fmaf(v, dw[0][o] * w[1][q] * w[2][s], gr[0]);
+        gr[1] = fmaf(v, w[0][o] * dw[1][q] * w[2][s], gr[1]);
+        gr[2] = fmaf(v, w[0][o] * w[1][q] * dw[2][s], gr[2]);
+      }
+    }
+  }
+  // the border mean: every border voxel carries (nn^3 Re G(0) - S_t) / count
+  const float cm = static_cast<float>((static_cast<double>(j.dcg[t]) - j.S[t]) / a.border_count);
+  float sx = 0.f, sy = 0.f, szb = 0.f, dsx = 0.f, dsy = 0.f, dszb = 0.f;
+#pragma unroll
+  for (int o = 0; o < 4; ++o) {
+    if (o < nt) {
+      sx += w[0][o];
+      sy += w[1][o];
+      dsx += dw[0][o];
+      dsy += dw[1][o];
+      int z = m[2] - P + o;
+      if (z < 0) z += a.n[2];
+      if (z <= a.dz || z >= a.n[2] - a.dz) {
+        szb += w[2][o];
+        dszb += dw[2][o];
+      }
+    }
+  }
+  gr[0] = fmaf(cm, dsx * sy * szb, gr[0]);
+  gr[1] = fmaf(cm, sx * dsy * szb, gr[1]);
+  gr[2] = fmaf(cm, sx * sy * dszb, gr[2]);
+  // r_d = n_d * (oc_d . x) + const
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const float g = gr[0] * a.n[0] * oc[c] + gr[1] * a.n[1] * oc[3 + c] + gr[2] * a.n[2] * oc[6 + c];
+    atomicAdd(j.grad + 3ll * at + c, g);
+  }
+}
+
 // grid (ceil(points/256)), block 256: nvt intensity sum over the batch's frames.
 __global__ void k_accumulate(DevArgs a, int nframes) {
   const int64_t npl = static_cast<int64_t>(a.nkz) * a.nky * a.nkx;
@@ -782,6 +1072,11 @@ struct SaxsPlan {
   Ring ring;
   float *d_geom0 = nullptr;
   double *d_tmp_hist = nullptr;
+  // adjoint buffers, allocated by the first saxs_backward
+  double *d_adj_dl = nullptr, *d_adj_S = nullptr;
+  float2 *d_adj_G = nullptr;
+  float *d_adj_dg = nullptr, *d_adj_dcg = nullptr;
+  size_t smem_xgrad = 0;
   int spread_ctas = 1;  // resident CTAs of the persistent spreading kernel
   int xc = 1;           // x values per shared-memory chunk in k_xdft_post
   bool profiling = false;
@@ -1337,6 +1632,92 @@ int histogram(SaxsPlan *pl, double *hist, double *nhist, cudaStream_t st) {
   return SAXS_OK;
 }
 
+
+int ensure_adjoint(SaxsPlan *pl) {
+  if (pl->d_adj_G) return SAXS_OK;
+  const DevArgs &a = pl->a;
+  int rc;
+  if ((rc = dalloc(pl, &pl->d_adj_dl, a.num_bins)) ||
+      (rc = dalloc(pl, &pl->d_adj_S, a.T)) ||
+      (rc = dalloc(pl, &pl->d_adj_dcg, a.T)) ||
+      (rc = dalloc(pl, &pl->d_adj_dg, static_cast<size_t>(a.T) * a.ext[0] * a.ext[1] * a.ext[2])) ||
+      (rc = dalloc(pl, &pl->d_adj_G, static_cast<size_t>(a.T) * a.nkz * a.nky * a.nkx)))
+    return rc;
+  CUDA_TRY(raise_smem_limit(k_xdft_grad));
+  return SAXS_OK;
+}
+
+int backward(SaxsPlan *pl, const float *xyz, const float *box, const double *dl, float *grad,
+             cudaStream_t st) {
+  if (!pl || !box || !dl || !grad || (!xyz && pl->a.M > 0)) return fail(SAXS_E_INVALID, "null argument");
+  if (int rc = check_box(box)) return rc;
+  if (int rc = ensure_adjoint(pl)) return rc;
+  DevArgs a = pl->a;
+  a.xyz = xyz;
+  a.frame_stride = 3ll * pl->p.natoms;
+  double *th = pl->d_tmp_hist, *tn = pl->d_tmp_hist + a.num_bins;
+  AdjArgs j{};
+  j.dl = pl->d_adj_dl;
+  j.nh = tn;
+  j.G = pl->d_adj_G;
+  j.H1 = a.Y;  // Y is consumed by k_xdft_grad before k_xadj overwrites it
+  j.H2 = a.Z;  // Z is consumed by k_ydft before k_yadj overwrites it
+  j.dg = pl->d_adj_dg;
+  j.S = pl->d_adj_S;
+  j.dcg = pl->d_adj_dcg;
+  j.grad = grad;
+  // geometry of the frame through the pinned ring, checked against the k-box
+  Ring &ring = pl->ring;
+  const int slot = ring.next;
+  ring.next = (ring.next + 1) % kRing;
+  CUDA_TRY(cudaEventSynchronize(ring.ev[slot]));
+  float *g = ring.host + static_cast<size_t>(slot) * pl->p.max_frames * kGeom;
+  frame_geometry(pl, box, g);
+  long long h[3];
+  saxs::kbox_halfwidths(g + 9, a.qcut, 1e-5, h);
+  for (int d = 0; d < 3; ++d)
+    if (!pl->full_axis[d] && h[d] > pl->half[d])
+      return fail(SAXS_E_RANGE, "frame box shrank beyond the planned k-box margin");
+  CUDA_TRY(cudaMemcpyAsync(const_cast<float *>(a.geom), g, sizeof(float) * kGeom,
+                           cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaEventRecord(ring.ev[slot], st));
+  CUDA_TRY(cudaMemcpyAsync(pl->d_adj_dl, dl, sizeof(double) * a.num_bins, cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaMemsetAsync(a.counts, 0, sizeof(int) * a.nbins, st));
+  CUDA_TRY(cudaMemsetAsync(a.border, 0, sizeof(double) * a.T, st));
+  CUDA_TRY(cudaMemsetAsync(th, 0, 2 * sizeof(double) * a.num_bins, st));
+  CUDA_TRY(cudaMemsetAsync(pl->d_adj_S, 0, sizeof(double) * a.T, st));
+  CUDA_TRY(cudaMemsetAsync(grad, 0, sizeof(float) * 3 * static_cast<size_t>(pl->p.natoms), st));
+  // recompute the frame's per-type transforms (nothing is kept from the forward)
+  if (a.M > 0) {
+    dim3 gb((a.M + kThreads - 1) / kThreads, 1);
+    k_bin_atoms<<<gb, kThreads, pl->smem_bin, st>>>(a);
+    k_scan<<<1, 1024, 0, st>>>(a);
+    k_scatter_atoms<<<gb, kThreads, 0, st>>>(a);
+  } else {
+    CUDA_TRY(cudaMemsetAsync(a.offsets, 0, sizeof(int) * (a.nbins + 1), st));
+  }
+  const int items = a.stiles[0] * a.stiles[1] * a.T;
+  k_spread_zdft<<<std::max(1, std::min(items, pl->spread_ctas)), kThreads, pl->smem_spread, st>>>(
+      a, items);
+  dim3 gy((a.ext[0] + kYRows - 1) / kYRows, a.nkz, a.T);
+  k_ydft<<<gy, kThreads, pl->smem_ydft, st>>>(a);
+  dim3 gx((a.nky + kXRows - 1) / kXRows, a.nkz, 1);
+  k_xdft_post<<<gx, kThreads, pl->smem_xdft, st>>>(a, pl->xc);
+  k_hist<float><<<dim3(a.nkz, 1), kThreads, pl->smem_hist, st>>>(a, a.ibox, a.geom, kGeom, 1.0, th, tn);
+  if (int rc = launch_check("backward recompute")) return rc;
+  // adjoint passes
+  k_xdft_grad<<<gx, kThreads, pl->smem_xdft, st>>>(a, j, pl->xc);
+  const int64_t n1 = static_cast<int64_t>(a.T) * a.nkz * a.ext[0] * a.nky;
+  k_xadj<<<static_cast<unsigned>((n1 + kThreads - 1) / kThreads), kThreads, 0, st>>>(a, j);
+  const int64_t n2 = static_cast<int64_t>(a.T) * a.ext[0] * a.ext[1] * a.nkz;
+  k_yadj<<<static_cast<unsigned>((n2 + kThreads - 1) / kThreads), kThreads, 0, st>>>(a, j);
+  const int64_t n3 = static_cast<int64_t>(a.T) * a.ext[0] * a.ext[1] * a.ext[2];
+  k_zadj<<<static_cast<unsigned>((n3 + kThreads - 1) / kThreads), kThreads, 0, st>>>(a, j);
+  k_sum_dg<<<dim3(64, a.T), kThreads, 0, st>>>(a, j);
+  if (a.M > 0) k_gather<<<(a.M + kThreads - 1) / kThreads, kThreads, 0, st>>>(a, j);
+  return launch_check("backward");
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -1537,8 +1918,16 @@ int saxs_debug_border_sums(SaxsPlan *pl, double *out, void *stream) {
   return SAXS_OK;
 }
 
-int saxs_backward(SaxsPlan *, const float *, const float *, const double *, float *, void *) {
-  return fail(SAXS_E_INVALID, "saxs_backward: not available in this build");
+int saxs_backward(SaxsPlan *plan, const float *xyz_dev, const float *box_host,
+                  const double *dl_dprofile_host, float *grad_xyz_dev, void *stream) {
+  g_err.clear();
+  int prev = 0;
+  cudaGetDevice(&prev);
+  if (plan && prev != plan->device) cudaSetDevice(plan->device);
+  const int rc = backward(plan, xyz_dev, box_host, dl_dprofile_host, grad_xyz_dev,
+                          static_cast<cudaStream_t>(stream));
+  if (plan && prev != plan->device) cudaSetDevice(prev);
+  return rc;
 }
 
 int saxs_profile_stages(void) { return kStages; }

@@ -254,6 +254,35 @@ class SaxsEngine:
             ctypes.c_void_p(self.stream.cuda_stream)))
         return out
 
+    def backward(self, xyz, box, dl_dprofile):
+        """dL/dxyz (natoms, 3) float32 CUDA tensor for one frame.
+
+        ``dl_dprofile`` holds dL/dI for every histogram bin (num_bins values;
+        bins the profile does not report carry 0).  The frame's grids are
+        recomputed from ``xyz``; the plan's accumulators are not touched.
+        """
+        torch = self._torch
+        x = xyz.detach()
+        if x.dim() == 3:
+            x = x[0]
+        if x.dtype != torch.float32 or x.device != self.device or not x.is_contiguous():
+            x = x.to(self.device, torch.float32).contiguous()
+        if x.shape[0] < self.natoms:
+            raise ValueError("xyz must have natoms rows")
+        dl = np.ascontiguousarray(np.asarray(dl_dprofile, dtype=np.float64).reshape(-1))
+        if dl.size != self.info.num_bins:
+            raise ValueError(f"dl_dprofile must have {self.info.num_bins} entries")
+        b = np.ascontiguousarray(np.asarray(box, dtype=np.float32).reshape(9))
+        grad = torch.empty((x.shape[0], 3), dtype=torch.float32, device=self.device)
+        if x.shape[0] > self.natoms:
+            grad.zero_()
+        _native.check(self.lib.saxs_backward(
+            self._plan, ctypes.c_void_p(x.data_ptr()), b.ctypes.data_as(_native.c_float_p),
+            dl.ctypes.data_as(_native.c_double_p), ctypes.c_void_p(grad.data_ptr()),
+            ctypes.c_void_p(self.stream.cuda_stream)))
+        torch.cuda.current_stream(self.device).wait_stream(self.stream)
+        return grad
+
     def profile_enable(self, on: bool = True) -> None:
         """Time every kernel of ``forward`` with CUDA events on the engine stream."""
         _native.check(self.lib.saxs_profile_enable(self._plan, int(bool(on))))

@@ -1,0 +1,85 @@
+"""The hand-written CUDA adjoint vs the FP64 torch oracle gradient (GPU).
+
+Loss: sum over reported bins of (log I(q) - log I_target(q))^2 (the refinement
+workload's loss).  The oracle gradient is itself checked against central finite
+differences in tests/test_gradient_oracle.py.  Tolerance: relative L2 error of
+the whole (N, 3) gradient below GRAD_RTOL, and every component within
+GRAD_RTOL of the largest component (FP32 forward vs FP64 oracle).
+"""
+import numpy as np
+import pytest
+import torch
+
+from oracle import saxs_oracle as O
+from oracle import torch_oracle as TO
+from pycusaxs_b200 import SaxsEngine
+from pycusaxs_b200.autograd import saxs_profile
+from pycusaxs_b200.synthetic import System, cubic_system
+
+pytestmark = pytest.mark.gpu
+
+GRAD_RTOL = 2e-3
+
+
+def _compare(s, grid, sigma=2.0, qcut=0.8, order=4, seed=0):
+    names = sorted({str(e) for e in s.elements}, key=lambda k: k.encode())
+    ff = O.load_form_factors()
+    plan = O.OraclePlan(grid=grid, types=names, coeffs=np.stack([ff[k] for k in names]),
+                        box0=s.box, sigma=sigma, qcut=qcut, order=order)
+    toa = s.type_of_atom(names)
+    x64 = torch.tensor(s.positions.astype(np.float64), requires_grad=True)
+    prof_o, _ = TO.profile(plan, x64, toa, s.box)
+    sel = prof_o.detach() > 0
+    target = prof_o.detach() * (1 + 0.05 * torch.cos(torch.arange(len(prof_o), dtype=torch.float64)))
+    ((torch.log(prof_o[sel]) - torch.log(target[sel])) ** 2).sum().backward()
+    g_ref = x64.grad.numpy()
+
+    eng = SaxsEngine(grid, s.atom_index(), s.natoms, s.box, scale_factor=sigma, qcut=qcut,
+                     order=order)
+    xg = torch.tensor(s.positions, device=eng.device, requires_grad=True)
+    prof = saxs_profile(xg, eng, s.box)
+    sel_g = sel.to(prof.device)
+    tg = target.to(prof.device)
+    ((torch.log(prof[sel_g]) - torch.log(tg[sel_g])) ** 2).sum().backward()
+    g = xg.grad.double().cpu().numpy()
+    eng.close()
+    rel_l2 = np.linalg.norm(g - g_ref) / np.linalg.norm(g_ref)
+    worst = np.abs(g - g_ref).max() / np.abs(g_ref).max()
+    print(f"gradient vs FP64 oracle: relative L2 {rel_l2:.2e}, worst component {worst:.2e}")
+    assert rel_l2 < GRAD_RTOL and worst < GRAD_RTOL, (rel_l2, worst)
+    return rel_l2, worst
+
+
+def test_adjoint_small_cubic(cuda):
+    _compare(cubic_system(800, 30.0, seed=3), (16, 16, 16))
+
+
+def test_adjoint_grid32_six_elements(cuda):
+    _compare(cubic_system(4000, 40.0, seed=4), (32, 32, 32), qcut=0.7)
+
+
+def test_adjoint_order2_and_upper_triangular_box(cuda):
+    rng = np.random.default_rng(5)
+    box = np.array([[36.0, 4.0, -3.0], [0.0, 40.0, 5.0], [0.0, 0.0, 44.0]], np.float32)
+    pos = (rng.uniform(0, 1, (2500, 3)) @ box).astype(np.float32)
+    el = np.array(["C", "O", "N"], dtype=object)[rng.choice(3, 2500)]
+    _compare(System(el, pos, box), (24, 24, 24), order=2, qcut=0.7)
+
+
+def test_adjoint_refinement_sized_system(cuda):
+    # 50k atoms in a 10 nm box on grid 64 (128^3 supercell)
+    _compare(cubic_system(50_000, 100.0, seed=6), (64, 64, 64), qcut=0.5)
+
+
+def test_profile_forward_equals_engine_histogram(cuda):
+    s = cubic_system(3000, 36.0, seed=7)
+    eng = SaxsEngine((32, 32, 32), s.atom_index(), s.natoms, s.box, scale_factor=2.0, qcut=0.7)
+    x = torch.tensor(s.positions, device=eng.device)
+    prof = saxs_profile(x, eng, s.box).cpu().numpy()
+    eng.forward(x, s.box)
+    h, n = eng.histogram()
+    sel = n > 0
+    sel[0] = False
+    np.testing.assert_allclose(prof[sel], h[sel] / n[sel], rtol=1e-6)
+    assert np.all(prof[~sel] == 0)
+    eng.close()
