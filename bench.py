@@ -347,7 +347,7 @@ def refinement(steps: int = 100) -> dict:
 
     fwd_ms = timed(fwd, 10)
     fb_ms = timed(fwd_bwd, 10)
-    opt = torch.optim.Adam([x], lr=0.01)
+    opt = torch.optim.Adam([x], lr=3e-4)
     l0 = float(loss_fn().detach())
     torch.cuda.synchronize()
     t0 = time.perf_counter()

@@ -114,15 +114,15 @@ int saxs_debug_kbox_intensity(SaxsPlan *plan, float *out_host, void *stream);
 /* Per-type FP64 z-border sums of the last frame (saxsDeviceKernels.cu:446-465). */
 int saxs_debug_border_sums(SaxsPlan *plan, double *out_host, void *stream);
 
-/* Reverse-mode derivative of a profile loss with respect to the positions of one
- * frame.  Given dL/dI for each histogram bin (num_bins doubles, host; bins that
- * the profile does not report carry 0), recompute the frame's per-type grids
- * and write dL/dxyz (3*natoms float32, device, overwritten) for the frame's
- * positions xyz_dev with box box_host.  npt semantics of a single frame
- * (I_bin = hist/nhist).  No reference counterpart: the reference has no
- * derivative. */
+/* Reverse-mode derivative with respect to the positions of one frame.  Given
+ * dL/dhist for each histogram bin of that frame (num_bins doubles, host memory;
+ * the reported profile is hist/nhist, so dL/dhist = dL/dI(q) / nhist and 0 for
+ * bins that are not reported), recompute the frame's transforms and write dL/dxyz
+ * (3*natoms float32, device, overwritten) for positions xyz_dev with box
+ * box_host.  The plan's accumulators are not touched; its intermediate buffers
+ * are.  No reference counterpart: the reference has no derivative. */
 int saxs_backward(SaxsPlan *plan, const float *xyz_dev, const float *box_host,
-                  const double *dl_dprofile_host, float *grad_xyz_dev, void *stream);
+                  const double *dl_dhist_host, float *grad_xyz_dev, void *stream);
 
 /* ---- allocation-free single frame (no counterpart in the reference) ----
  *

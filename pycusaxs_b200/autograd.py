@@ -28,6 +28,7 @@ class _SaxsProfile(torch.autograd.Function):
         prof = np.where(n > 0, h / np.where(n > 0, n, 1.0), 0.0)
         prof[0] = 0.0
         ctx.engine = engine
+        ctx.nhist = n
         ctx.box = np.asarray(box, dtype=np.float32)
         ctx.save_for_backward(xyz)
         return torch.from_numpy(prof).to(xyz.device)
@@ -35,7 +36,10 @@ class _SaxsProfile(torch.autograd.Function):
     @staticmethod
     def backward(ctx, grad_out):
         (xyz,) = ctx.saved_tensors
-        dl = grad_out.detach().to(torch.float64).cpu().numpy()
+        dprof = grad_out.detach().to(torch.float64).cpu().numpy()
+        n = ctx.nhist
+        dl = np.where(n > 0, dprof / np.where(n > 0, n, 1.0), 0.0)
+        dl[0] = 0.0
         g = ctx.engine.backward(xyz.detach().to(ctx.engine.device, torch.float32).contiguous(),
                                 ctx.box, dl)
         return g.to(device=xyz.device, dtype=xyz.dtype), None, None

@@ -739,11 +739,13 @@ __global__ void __launch_bounds__(kThreads)
 
 // Extra device buffers of the adjoint, allocated on first use.
 struct AdjArgs {
-  const double *dl;   // [num_bins] dL/d profile
-  const double *nh;   // [num_bins] the frame's bin counts
+  const double *dl;   // [num_bins] dL/d hist
   float2 *G;          // [T][nkz][nky][nkx] dL/dF_t (Re + i Im)
-  float2 *H1;         // [T][nkz][ex][nky]
-  float2 *H2;         // [T][ex][ey][nkz]
+  float2 *H1;         // [T][nkz][nky][ex]  (the layout of Y)
+  float2 *H2;         // [T][nkz][ex][ey]   (the layout of Z)
+  const float2 *twyT; // [nky][eyp]: exp(-2 pi i ky y / nny) transposed
+  const float2 *twzT; // [nkz][ezp]: exp(-2 pi i kz z / nnz) transposed
+  int eyp, ezp;
   float *dg;          // [T][ex][ey][ez] dL/dg' on the corner block
   double *S;          // [T] sum of dg over the corner block
   float *dcg;         // [T] nn^3 * Re G_t(k = 0)
@@ -756,8 +758,7 @@ __device__ __forceinline__ double bin_weight(const DevArgs &a, const AdjArgs &j,
   if (mw > a.qcut || a.dq <= 0.0f) return 0.0;
   const int h0 = static_cast<int>(mw / a.dq);
   if (h0 < 0 || h0 >= a.num_bins) return 0.0;
-  const double n = j.nh[h0];
-  return n != 0.0 ? j.dl[h0] / n : 0.0;
+  return j.dl[h0];
 }
 
 // grid (ceil(nky/4), nkz), block 256: x-axis DFT of the recomputed Y rows, then
@@ -860,16 +861,15 @@ __global__ void __launch_bounds__(kThreads) k_xdft_grad(DevArgs a, AdjArgs j, in
   }
 }
 
-// H1[t][kz][x][ky] = sum_kx G[t][kz][ky][kx] conj(exp(-2 pi i kx x / nnx)); thread per output.
+// H1[t][kz][ky][x] = sum_kx G[t][kz][ky][kx] conj(exp(-2 pi i kx x / nnx)); thread per output.
 __global__ void k_xadj(DevArgs a, AdjArgs j) {
   const int ex = a.ext[0];
-  const int64_t total = static_cast<int64_t>(a.T) * a.nkz * ex * a.nky;
+  const int64_t total = static_cast<int64_t>(a.T) * a.nkz * a.nky * ex;
   const int64_t o = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (o >= total) return;
-  const int ky = o % a.nky;
-  const int x = (o / a.nky) % ex;
-  const int64_t tk = o / (static_cast<int64_t>(a.nky) * ex);
-  const float2 *g = j.G + (tk * a.nky + ky) * a.nkx;
+  const int x = o % ex;
+  const int64_t row = o / ex;  // (t, kz, ky)
+  const float2 *g = j.G + row * a.nkx;
   const float2 *w = a.twx + static_cast<size_t>(x) * a.nkxp;
   float2 acc = make_float2(0.f, 0.f);
   for (int kx = 0; kx < a.nkx; ++kx) {
@@ -880,28 +880,84 @@ __global__ void k_xadj(DevArgs a, AdjArgs j) {
   j.H1[o] = acc;
 }
 
-// H2[t][x][y][kz] = sum_ky H1[t][kz][x][ky] conj(exp(-2 pi i ky y / nny)); thread per output.
+// H2[t][kz][x][y] = sum_ky H1[t][kz][ky][x] conj(exp(-2 pi i ky y / nny)); thread per output
+// (used when the tiled version does not fit shared memory).
 __global__ void k_yadj(DevArgs a, AdjArgs j) {
   const int ex = a.ext[0], ey = a.ext[1];
-  const int64_t total = static_cast<int64_t>(a.T) * ex * ey * a.nkz;
+  const int64_t total = static_cast<int64_t>(a.T) * a.nkz * ex * ey;
   const int64_t o = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (o >= total) return;
-  const int kz = o % a.nkz;
-  const int y = (o / a.nkz) % ey;
-  const int x = (o / (static_cast<int64_t>(a.nkz) * ey)) % ex;
-  const int t = static_cast<int>(o / (static_cast<int64_t>(a.nkz) * ey * ex));
-  const float2 *h = j.H1 + ((static_cast<int64_t>(t) * a.nkz + kz) * ex + x) * a.nky;
+  const int y = o % ey;
+  const int x = (o / ey) % ex;
+  const int64_t tk = o / (static_cast<int64_t>(ey) * ex);
+  const float2 *h = j.H1 + tk * a.nky * ex + x;
   const float2 *w = a.twy + static_cast<size_t>(y) * a.nkyp;
   float2 acc = make_float2(0.f, 0.f);
   for (int ky = 0; ky < a.nky; ++ky) {
-    const float2 v = h[ky], c = w[ky];
+    const float2 v = h[static_cast<int64_t>(ky) * ex], c = w[ky];
     acc.x = fmaf(v.x, c.x, fmaf(v.y, c.y, acc.x));
     acc.y = fmaf(v.y, c.x, fmaf(-v.x, c.y, acc.y));
   }
   j.H2[o] = acc;
 }
 
-// dg[t][x][y][z] = Re sum_kz H2[t][x][y][kz] conj(exp(-2 pi i kz z / nnz)); thread per output.
+// grid (ceil(ex/64), nkz, T), block 256: the same contraction in shared-memory tiles.
+// Thread: 2 x rows x 16 y values.  Dynamic smem: H1 tile nky x 64 | twyT nky x eyp (float2).
+__global__ void __launch_bounds__(kThreads) k_yadj_tile(DevArgs a, AdjArgs j) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  float2 *h1 = reinterpret_cast<float2 *>(smem);
+  float2 *tw = h1 + static_cast<size_t>(a.nky) * 64;
+  const int t = blockIdx.z, kz = blockIdx.y, xb = blockIdx.x * 64;
+  const int ex = a.ext[0], ey = a.ext[1];
+  const int tid = threadIdx.x, lane = tid & 31, yg = tid >> 5;
+  const float2 *src = j.H1 + (static_cast<int64_t>(t) * a.nkz + kz) * a.nky * ex;
+  for (int i = tid; i < a.nky * 64; i += blockDim.x) {
+    const int ky = i / 64, xl = i % 64;
+    h1[i] = (xb + xl < ex) ? src[static_cast<int64_t>(ky) * ex + xb + xl] : make_float2(0.f, 0.f);
+  }
+  {
+    const float4 *s4 = reinterpret_cast<const float4 *>(j.twyT);
+    float4 *d4 = reinterpret_cast<float4 *>(tw);
+    const int n4 = a.nky * j.eyp / 2;
+    for (int i = tid; i < n4; i += blockDim.x) d4[i] = s4[i];
+  }
+  __syncthreads();
+  float2 *dst = j.H2 + (static_cast<int64_t>(t) * a.nkz + kz) * ex * ey;
+  const int x = xb + 2 * lane;
+  for (int yb = yg * 16; yb < ey; yb += 128) {
+    float2 acc0[16], acc1[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) acc0[q] = acc1[q] = make_float2(0.f, 0.f);
+    for (int ky = 0; ky < a.nky; ++ky) {
+      const float4 hv = *reinterpret_cast<const float4 *>(h1 + ky * 64 + 2 * lane);
+      const float4 *w4 = reinterpret_cast<const float4 *>(tw + static_cast<size_t>(ky) * j.eyp + yb);
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const float4 w = w4[q];
+        // h * conj(w): re = hr wr + hi wi, im = hi wr - hr wi
+        acc0[2 * q].x = fmaf(hv.x, w.x, fmaf(hv.y, w.y, acc0[2 * q].x));
+        acc0[2 * q].y = fmaf(hv.y, w.x, fmaf(-hv.x, w.y, acc0[2 * q].y));
+        acc1[2 * q].x = fmaf(hv.z, w.x, fmaf(hv.w, w.y, acc1[2 * q].x));
+        acc1[2 * q].y = fmaf(hv.w, w.x, fmaf(-hv.z, w.y, acc1[2 * q].y));
+        acc0[2 * q + 1].x = fmaf(hv.x, w.z, fmaf(hv.y, w.w, acc0[2 * q + 1].x));
+        acc0[2 * q + 1].y = fmaf(hv.y, w.z, fmaf(-hv.x, w.w, acc0[2 * q + 1].y));
+        acc1[2 * q + 1].x = fmaf(hv.z, w.z, fmaf(hv.w, w.w, acc1[2 * q + 1].x));
+        acc1[2 * q + 1].y = fmaf(hv.w, w.z, fmaf(-hv.z, w.w, acc1[2 * q + 1].y));
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      const int y = yb + q;
+      if (y < ey) {
+        if (x < ex) dst[static_cast<int64_t>(x) * ey + y] = acc0[q];
+        if (x + 1 < ex) dst[static_cast<int64_t>(x + 1) * ey + y] = acc1[q];
+      }
+    }
+  }
+}
+
+// dg[t][x][y][z] = Re sum_kz H2[t][kz][x][y] conj(exp(-2 pi i kz z / nnz)); thread per output
+// (used when the fused tiled version does not fit shared memory).
 __global__ void k_zadj(DevArgs a, AdjArgs j) {
   const int ex = a.ext[0], ey = a.ext[1], ez = a.ext[2];
   const int64_t total = static_cast<int64_t>(a.T) * ex * ey * ez;
@@ -909,11 +965,13 @@ __global__ void k_zadj(DevArgs a, AdjArgs j) {
   if (o >= total) return;
   const int z = o % ez;
   const int64_t col = o / ez;  // (t, x, y)
-  const float2 *h = j.H2 + col * a.nkz;
+  const int64_t xy = col % (static_cast<int64_t>(ex) * ey);
+  const int t = static_cast<int>(col / (static_cast<int64_t>(ex) * ey));
+  const float2 *h = j.H2 + static_cast<int64_t>(t) * a.nkz * ex * ey + xy;
   const float2 *w = a.twz + static_cast<size_t>(z) * a.nkzp;
   float acc = 0.f;
   for (int kz = 0; kz < a.nkz; ++kz) {
-    const float2 v = h[kz], c = w[kz];
+    const float2 v = h[static_cast<int64_t>(kz) * ex * ey], c = w[kz];
     acc = fmaf(v.x, c.x, fmaf(v.y, c.y, acc));
   }
   j.dg[o] = acc;
@@ -1023,6 +1081,200 @@ __global__ void __launch_bounds__(kThreads) k_gather(DevArgs a, AdjArgs j) {
   }
 }
 
+__device__ __forceinline__ void spline_and_derivative(float u, float w[4], float dw[4]) {
+  cubic_weights(u, w);
+  const float v = 1.0f - u;
+  dw[0] = -0.5f * v * v;
+  dw[1] = 1.5f * u * u - 2.0f * u;
+  dw[2] = -1.5f * u * u + u + 0.5f;
+  dw[3] = 0.5f * u * u;
+}
+
+// dL/dr (grid units) -> dL/dxyz of the atom: r_d = n_d (oc_d . x) + const.
+__device__ __forceinline__ void add_position_gradient(const DevArgs &a, const float *oc,
+                                                      const float gr[3], float *g) {
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const float v = gr[0] * a.n[0] * oc[c] + gr[1] * a.n[1] * oc[3 + c] + gr[2] * a.n[2] * oc[6 + c];
+    atomicAdd(g + c, v);
+  }
+}
+
+// Persistent over (type, 8x8 column tile) of frame 0; block 256.  The z-axis
+// adjoint of the tile's 64 columns into shared memory (a small GEMM: 4 columns x
+// 8 z per thread), its sum into S_t, then the B-spline derivative gather of every
+// atom whose stencil reaches the tile.  Dynamic smem:
+//   twzT nkz x ezp float2 | H2 columns nkz x 64 float2 | dg tile ez x 64 float.
+__global__ void __launch_bounds__(kThreads) k_zadj_gather(DevArgs a, AdjArgs j, int items) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int ex = a.ext[0], ey = a.ext[1], ez = a.ext[2];
+  float2 *tw = reinterpret_cast<float2 *>(smem);
+  float2 *hz = tw + static_cast<size_t>(a.nkz) * j.ezp;
+  float *dgt = reinterpret_cast<float *>(hz + static_cast<size_t>(a.nkz) * kCols);
+  __shared__ TileAtoms ta;
+  __shared__ float oc[9];
+  __shared__ double red[kThreads / 32];
+  const int tid = threadIdx.x;
+  {
+    const float4 *s4 = reinterpret_cast<const float4 *>(j.twzT);
+    float4 *d4 = reinterpret_cast<float4 *>(tw);
+    const int n4 = a.nkz * j.ezp / 2;
+    for (int i = tid; i < n4; i += blockDim.x) d4[i] = s4[i];
+  }
+  if (tid < 9) oc[tid] = a.geom[tid];
+  const int st = a.stiles[0] * a.stiles[1];
+  const int cg = tid % 16, zg = tid / 16;
+  const float4 *hz4 = reinterpret_cast<const float4 *>(hz);
+  const float4 *tw4 = reinterpret_cast<const float4 *>(tw);
+  const float4 *rec = a.rec;
+  const int P = a.order, nt = a.ntaps, nz = a.n[2];
+  for (int w = blockIdx.x; w < items; w += gridDim.x) {
+    const int t = w / st, tl = w % st;
+    const int x0 = (tl % a.stiles[0]) * kTile, y0 = (tl / a.stiles[0]) * kTile;
+    const int cw = min(kTile, ex - x0), ch = min(kTile, ey - y0);
+    const float2 *src = j.H2 + static_cast<int64_t>(t) * a.nkz * ex * ey;
+    for (int i = tid; i < a.nkz * kCols; i += blockDim.x) {
+      const int kz = i / kCols, col = i % kCols, lx = col / kTile, ly = col % kTile;
+      hz[i] = (lx < cw && ly < ch)
+                  ? src[(static_cast<int64_t>(kz) * ex + x0 + lx) * ey + y0 + ly]
+                  : make_float2(0.f, 0.f);
+    }
+    tile_atom_ranges(a, ta, 0, t, x0, y0);
+    __syncthreads();
+    double part = 0.0;
+    for (int zb = zg * 8; zb < ez; zb += 128) {
+      float acc[4][8];
+#pragma unroll
+      for (int c = 0; c < 4; ++c)
+#pragma unroll
+        for (int q = 0; q < 8; ++q) acc[c][q] = 0.f;
+      for (int kz = 0; kz < a.nkz; ++kz) {
+        const float4 h01 = hz4[kz * (kCols / 2) + 2 * cg];
+        const float4 h23 = hz4[kz * (kCols / 2) + 2 * cg + 1];
+        const float hr[4] = {h01.x, h01.z, h23.x, h23.z};
+        const float hi[4] = {h01.y, h01.w, h23.y, h23.w};
+        const float4 *w4 = tw4 + (static_cast<size_t>(kz) * j.ezp + zb) / 2;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const float4 wv = w4[q];
+#pragma unroll
+          for (int c = 0; c < 4; ++c) {
+            acc[c][2 * q] = fmaf(hr[c], wv.x, fmaf(hi[c], wv.y, acc[c][2 * q]));
+            acc[c][2 * q + 1] = fmaf(hr[c], wv.z, fmaf(hi[c], wv.w, acc[c][2 * q + 1]));
+          }
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int z = zb + q;
+        if (z < ez) {
+          *reinterpret_cast<float4 *>(dgt + z * kCols + 4 * cg) =
+              make_float4(acc[0][q], acc[1][q], acc[2][q], acc[3][q]);
+#pragma unroll
+          for (int c = 0; c < 4; ++c) {
+            const int col = 4 * cg + c;
+            if ((col / kTile) < cw && (col % kTile) < ch) part += acc[c][q];
+          }
+        }
+      }
+    }
+    part = warp_sum(part);
+    if ((tid & 31) == 0) red[tid >> 5] = part;
+    __syncthreads();
+    if (tid == 0) {
+      double tot = 0.0;
+      for (int q = 0; q < kThreads / 32; ++q) tot += red[q];
+      if (tot != 0.0) atomicAdd(j.S + t, tot);
+    }
+    // gather dL/dg' at the taps of every atom whose stencil reaches this tile
+    const int total = ta.cum[ta.nb];
+    for (int k = tid; k < total; k += blockDim.x) {
+      int jb = 0;
+      while (k >= ta.cum[jb + 1]) ++jb;
+      const float4 q = rec[ta.start[jb] + (k - ta.cum[jb])];
+      const int m0 = static_cast<int>(q.x), m1 = static_cast<int>(q.y), m2 = static_cast<int>(q.z);
+      float wx[4], wy[4], wz[4], dx[4], dy[4], dz[4];
+      spline_and_derivative(q.x - static_cast<float>(m0), wx, dx);
+      spline_and_derivative(q.y - static_cast<float>(m1), wy, dy);
+      spline_and_derivative(q.z - static_cast<float>(m2), wz, dz);
+      float gr[3] = {0.f, 0.f, 0.f};
+      bool hit = false;
+#pragma unroll
+      for (int o = 0; o < 4; ++o) {
+        if (o >= nt) break;
+        int x = m0 - P + o;
+        if (x < 0) x += a.n[0];
+        const int lx = x - x0;
+        if (static_cast<unsigned>(lx) >= static_cast<unsigned>(cw)) continue;
+#pragma unroll
+        for (int p = 0; p < 4; ++p) {
+          if (p >= nt) break;
+          int y = m1 - P + p;
+          if (y < 0) y += a.n[1];
+          const int ly = y - y0;
+          if (static_cast<unsigned>(ly) >= static_cast<unsigned>(ch)) continue;
+          const float *colp = dgt + lx * kTile + ly;
+#pragma unroll
+          for (int r = 0; r < 4; ++r) {
+            if (r >= nt) break;
+            int z = m2 - P + r;
+            if (z < 0) z += nz;
+            if (z >= ez) continue;
+            const float v = colp[z * kCols];
+            gr[0] = fmaf(v, dx[o] * wy[p] * wz[r], gr[0]);
+            gr[1] = fmaf(v, wx[o] * dy[p] * wz[r], gr[1]);
+            gr[2] = fmaf(v, wx[o] * wy[p] * dz[r], gr[2]);
+            hit = true;
+          }
+        }
+      }
+      if (hit) {
+        const int e = __float_as_int(q.w);
+        add_position_gradient(a, oc, gr, j.grad + 3ll * a.entry_atom[e]);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// One thread per sorted record of frame 0: the border-mean part of dL/dx,
+// (nn^3 Re G_t(0) - S_t) / count per border voxel.
+__global__ void __launch_bounds__(kThreads) k_mean_grad(DevArgs a, AdjArgs j) {
+  __shared__ float oc[9];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (threadIdx.x < 9) oc[threadIdx.x] = a.geom[threadIdx.x];
+  __syncthreads();
+  if (i >= a.M) return;
+  const float4 q = a.rec[i];
+  const int e = __float_as_int(q.w);
+  const int t = a.entry_type[e];
+  const float cm = static_cast<float>((static_cast<double>(j.dcg[t]) - j.S[t]) / a.border_count);
+  if (cm == 0.0f) return;
+  const int m[3] = {static_cast<int>(q.x), static_cast<int>(q.y), static_cast<int>(q.z)};
+  float w[3][4], dw[3][4];
+  spline_and_derivative(q.x - static_cast<float>(m[0]), w[0], dw[0]);
+  spline_and_derivative(q.y - static_cast<float>(m[1]), w[1], dw[1]);
+  spline_and_derivative(q.z - static_cast<float>(m[2]), w[2], dw[2]);
+  float sx = 0.f, sy = 0.f, szb = 0.f, dsx = 0.f, dsy = 0.f, dszb = 0.f;
+#pragma unroll
+  for (int o = 0; o < 4; ++o) {
+    if (o < a.ntaps) {
+      sx += w[0][o];
+      sy += w[1][o];
+      dsx += dw[0][o];
+      dsy += dw[1][o];
+      int z = m[2] - a.order + o;
+      if (z < 0) z += a.n[2];
+      if (z <= a.dz || z >= a.n[2] - a.dz) {
+        szb += w[2][o];
+        dszb += dw[2][o];
+      }
+    }
+  }
+  const float gr[3] = {cm * dsx * sy * szb, cm * sx * dsy * szb, cm * sx * sy * dszb};
+  add_position_gradient(a, oc, gr, j.grad + 3ll * a.entry_atom[e]);
+}
+
 // grid (ceil(points/256)), block 256: nvt intensity sum over the batch's frames.
 __global__ void k_accumulate(DevArgs a, int nframes) {
   const int64_t npl = static_cast<int64_t>(a.nkz) * a.nky * a.nkx;
@@ -1074,9 +1326,11 @@ struct SaxsPlan {
   double *d_tmp_hist = nullptr;
   // adjoint buffers, allocated by the first saxs_backward
   double *d_adj_dl = nullptr, *d_adj_S = nullptr;
-  float2 *d_adj_G = nullptr;
+  float2 *d_adj_G = nullptr, *d_adj_twyT = nullptr, *d_adj_twzT = nullptr;
   float *d_adj_dg = nullptr, *d_adj_dcg = nullptr;
-  size_t smem_xgrad = 0;
+  int adj_eyp = 0, adj_ezp = 0, zadj_ctas = 1;
+  bool adj_tiled_y = false, adj_tiled_z = false;
+  size_t smem_yadj = 0, smem_zadj = 0;
   int spread_ctas = 1;  // resident CTAs of the persistent spreading kernel
   int xc = 1;           // x values per shared-memory chunk in k_xdft_post
   bool profiling = false;
@@ -1636,14 +1890,46 @@ int histogram(SaxsPlan *pl, double *hist, double *nhist, cudaStream_t st) {
 int ensure_adjoint(SaxsPlan *pl) {
   if (pl->d_adj_G) return SAXS_OK;
   const DevArgs &a = pl->a;
+  const int ex = a.ext[0], ey = a.ext[1], ez = a.ext[2];
+  pl->adj_eyp = round_up(ey, 16);
+  pl->adj_ezp = round_up(ez, 8);
   int rc;
   if ((rc = dalloc(pl, &pl->d_adj_dl, a.num_bins)) ||
       (rc = dalloc(pl, &pl->d_adj_S, a.T)) ||
       (rc = dalloc(pl, &pl->d_adj_dcg, a.T)) ||
-      (rc = dalloc(pl, &pl->d_adj_dg, static_cast<size_t>(a.T) * a.ext[0] * a.ext[1] * a.ext[2])) ||
-      (rc = dalloc(pl, &pl->d_adj_G, static_cast<size_t>(a.T) * a.nkz * a.nky * a.nkx)))
+      (rc = dalloc(pl, &pl->d_adj_G, static_cast<size_t>(a.T) * a.nkz * a.nky * a.nkx)) ||
+      (rc = dalloc(pl, &pl->d_adj_twyT, static_cast<size_t>(a.nky) * pl->adj_eyp)) ||
+      (rc = dalloc(pl, &pl->d_adj_twzT, static_cast<size_t>(a.nkz) * pl->adj_ezp)))
     return rc;
+  std::vector<float2> ty(static_cast<size_t>(a.nky) * pl->adj_eyp, make_float2(0.f, 0.f));
+  for (int k = 0; k < a.nky; ++k)
+    for (int y = 0; y < ey; ++y)
+      saxs::twiddle(a.ky_lo + k, y, a.nn[1], &ty[k * pl->adj_eyp + y].x, &ty[k * pl->adj_eyp + y].y);
+  std::vector<float2> tz(static_cast<size_t>(a.nkz) * pl->adj_ezp, make_float2(0.f, 0.f));
+  for (int k = 0; k < a.nkz; ++k)
+    for (int z = 0; z < ez; ++z)
+      saxs::twiddle(k, z, a.nn[2], &tz[k * pl->adj_ezp + z].x, &tz[k * pl->adj_ezp + z].y);
+  CUDA_TRY(cudaMemcpy(pl->d_adj_twyT, ty.data(), sizeof(float2) * ty.size(), cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(pl->d_adj_twzT, tz.data(), sizeof(float2) * tz.size(), cudaMemcpyHostToDevice));
+  const size_t optin = static_cast<size_t>(optin_smem());
+  pl->smem_yadj = (static_cast<size_t>(a.nky) * 64 + static_cast<size_t>(a.nky) * pl->adj_eyp) *
+                  sizeof(float2);
+  pl->smem_zadj = (static_cast<size_t>(a.nkz) * pl->adj_ezp + static_cast<size_t>(a.nkz) * kCols) *
+                      sizeof(float2) + static_cast<size_t>(ez) * kCols * sizeof(float);
+  pl->adj_tiled_y = pl->smem_yadj + static_smem(k_yadj_tile) <= optin;
+  pl->adj_tiled_z = pl->smem_zadj + static_smem(k_zadj_gather) <= optin;
   CUDA_TRY(raise_smem_limit(k_xdft_grad));
+  if (pl->adj_tiled_y) CUDA_TRY(raise_smem_limit(k_yadj_tile));
+  if (pl->adj_tiled_z) {
+    CUDA_TRY(raise_smem_limit(k_zadj_gather));
+    int per_sm = 0, sms = 0;
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_zadj_gather, kThreads,
+                                                           pl->smem_zadj));
+    CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, pl->device));
+    pl->zadj_ctas = std::max(1, per_sm) * std::max(1, sms);
+  } else {
+    if ((rc = dalloc(pl, &pl->d_adj_dg, static_cast<size_t>(a.T) * ex * ey * ez))) return rc;
+  }
   return SAXS_OK;
 }
 
@@ -1655,13 +1941,15 @@ int backward(SaxsPlan *pl, const float *xyz, const float *box, const double *dl,
   DevArgs a = pl->a;
   a.xyz = xyz;
   a.frame_stride = 3ll * pl->p.natoms;
-  double *th = pl->d_tmp_hist, *tn = pl->d_tmp_hist + a.num_bins;
   AdjArgs j{};
   j.dl = pl->d_adj_dl;
-  j.nh = tn;
   j.G = pl->d_adj_G;
   j.H1 = a.Y;  // Y is consumed by k_xdft_grad before k_xadj overwrites it
-  j.H2 = a.Z;  // Z is consumed by k_ydft before k_yadj overwrites it
+  j.H2 = a.Z;  // Z is consumed by k_ydft before the y adjoint overwrites it
+  j.twyT = pl->d_adj_twyT;
+  j.twzT = pl->d_adj_twzT;
+  j.eyp = pl->adj_eyp;
+  j.ezp = pl->adj_ezp;
   j.dg = pl->d_adj_dg;
   j.S = pl->d_adj_S;
   j.dcg = pl->d_adj_dcg;
@@ -1684,10 +1972,9 @@ int backward(SaxsPlan *pl, const float *xyz, const float *box, const double *dl,
   CUDA_TRY(cudaMemcpyAsync(pl->d_adj_dl, dl, sizeof(double) * a.num_bins, cudaMemcpyHostToDevice, st));
   CUDA_TRY(cudaMemsetAsync(a.counts, 0, sizeof(int) * a.nbins, st));
   CUDA_TRY(cudaMemsetAsync(a.border, 0, sizeof(double) * a.T, st));
-  CUDA_TRY(cudaMemsetAsync(th, 0, 2 * sizeof(double) * a.num_bins, st));
   CUDA_TRY(cudaMemsetAsync(pl->d_adj_S, 0, sizeof(double) * a.T, st));
   CUDA_TRY(cudaMemsetAsync(grad, 0, sizeof(float) * 3 * static_cast<size_t>(pl->p.natoms), st));
-  // recompute the frame's per-type transforms (nothing is kept from the forward)
+  // recompute the frame's y-transformed planes (nothing is kept from the forward)
   if (a.M > 0) {
     dim3 gb((a.M + kThreads - 1) / kThreads, 1);
     k_bin_atoms<<<gb, kThreads, pl->smem_bin, st>>>(a);
@@ -1701,20 +1988,30 @@ int backward(SaxsPlan *pl, const float *xyz, const float *box, const double *dl,
       a, items);
   dim3 gy((a.ext[0] + kYRows - 1) / kYRows, a.nkz, a.T);
   k_ydft<<<gy, kThreads, pl->smem_ydft, st>>>(a);
-  dim3 gx((a.nky + kXRows - 1) / kXRows, a.nkz, 1);
-  k_xdft_post<<<gx, kThreads, pl->smem_xdft, st>>>(a, pl->xc);
-  k_hist<float><<<dim3(a.nkz, 1), kThreads, pl->smem_hist, st>>>(a, a.ibox, a.geom, kGeom, 1.0, th, tn);
   if (int rc = launch_check("backward recompute")) return rc;
   // adjoint passes
+  dim3 gx((a.nky + kXRows - 1) / kXRows, a.nkz, 1);
   k_xdft_grad<<<gx, kThreads, pl->smem_xdft, st>>>(a, j, pl->xc);
-  const int64_t n1 = static_cast<int64_t>(a.T) * a.nkz * a.ext[0] * a.nky;
+  const int64_t n1 = static_cast<int64_t>(a.T) * a.nkz * a.nky * a.ext[0];
   k_xadj<<<static_cast<unsigned>((n1 + kThreads - 1) / kThreads), kThreads, 0, st>>>(a, j);
-  const int64_t n2 = static_cast<int64_t>(a.T) * a.ext[0] * a.ext[1] * a.nkz;
-  k_yadj<<<static_cast<unsigned>((n2 + kThreads - 1) / kThreads), kThreads, 0, st>>>(a, j);
-  const int64_t n3 = static_cast<int64_t>(a.T) * a.ext[0] * a.ext[1] * a.ext[2];
-  k_zadj<<<static_cast<unsigned>((n3 + kThreads - 1) / kThreads), kThreads, 0, st>>>(a, j);
-  k_sum_dg<<<dim3(64, a.T), kThreads, 0, st>>>(a, j);
-  if (a.M > 0) k_gather<<<(a.M + kThreads - 1) / kThreads, kThreads, 0, st>>>(a, j);
+  if (pl->adj_tiled_y) {
+    dim3 gya((a.ext[0] + 63) / 64, a.nkz, a.T);
+    k_yadj_tile<<<gya, kThreads, pl->smem_yadj, st>>>(a, j);
+  } else {
+    const int64_t n2 = static_cast<int64_t>(a.T) * a.nkz * a.ext[0] * a.ext[1];
+    k_yadj<<<static_cast<unsigned>((n2 + kThreads - 1) / kThreads), kThreads, 0, st>>>(a, j);
+  }
+  if (pl->adj_tiled_z) {
+    k_zadj_gather<<<std::max(1, std::min(items, pl->zadj_ctas)), kThreads, pl->smem_zadj, st>>>(
+        a, j, items);
+  } else {
+    const int64_t n3 = static_cast<int64_t>(a.T) * a.ext[0] * a.ext[1] * a.ext[2];
+    k_zadj<<<static_cast<unsigned>((n3 + kThreads - 1) / kThreads), kThreads, 0, st>>>(a, j);
+    k_sum_dg<<<dim3(64, a.T), kThreads, 0, st>>>(a, j);
+    if (a.M > 0) k_gather<<<(a.M + kThreads - 1) / kThreads, kThreads, 0, st>>>(a, j);
+  }
+  if (pl->adj_tiled_z && a.M > 0)
+    k_mean_grad<<<(a.M + kThreads - 1) / kThreads, kThreads, 0, st>>>(a, j);
   return launch_check("backward");
 }
 

@@ -254,12 +254,13 @@ class SaxsEngine:
             ctypes.c_void_p(self.stream.cuda_stream)))
         return out
 
-    def backward(self, xyz, box, dl_dprofile):
+    def backward(self, xyz, box, dl_dhist):
         """dL/dxyz (natoms, 3) float32 CUDA tensor for one frame.
 
-        ``dl_dprofile`` holds dL/dI for every histogram bin (num_bins values;
-        bins the profile does not report carry 0).  The frame's grids are
-        recomputed from ``xyz``; the plan's accumulators are not touched.
+        ``dl_dhist`` holds dL/dhist for every histogram bin of the frame
+        (num_bins values; the profile is hist/nhist, so pass dL/dI / nhist, 0
+        for unreported bins).  The frame's transforms are recomputed from
+        ``xyz``; the plan's accumulators are not touched.
         """
         torch = self._torch
         x = xyz.detach()
@@ -269,9 +270,9 @@ class SaxsEngine:
             x = x.to(self.device, torch.float32).contiguous()
         if x.shape[0] < self.natoms:
             raise ValueError("xyz must have natoms rows")
-        dl = np.ascontiguousarray(np.asarray(dl_dprofile, dtype=np.float64).reshape(-1))
+        dl = np.ascontiguousarray(np.asarray(dl_dhist, dtype=np.float64).reshape(-1))
         if dl.size != self.info.num_bins:
-            raise ValueError(f"dl_dprofile must have {self.info.num_bins} entries")
+            raise ValueError(f"dl_dhist must have {self.info.num_bins} entries")
         b = np.ascontiguousarray(np.asarray(box, dtype=np.float32).reshape(9))
         grad = torch.empty((x.shape[0], 3), dtype=torch.float32, device=self.device)
         if x.shape[0] > self.natoms:

@@ -83,3 +83,21 @@ def test_profile_forward_equals_engine_histogram(cuda):
     np.testing.assert_allclose(prof[sel], h[sel] / n[sel], rtol=1e-6)
     assert np.all(prof[~sel] == 0)
     eng.close()
+
+
+def _line_system(n, lengths, seed):
+    rng = np.random.default_rng(seed)
+    L = np.asarray(lengths, np.float64)
+    pos = (rng.uniform(0, 1, (n, 3)) * L).astype(np.float32)
+    el = np.array(["C", "O"], dtype=object)[rng.choice(2, n)]
+    return System(el, pos, np.diag(L).astype(np.float32))
+
+
+def test_adjoint_long_z_axis_untiled_path(cuda):
+    # 253 kz values: the fused z-adjoint tile does not fit shared memory
+    _compare(_line_system(1200, (20.0, 20.0, 320.0), 61), (16, 16, 256), qcut=50.0)
+
+
+def test_adjoint_long_y_axis_untiled_path(cuda):
+    # a full ky range over a 256-long y axis: the tiled y-adjoint does not fit
+    _compare(_line_system(1200, (20.0, 320.0, 20.0), 62), (16, 256, 16), qcut=50.0)
