@@ -54,6 +54,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-multi", action="store_true")
     return ap.parse_args()
 
 
@@ -274,6 +275,9 @@ def bench_ours(args):
     adj = None
     if rank == 0 and world == 1 and not args.no_adjoint:
         adj = refinement()
+    multi = None
+    if rank == 0 and world == 1 and not args.no_multi:
+        multi = multi_system()
 
     launches = sum(v[1] for v in prof.values())
     out = {
@@ -287,7 +291,7 @@ def bench_ours(args):
                    "frames_per_step_per_gpu": FRAMES, "batch": B, "l2": "flushed between steps",
                    "kbox": [nkx, nky, nkz], "plain_path_frames_per_s": round(plain, 1) if plain else None,
                    "stage_share": stage_share, "parallelism": f"frames sharded over {world} GPU(s)",
-                   "adjoint": adj},
+                   "adjoint": adj, "multi_system": multi},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": ck,
         "gpu_launches": int(launches),
     }
@@ -364,6 +368,64 @@ def refinement(steps: int = 100) -> dict:
             "forward_ms": round(fwd_ms, 3), "forward_adjoint_ms": round(fb_ms, 3),
             "adjoint_over_forward": round(fb_ms / fwd_ms, 2),
             "adam_steps": steps, "adam_s": round(adam_s, 3), "loss_start": l0, "loss_end": l1}
+
+
+def multi_system(launches: int = 3) -> dict:
+    """64 independent systems (5k-200k atoms, grids 48-160), 8 frames each.
+
+    Batched: one CUDA-graph launch per grid bucket with every system on its own
+    branch (frames resident on the device).  Plain: the same 512 frames one at a
+    time through per-system engines.
+    """
+    import torch
+
+    from pycusaxs_b200 import SaxsEngine
+    from pycusaxs_b200.batch import BatchedSaxs
+    from pycusaxs_b200.synthetic import uneven_systems
+
+    systems = uneven_systems(64, frames=8, seed=11)
+    specs = [dict(atom_index=s.atom_index(), natoms=s.natoms, box0=s.box, grid=(g,) * 3,
+                  scale_factor=2.0, bin_size=0.002, qcut=0.5) for s, g in systems]
+    frames = [s.frames(0, 8) for s, _ in systems]
+    boxes = [np.stack([s.box] * 8) for s, _ in systems]
+    batch = BatchedSaxs(specs, frames=8)
+    batch.run(frames, boxes)
+    batch.synchronize()
+    for _ in range(2):
+        batch.run_resident(boxes)
+    batch.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(batch.stream)
+    for _ in range(launches):
+        batch.run_resident(boxes)
+    b.record(batch.stream)
+    b.synchronize()
+    nframes = 8 * len(systems)
+    batched = nframes * launches / (a.elapsed_time(b) / 1e3)
+    buckets = {str(k[0]): len(v) for k, v in batch.buckets.items()}
+    batch.close()
+    # plain per-frame path on the same frames
+    total = 0.0
+    for (s, g), x, bx in zip(systems, frames, boxes):
+        eng = SaxsEngine((g,) * 3, s.atom_index(), s.natoms, s.box, scale_factor=2.0,
+                         bin_size=0.002, qcut=0.5, max_frames=1)
+        xd = torch.from_numpy(x).to(eng.device)
+        eng.forward(xd[0], bx[0])
+        eng.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(eng.stream)
+        for k in range(8):
+            eng.forward(xd[k], bx[k])
+        e1.record(eng.stream)
+        e1.synchronize()
+        total += e0.elapsed_time(e1) / 1e3
+        eng.close()
+    plain = nframes / total
+    return {"workload": "64 systems, 5k-200k atoms (log-uniform), 100 atoms/nm^3, grids "
+                        "48-160 by box, scale 2, qcut 0.5/A, 8 frames each",
+            "atoms_total": int(sum(s.natoms for s, _ in systems)), "buckets": buckets,
+            "batched_frames_per_s": round(batched, 1), "plain_frames_per_s": round(plain, 1),
+            "speedup": round(batched / plain, 2)}
 
 
 def cpu_baseline(system) -> dict:

@@ -124,6 +124,28 @@ int saxs_debug_border_sums(SaxsPlan *plan, double *out_host, void *stream);
 int saxs_backward(SaxsPlan *plan, const float *xyz_dev, const float *box_host,
                   const double *dl_dhist_host, float *grad_xyz_dev, void *stream);
 
+/* ---- batched form: many systems and frames per CUDA graph launch (no counterpart
+ * in the reference, which processes one frame of one system per call) ---- */
+
+typedef struct SaxsGraph SaxsGraph;
+
+/* Capture the forwards of `count` distinct plans into one CUDA graph: plan i
+ * processes nframes[i] (<= its max_frames) frames from xyz_dev[i] (device,
+ * frame_stride[i] floats apart; the buffers are read at every launch), each
+ * plan's kernels on its own graph branch so that small systems run side by
+ * side.  Two executable copies alternate so the host can stage the next
+ * launch's geometry while the previous one runs. */
+int saxs_graph_create(SaxsPlan *const *plans, const float *const *xyz_dev,
+                      const int64_t *frame_stride, const int *nframes, int count,
+                      SaxsGraph **graph);
+
+/* One launch: boxes_host holds one 3x3 box per frame, plans in order and frames
+ * within a plan in order (sum of nframes boxes).  Each plan's accumulators grow
+ * as with saxs_forward.  Enqueued on `stream`. */
+int saxs_graph_launch(SaxsGraph *graph, const float *boxes_host, void *stream);
+
+void saxs_graph_destroy(SaxsGraph *graph);
+
 /* ---- allocation-free single frame (no counterpart in the reference) ----
  *
  * For hosts that cannot let the library allocate device memory while they run

@@ -25,6 +25,7 @@ SAXS_NVT = 1
 EXPORTED = (
     "saxs_plan_create", "saxs_plan_destroy", "saxs_plan_info", "saxs_forward", "saxs_histogram",
     "saxs_reset", "saxs_debug_kbox_intensity", "saxs_debug_border_sums", "saxs_backward",
+    "saxs_graph_create", "saxs_graph_launch", "saxs_graph_destroy",
     "saxs_forward_noalloc", "saxs_profile_stages", "saxs_profile_stage_name", "saxs_profile_enable", "saxs_profile_read",
     "saxs_closest_product", "saxs_cell_oc", "saxs_histogram_parameters", "saxs_bspline_moduli",
     "saxs_last_error", "saxs_version",
@@ -113,6 +114,14 @@ def load(path: os.PathLike | str | None = None) -> ctypes.CDLL:
     lib.saxs_debug_border_sums.restype = ctypes.c_int
     lib.saxs_backward.argtypes = [vp, vp, c_float_p, c_double_p, vp, vp]
     lib.saxs_backward.restype = ctypes.c_int
+    lib.saxs_graph_create.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(vp),
+                                      ctypes.POINTER(ctypes.c_int64), c_int_p, ctypes.c_int,
+                                      ctypes.POINTER(vp)]
+    lib.saxs_graph_create.restype = ctypes.c_int
+    lib.saxs_graph_launch.argtypes = [vp, c_float_p, vp]
+    lib.saxs_graph_launch.restype = ctypes.c_int
+    lib.saxs_graph_destroy.argtypes = [vp]
+    lib.saxs_graph_destroy.restype = None
     lib.saxs_forward_noalloc.argtypes = [vp, vp, c_float_p, vp, vp, vp]
     lib.saxs_forward_noalloc.restype = ctypes.c_int
     lib.saxs_profile_stages.argtypes = []

@@ -1768,42 +1768,15 @@ struct StageTimer {
   }
 };
 
-int forward(SaxsPlan *pl, const float *xyz, int64_t stride, int nframes, const float *boxes,
-            cudaStream_t st) {
-  if (!pl) return fail(SAXS_E_INVALID, "null plan");
-  if (nframes < 1 || nframes > pl->p.max_frames)
-    return fail(SAXS_E_INVALID, "nframes must be in [1, max_frames]");
-  if (!boxes || (!xyz && pl->a.M > 0)) return fail(SAXS_E_INVALID, "null positions or boxes");
-  if (stride < 3ll * pl->p.natoms) return fail(SAXS_E_INVALID, "frame stride smaller than 3*natoms");
-  DevArgs a = pl->a;
-  a.xyz = xyz;
-  a.frame_stride = stride;
-  // geometry of each frame, checked against the planned k-box
-  Ring &ring = pl->ring;
-  const int slot = ring.next;
-  ring.next = (ring.next + 1) % kRing;
-  CUDA_TRY(cudaEventSynchronize(ring.ev[slot]));
-  float *g = ring.host + static_cast<size_t>(slot) * pl->p.max_frames * kGeom;
-  for (int f = 0; f < nframes; ++f) {
-    const float *box = boxes + 9 * f;
-    if (int rc = check_box(box)) return rc;
-    frame_geometry(pl, box, g + f * kGeom);
-    long long h[3];
-    saxs::kbox_halfwidths(g + f * kGeom + 9, a.qcut, 1e-5, h);
-    for (int d = 0; d < 3; ++d) {
-      if (!pl->full_axis[d] && h[d] > pl->half[d])
-        return fail(SAXS_E_RANGE, "frame box shrank beyond the planned k-box margin; "
-                                  "create the plan with a larger box_margin");
-    }
-  }
-  CUDA_TRY(cudaMemcpyAsync(const_cast<float *>(a.geom), g, sizeof(float) * nframes * kGeom,
-                           cudaMemcpyHostToDevice, st));
-  CUDA_TRY(cudaEventRecord(ring.ev[slot], st));
+// Enqueue the memsets and kernels of one batch of `nframes` frames whose
+// geometry is already in (or queued for) a.geom.  Host work free, so that it can
+// be captured in a CUDA graph.
+int enqueue_batch(SaxsPlan *pl, const DevArgs &a, int nframes, cudaStream_t st, bool timed) {
   CUDA_TRY(cudaMemsetAsync(a.counts, 0, sizeof(int) * nframes * a.nbins, st));
   CUDA_TRY(cudaMemsetAsync(a.border, 0, sizeof(double) * nframes * a.T, st));
 
   StageTimer tm{pl, nullptr, st};
-  if (pl->profiling) {
+  if (timed && pl->profiling) {
     pl->prof_pending.emplace_back();
     tm.rec = &pl->prof_pending.back();
   }
@@ -1857,8 +1830,189 @@ int forward(SaxsPlan *pl, const float *xyz, int64_t stride, int nframes, const f
   }
   tm.end(kStHist);
   if (int rc = launch_check("k_hist")) return rc;
+  return SAXS_OK;
+}
+
+int forward(SaxsPlan *pl, const float *xyz, int64_t stride, int nframes, const float *boxes,
+            cudaStream_t st) {
+  if (!pl) return fail(SAXS_E_INVALID, "null plan");
+  if (nframes < 1 || nframes > pl->p.max_frames)
+    return fail(SAXS_E_INVALID, "nframes must be in [1, max_frames]");
+  if (!boxes || (!xyz && pl->a.M > 0)) return fail(SAXS_E_INVALID, "null positions or boxes");
+  if (stride < 3ll * pl->p.natoms) return fail(SAXS_E_INVALID, "frame stride smaller than 3*natoms");
+  DevArgs a = pl->a;
+  a.xyz = xyz;
+  a.frame_stride = stride;
+  // geometry of each frame, checked against the planned k-box
+  Ring &ring = pl->ring;
+  const int slot = ring.next;
+  ring.next = (ring.next + 1) % kRing;
+  CUDA_TRY(cudaEventSynchronize(ring.ev[slot]));
+  float *g = ring.host + static_cast<size_t>(slot) * pl->p.max_frames * kGeom;
+  for (int f = 0; f < nframes; ++f) {
+    const float *box = boxes + 9 * f;
+    if (int rc = check_box(box)) return rc;
+    frame_geometry(pl, box, g + f * kGeom);
+    long long h[3];
+    saxs::kbox_halfwidths(g + f * kGeom + 9, a.qcut, 1e-5, h);
+    for (int d = 0; d < 3; ++d) {
+      if (!pl->full_axis[d] && h[d] > pl->half[d])
+        return fail(SAXS_E_RANGE, "frame box shrank beyond the planned k-box margin; "
+                                  "create the plan with a larger box_margin");
+    }
+  }
+  CUDA_TRY(cudaMemcpyAsync(const_cast<float *>(a.geom), g, sizeof(float) * nframes * kGeom,
+                           cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaEventRecord(ring.ev[slot], st));
+  if (int rc = enqueue_batch(pl, a, nframes, st, true)) return rc;
   pl->frames += nframes;
   pl->last_frame_batch = nframes;
+  return SAXS_OK;
+}
+
+}  // namespace
+
+struct SaxsGraph {
+  std::vector<SaxsPlan *> plans;
+  std::vector<DevArgs> args;
+  std::vector<int> nframes;
+  std::vector<int> offset;  // first frame of each plan in the geometry slots
+  int total = 0;
+  int device = 0;
+  float *pinned[2] = {nullptr, nullptr};
+  cudaGraphExec_t exec[2] = {nullptr, nullptr};
+  cudaEvent_t done[2] = {nullptr, nullptr};
+  int next = 0;
+};
+
+namespace {
+
+void graph_destroy(SaxsGraph *g) {
+  if (!g) return;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(g->device);
+  for (int k = 0; k < 2; ++k) {
+    if (g->done[k]) {
+      cudaEventSynchronize(g->done[k]);
+      cudaEventDestroy(g->done[k]);
+    }
+    if (g->exec[k]) cudaGraphExecDestroy(g->exec[k]);
+    if (g->pinned[k]) cudaFreeHost(g->pinned[k]);
+  }
+  cudaSetDevice(prev);
+  delete g;
+}
+
+int graph_create(SaxsPlan *const *plans, const float *const *xyz, const int64_t *stride,
+                 const int *nframes, int count, SaxsGraph **out) {
+  if (!plans || !xyz || !stride || !nframes || !out || count < 1)
+    return fail(SAXS_E_INVALID, "null argument or empty plan list");
+  *out = nullptr;
+  SaxsGraph *g = new SaxsGraph();
+  g->device = plans[0] ? plans[0]->device : 0;
+  for (int i = 0; i < count; ++i) {
+    SaxsPlan *pl = plans[i];
+    if (!pl) {
+      graph_destroy(g);
+      return fail(SAXS_E_INVALID, "null plan in the list");
+    }
+    for (int k = 0; k < i; ++k)
+      if (plans[k] == pl) {
+        graph_destroy(g);
+        return fail(SAXS_E_INVALID, "a plan appears twice in one graph");
+      }
+    if (pl->device != g->device) {
+      graph_destroy(g);
+      return fail(SAXS_E_INVALID, "all plans of a graph must be on one device");
+    }
+    if (nframes[i] < 1 || nframes[i] > pl->p.max_frames || stride[i] < 3ll * pl->p.natoms ||
+        (!xyz[i] && pl->a.M > 0)) {
+      graph_destroy(g);
+      return fail(SAXS_E_INVALID, "bad frame count, stride or positions for plan " + std::to_string(i));
+    }
+    DevArgs a = pl->a;
+    a.xyz = xyz[i];
+    a.frame_stride = stride[i];
+    g->plans.push_back(pl);
+    g->args.push_back(a);
+    g->nframes.push_back(nframes[i]);
+    g->offset.push_back(g->total);
+    g->total += nframes[i];
+  }
+  cudaStream_t origin = nullptr;
+  std::vector<cudaStream_t> br(count, nullptr);
+  std::vector<cudaEvent_t> fork(count, nullptr), join(count, nullptr);
+  cudaError_t e = cudaStreamCreateWithFlags(&origin, cudaStreamNonBlocking);
+  for (int i = 0; e == cudaSuccess && i < count; ++i) {
+    e = cudaStreamCreateWithFlags(&br[i], cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&fork[i], cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&join[i], cudaEventDisableTiming);
+  }
+  int rc = SAXS_OK;
+  for (int k = 0; e == cudaSuccess && rc == SAXS_OK && k < 2; ++k) {
+    e = cudaMallocHost(reinterpret_cast<void **>(&g->pinned[k]), sizeof(float) * g->total * kGeom);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g->done[k], cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaStreamBeginCapture(origin, cudaStreamCaptureModeThreadLocal);
+    for (int i = 0; e == cudaSuccess && rc == SAXS_OK && i < count; ++i) {
+      const DevArgs &a = g->args[i];
+      e = cudaEventRecord(fork[i], origin);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(br[i], fork[i], 0);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(const_cast<float *>(a.geom), g->pinned[k] + g->offset[i] * kGeom,
+                            sizeof(float) * g->nframes[i] * kGeom, cudaMemcpyHostToDevice, br[i]);
+      if (e == cudaSuccess) rc = enqueue_batch(g->plans[i], a, g->nframes[i], br[i], false);
+      if (e == cudaSuccess && rc == SAXS_OK) e = cudaEventRecord(join[i], br[i]);
+      if (e == cudaSuccess && rc == SAXS_OK) e = cudaStreamWaitEvent(origin, join[i], 0);
+    }
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ee = cudaStreamEndCapture(origin, &graph);
+    if (e == cudaSuccess) e = ee;
+    if (e == cudaSuccess && rc == SAXS_OK) e = cudaGraphInstantiate(&g->exec[k], graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+  }
+  for (int i = 0; i < count; ++i) {
+    if (br[i]) cudaStreamDestroy(br[i]);
+    if (fork[i]) cudaEventDestroy(fork[i]);
+    if (join[i]) cudaEventDestroy(join[i]);
+  }
+  if (origin) cudaStreamDestroy(origin);
+  if (e != cudaSuccess || rc != SAXS_OK) {
+    graph_destroy(g);
+    if (rc != SAXS_OK) return rc;
+    cudaGetLastError();
+    return fail(SAXS_E_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+  }
+  *out = g;
+  return SAXS_OK;
+}
+
+int graph_launch(SaxsGraph *g, const float *boxes, cudaStream_t st) {
+  if (!g || !boxes) return fail(SAXS_E_INVALID, "null argument");
+  const int slot = g->next;
+  g->next ^= 1;
+  CUDA_TRY(cudaEventSynchronize(g->done[slot]));
+  for (size_t i = 0; i < g->plans.size(); ++i) {
+    SaxsPlan *pl = g->plans[i];
+    for (int f = 0; f < g->nframes[i]; ++f) {
+      const int k = g->offset[i] + f;
+      const float *box = boxes + 9 * k;
+      if (int rc = check_box(box)) return rc;
+      float *geo = g->pinned[slot] + static_cast<size_t>(k) * kGeom;
+      frame_geometry(pl, box, geo);
+      long long h[3];
+      saxs::kbox_halfwidths(geo + 9, pl->a.qcut, 1e-5, h);
+      for (int d = 0; d < 3; ++d)
+        if (!pl->full_axis[d] && h[d] > pl->half[d])
+          return fail(SAXS_E_RANGE, "frame box shrank beyond the planned k-box margin");
+    }
+  }
+  CUDA_TRY(cudaGraphLaunch(g->exec[slot], st));
+  CUDA_TRY(cudaEventRecord(g->done[slot], st));
+  for (size_t i = 0; i < g->plans.size(); ++i) {
+    g->plans[i]->frames += g->nframes[i];
+    g->plans[i]->last_frame_batch = g->nframes[i];
+  }
   return SAXS_OK;
 }
 
@@ -2226,6 +2380,30 @@ int saxs_backward(SaxsPlan *plan, const float *xyz_dev, const float *box_host,
   if (plan && prev != plan->device) cudaSetDevice(prev);
   return rc;
 }
+
+int saxs_graph_create(SaxsPlan *const *plans, const float *const *xyz_dev,
+                      const int64_t *frame_stride, const int *nframes, int count, SaxsGraph **graph) {
+  g_err.clear();
+  int prev = 0;
+  cudaGetDevice(&prev);
+  const int dev = (plans && count > 0 && plans[0]) ? plans[0]->device : prev;
+  if (prev != dev) cudaSetDevice(dev);
+  const int rc = graph_create(plans, xyz_dev, frame_stride, nframes, count, graph);
+  if (prev != dev) cudaSetDevice(prev);
+  return rc;
+}
+
+int saxs_graph_launch(SaxsGraph *graph, const float *boxes_host, void *stream) {
+  g_err.clear();
+  int prev = 0;
+  cudaGetDevice(&prev);
+  if (graph && prev != graph->device) cudaSetDevice(graph->device);
+  const int rc = graph_launch(graph, boxes_host, static_cast<cudaStream_t>(stream));
+  if (graph && prev != graph->device) cudaSetDevice(prev);
+  return rc;
+}
+
+void saxs_graph_destroy(SaxsGraph *graph) { graph_destroy(graph); }
 
 int saxs_profile_stages(void) { return kStages; }
 

@@ -136,6 +136,26 @@ def large_triclinic(seed: int = 0, natoms: int = 1_000_000, frames: int = 20) ->
                    jitter=0.5)
 
 
+def uneven_systems(n_systems: int = 64, frames: int = 8, seed: int = 0, nmin: int = 5_000,
+                   nmax: int = 200_000, density: float = 0.1,
+                   grids=(48, 64, 96, 128, 160)) -> list[tuple[System, int]]:
+    """Independent cubic systems with log-uniform atom counts in [nmin, nmax].
+
+    Box edge L = (N / density)^(1/3) A (density 0.1 /A^3 = 100 atoms/nm^3); the
+    grid is the smallest of ``grids`` not below L (about 1 A spacing).
+    Returns [(system, grid)].
+    """
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n_systems):
+        n = int(round(math.exp(rng.uniform(math.log(nmin), math.log(nmax)))))
+        L = (n / density) ** (1.0 / 3.0)
+        grid = next((g for g in grids if g >= L), grids[-1])
+        s = cubic_system(n, L, seed=10_000 * (seed + 1) + i, jitter=0.5, nframes=frames)
+        out.append((s, grid))
+    return out
+
+
 class SyntheticTopology:
     """Topology duck type over a ``System`` (the reference's callback contract)."""
 
