@@ -35,6 +35,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -83,6 +84,8 @@ struct DevArgs {
   int tiles[2], stiles[2], nbins;
   int kx_lo, nkx, ky_lo, nky, nkz, nkzp, nkxp, nkyp;
   int zc;  // z rows of twiddles k_spread_zdft holds in shared memory at once
+  // tensor-core z-DFT (k_spread_zdft_tc): GEMM N, K, spread rows, stages, TMEM columns
+  int tcN, tcK, tcR, tcS, tcCols, tcRB;
   int nf[3];
   int dz;
   float dq, qcut;
@@ -100,6 +103,7 @@ struct DevArgs {
   const float *modx, *mody, *modz;
   const float *ff;    // [T][9]
   const float *twz_sum; // [2*nkzp]: sum over z < ez of the z twiddles (re, im)
+  const float *twz_tc;  // [2][tcK x tcN]: z twiddles as TF32 head / remainder, K-major
   const int4 *home_x; // per spread tile along x: home tiles whose atoms reach it (-1 padded)
   const int4 *home_y;
   int2 *key;
@@ -514,6 +518,435 @@ __global__ void __launch_bounds__(kThreads, 2) k_spread_zdft(DevArgs a, int item
     }
     __syncthreads();
   }
+}
+
+// ---------------------------------------------------------------------------
+// Tensor-core z-axis DFT (tcgen05, 3xTF32)
+// ---------------------------------------------------------------------------
+//
+// The column DFT of one 8x8 column tile is the GEMM D[c][n] = sum_z g[z][c] B[z][n]
+// with M = 64 columns, N = 2*nkz (re, im interleaved, padded to a multiple of 8)
+// and K = the z extent.  Both operands sit in shared memory in the K-major
+// no-swizzle canonical layout of tcgen05 (core matrices of 8 rows x 16 bytes):
+//   A (64 x K):  float offset (z/4)*256 + (c/8)*32 + (c%8)*4 + z%4
+//                 (LBO = 1024 B between z quads, SBO = 128 B between 8-column groups)
+//   B (N x K):   float offset (z/4)*(N/8)*32 + (n/8)*32 + (n%8)*4 + z%4
+//                 (LBO = N*16 B, SBO = 128 B)
+// Column c of the tile is (lx, ly) = (c/8, c%8).  FP32 accuracy comes from
+// splitting each operand into a TF32 head (low 13 mantissa bits cleared) and the
+// exact FP32 remainder: A*B ~ Ah*Bh + Ah*Bl + Al*Bh, accumulated in FP32 in
+// tensor memory.  The dropped Al*Bl term and the TF32 rounding of the remainders
+// are below 2^-19 of each product.
+constexpr int kTcProducerWarps = 16;
+constexpr int kTcProducers = 32 * kTcProducerWarps;
+constexpr int kTcMmaWarp = 16;
+constexpr int kTcLoaderWarp = 17;
+constexpr int kTcThreads = 32 * 22;  // producers, MMA warp, loader warp, 4 epilogue warps
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Shared-memory matrix descriptor: start, leading/stride byte offsets (>> 4),
+// descriptor version 1 at bit 46, base offset 0, no swizzle.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  return static_cast<uint64_t>((addr >> 4) & 0x3FFFu) |
+         (static_cast<uint64_t>((lbo >> 4) & 0x3FFFu) << 16) |
+         (static_cast<uint64_t>((sbo >> 4) & 0x3FFFu) << 32) | (static_cast<uint64_t>(1) << 46);
+}
+
+__device__ __forceinline__ void umma_tf32(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc,
+                                          uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(da), "l"(db), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Bounded wait for the given phase parity of an mbarrier: gives up after 2^24
+// polls or 2 s, whichever comes first, and returns false.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  const uint64_t t0 = global_ns();
+  for (int it = 0; it < (1 << 24); ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P1;\n\t}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if ((it & 255) == 255 && global_ns() - t0 > 2000000000ull) return false;
+  }
+  return false;
+}
+
+__device__ __forceinline__ float tf32_head(float v) {
+  return __uint_as_float(__float_as_uint(v) & 0xFFFFE000u);
+}
+
+// Home-tile record ranges of one item (lane 4*ix + iy of the calling warp owns
+// home tile (hx[ix], hy[iy])), compacted and prefix-summed with shuffles; lane 0
+// writes them to `ta`.  Called by one whole warp.
+__device__ __forceinline__ void tile_atom_ranges_warp(const DevArgs &a, const int4 *home_x,
+                                                      const int4 *home_y, TileAtoms &ta, int f,
+                                                      int t, int x0, int y0) {
+  const int lane = threadIdx.x & 31;
+  const int4 hxv = home_x[x0 / kTile], hyv = home_y[y0 / kTile];
+  const int ix = (lane >> 2) & 3, iy = lane & 3;
+  const int hx = ix == 0 ? hxv.x : ix == 1 ? hxv.y : ix == 2 ? hxv.z : hxv.w;
+  const int hy = iy == 0 ? hyv.x : iy == 1 ? hyv.y : iy == 2 ? hyv.z : hyv.w;
+  const bool valid = lane < 16 && hx >= 0 && hy >= 0;
+  int s0 = 0, cnt = 0;
+  if (valid) {
+    const int *off = a.offsets + static_cast<int64_t>(f) * (a.nbins + 1);
+    const int bin = (t * a.tiles[1] + hy) * a.tiles[0] + hx;
+    s0 = off[bin];
+    cnt = off[bin + 1] - s0;
+  }
+  const unsigned bal = __ballot_sync(0xffffffffu, valid);
+  const int pos = __popc(bal & ((1u << lane) - 1u));
+  int inc = cnt;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const int v = __shfl_up_sync(0xffffffffu, inc, d);
+    if (lane >= d) inc += v;
+  }
+  // lane 0 gathers (pos, start, inclusive count) of the valid lanes and writes them
+  int nb = 0;
+  for (int l = 0; l < 16; ++l) {
+    const int sl = __shfl_sync(0xffffffffu, s0, l);
+    const int il = __shfl_sync(0xffffffffu, inc, l);
+    if ((bal >> l) & 1u) {
+      if (lane == 0) {
+        ta.start[nb] = sl;
+        ta.cum[nb + 1] = il;
+      }
+      ++nb;
+    }
+  }
+  if (lane == 0) {
+    ta.cum[0] = 0;
+    ta.nb = nb;
+  }
+  (void)pos;
+}
+
+// Spreading of one column tile into the K-major A layout, one thread per
+// (atom, z tap): the four lanes of an atom write four different banks.  Records
+// [0, nrec_smem) come from the shared-memory copy, the rest from global memory.
+__device__ __forceinline__ void spread_tile_kmajor(const DevArgs &a, const TileAtoms &ta,
+                                                   const float4 *srec, int nrec_smem, float *A,
+                                                   int f, int x0, int y0, int cw, int ch, int tid,
+                                                   int nthreads) {
+  const float4 *rec = a.rec + static_cast<int64_t>(f) * a.M;
+  const int P = a.order, nt = a.ntaps, nz = a.n[2];
+  const int total = ta.cum[ta.nb] * nt;
+  for (int k = tid; k < total; k += nthreads) {
+    const int v = nt == 4 ? (k >> 2) : k / nt;
+    const int r = k - v * nt;
+    float4 q;
+    if (v < nrec_smem) {
+      q = srec[v];
+    } else {
+      int j = 0;
+      while (v >= ta.cum[j + 1]) ++j;
+      q = rec[ta.start[j] + (v - ta.cum[j])];
+    }
+    const int m0 = static_cast<int>(q.x), m1 = static_cast<int>(q.y), m2 = static_cast<int>(q.z);
+    float wx[4], wy[4], wz[4];
+    cubic_weights(q.x - static_cast<float>(m0), wx);
+    cubic_weights(q.y - static_cast<float>(m1), wy);
+    cubic_weights(q.z - static_cast<float>(m2), wz);
+    const float wzr = r == 0 ? wz[0] : r == 1 ? wz[1] : r == 2 ? wz[2] : wz[3];
+    int z = m2 - P + r;
+    if (z < 0) z += nz;
+    float *colz = A + (z >> 2) * 256 + (z & 3);
+#pragma unroll
+    for (int o = 0; o < 4; ++o) {
+      if (o >= nt) break;
+      int x = m0 - P + o;
+      if (x < 0) x += a.n[0];
+      const int lx = x - x0;
+      if (static_cast<unsigned>(lx) >= static_cast<unsigned>(cw)) continue;
+#pragma unroll
+      for (int p = 0; p < 4; ++p) {
+        if (p >= nt) break;
+        int y = m1 - P + p;
+        if (y < 0) y += a.n[1];
+        const int ly = y - y0;
+        if (static_cast<unsigned>(ly) >= static_cast<unsigned>(ch)) continue;
+        atomicAdd(colz + lx * 32 + ly * 4, (wx[o] * wy[p]) * wzr);
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void producers_sync() {
+  asm volatile("bar.sync 1, %0;" ::"r"(kTcProducers) : "memory");
+}
+
+// Work item w -> (frame, type, tile origin, tile extent).
+struct TcItem {
+  int f, t, x0, y0, cw, ch;
+};
+
+__device__ __forceinline__ TcItem tc_item(const DevArgs &a, int w) {
+  const int st = a.stiles[0] * a.stiles[1];
+  TcItem it;
+  it.f = w / (a.T * st);
+  it.t = (w / st) % a.T;
+  const int tl = w % st;
+  it.x0 = (tl % a.stiles[0]) * kTile;
+  it.y0 = (tl / a.stiles[0]) * kTile;
+  it.cw = min(kTile, a.ext[0] - it.x0);
+  it.ch = min(kTile, a.ext[1] - it.y0);
+  return it;
+}
+
+// Persistent, warp-specialized: grid = min(work items, resident CTAs), block
+// kTcThreads = 22 warps.  Work items as in k_spread_zdft, in the same order in
+// every role:
+//   warps 0-15  producers: zero the stage's A tile, spread the item's atoms
+//               into it (shared-memory atomics), subtract the padding mean and
+//               split it into the TF32 head (in place) and remainder
+//   warp 16     one lane issues the 3xTF32 MMAs of an item into its TMEM stage
+//   warp 17     loader: home-tile record ranges of an item and bulk copies
+//               (cp.async.bulk) of its atom records into a staging buffer
+//   warps 18-21 epilogue: TMEM accumulator -> Z (warp w reads lane quarter w%4)
+// Hand-offs are mbarriers, every wait bounded:
+//   rec_full[b]   loader -> producers (records + ranges of buffer b landed)
+//   rec_empty[b]  producers -> loader (buffer b spread)
+//   full[s]       producers -> MMA (stage s operands written)
+//   done[s]       MMA commit -> epilogue (accumulator ready) and producers
+//                 (stage s operands free again)
+//   tmem_empty[s] epilogue -> MMA (TMEM stage s read out)
+// Dynamic shared memory: Bh, Bl (tcK x tcN floats each), tcS stages of
+// A32 (tcR x 64) + Al (tcK x 64), two record buffers of tcRB float4, and the
+// home-tile tables (stiles[0] + stiles[1] int4).
+__global__ void __launch_bounds__(kTcThreads, 1) k_spread_zdft_tc(DevArgs a, int items) {
+  extern __shared__ __align__(16) unsigned char smem[];  // no-swizzle operands need 16 B
+  __shared__ TileAtoms ta[2];
+  __shared__ __align__(8) uint64_t bars[10];
+  __shared__ uint32_t tmem_slot;
+  __shared__ volatile int abort_flag;
+  const int N = a.tcN, KT = a.tcK, R = a.tcR, S = a.tcS, RB = a.tcRB;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  float *bh = reinterpret_cast<float *>(smem);
+  float *bl = bh + KT * N;
+  float *stages = bl + KT * N;
+  float4 *recs = reinterpret_cast<float4 *>(stages + static_cast<size_t>(S) * (R + KT) * 64);
+  int4 *home_x = reinterpret_cast<int4 *>(recs + 2 * RB);
+  int4 *home_y = home_x + a.stiles[0];
+  uint64_t *rec_full = bars, *rec_empty = bars + 2, *full = bars + 4, *done = bars + 6,
+           *tmem_empty = bars + 8;
+  {
+    const float4 *src = reinterpret_cast<const float4 *>(a.twz_tc);
+    float4 *dst = reinterpret_cast<float4 *>(bh);
+    for (int i = tid; i < KT * N / 2; i += blockDim.x) dst[i] = src[i];
+    for (int i = tid; i < a.stiles[0]; i += blockDim.x) home_x[i] = a.home_x[i];
+    for (int i = tid; i < a.stiles[1]; i += blockDim.x) home_y[i] = a.home_y[i];
+  }
+  if (warp == kTcMmaWarp) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_addr(&tmem_slot)),
+                 "r"(a.tcCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+  }
+  if (tid == 0) {
+    const int counts[10] = {1, 1, 1, 1, kTcProducerWarps, kTcProducerWarps, 1, 1, 4, 4};
+    for (int i = 0; i < 10; ++i)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&bars[i])), "r"(counts[i]));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    abort_flag = 0;
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_slot;
+
+  // bounded wait; on a timeout the whole block switches to skipping its work
+  auto wait = [&](uint64_t *bar, int parity) {
+    if (abort_flag) return;
+    if (!mbar_wait(smem_addr(bar), static_cast<uint32_t>(parity & 1))) {
+      abort_flag = 1;
+      atomicExch(a.status, 1);
+    }
+  };
+
+  if (warp < kTcProducerWarps) {
+    int j = 0;
+    for (int w = blockIdx.x; w < items; w += gridDim.x, ++j) {
+      const int b = j & 1, s = S == 2 ? (j & 1) : 0;
+      float *A32 = stages + static_cast<size_t>(s) * (R + KT) * 64;
+      float *Al = A32 + static_cast<size_t>(R) * 64;
+      const TcItem it = tc_item(a, w);
+      if (j >= S) wait(&done[s], (j - S) / S);  // the stage's previous MMAs are finished
+      {
+        float4 *t4 = reinterpret_cast<float4 *>(A32);
+        for (int i = tid; i < R * 16; i += kTcProducers) t4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+      wait(&rec_full[b], j >> 1);
+      producers_sync();
+      if (!abort_flag) {
+        const int nrec = min(ta[b].cum[ta[b].nb], RB);
+        spread_tile_kmajor(a, ta[b], recs + static_cast<size_t>(b) * RB, nrec, A32, it.f, it.x0,
+                           it.y0, it.cw, it.ch, tid, kTcProducers);
+      }
+      producers_sync();
+      if (tid == 0) mbar_arrive(smem_addr(&rec_empty[b]));
+      {
+        // padding mean applied before the TF32 split: the tensor cores see
+        // g - mean (rows z >= ez meet zero twiddles)
+        const float mean = static_cast<float>(
+            a.border[static_cast<int64_t>(it.f) * a.T + it.t] / a.border_count);
+        float4 *h4 = reinterpret_cast<float4 *>(A32);
+        float4 *l4 = reinterpret_cast<float4 *>(Al);
+        for (int i = tid; i < KT * 16; i += kTcProducers) {
+          float4 v = h4[i];
+          v.x -= mean;
+          v.y -= mean;
+          v.z -= mean;
+          v.w -= mean;
+          const float4 h = make_float4(tf32_head(v.x), tf32_head(v.y), tf32_head(v.z), tf32_head(v.w));
+          h4[i] = h;
+          l4[i] = make_float4(v.x - h.x, v.y - h.y, v.z - h.z, v.w - h.w);
+        }
+      }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(smem_addr(&full[s]));
+    }
+  } else if (warp == kTcMmaWarp) {
+    if (lane == 0) {
+      // kind::tf32 instruction descriptor: D f32 (bits 4-5 = 1), A and B tf32 (2),
+      // both K-major, N >> 3 at bit 17, M >> 4 at bit 24 (M = 64).
+      const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) |
+                             (static_cast<uint32_t>(N >> 3) << 17) | (static_cast<uint32_t>(64 >> 4) << 24);
+      const uint32_t bstep = static_cast<uint32_t>(N) * 32;  // bytes per 8 z of B
+      const uint64_t dbh0 = umma_desc(smem_addr(bh), N * 16, 128);
+      const uint64_t dbl0 = umma_desc(smem_addr(bl), N * 16, 128);
+      int j = 0;
+      uint32_t last_bar = 0;
+      int last_parity = 0;
+      for (int w = blockIdx.x; w < items && !abort_flag; w += gridDim.x, ++j) {
+        const int s = S == 2 ? (j & 1) : 0;
+        const float *A32 = stages + static_cast<size_t>(s) * (R + KT) * 64;
+        const float *Al = A32 + static_cast<size_t>(R) * 64;
+        wait(&full[s], j / S);
+        if (j >= S) wait(&tmem_empty[s], (j - S) / S);
+        if (abort_flag) break;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t d = tmem + static_cast<uint32_t>(s * N);
+        const uint64_t dah0 = umma_desc(smem_addr(A32), 1024, 128);
+        const uint64_t dal0 = umma_desc(smem_addr(Al), 1024, 128);
+        // descriptor start addresses are in 16-byte units: one k step of A is
+        // 2048 B (+128), of B N*32 B (+N*2)
+        for (int kk = 0; kk < KT / 8; ++kk) {
+          const uint64_t dah = dah0 + static_cast<uint64_t>(kk * 128);
+          const uint64_t dal = dal0 + static_cast<uint64_t>(kk * 128);
+          const uint64_t dbh = dbh0 + static_cast<uint64_t>(kk * (bstep >> 4));
+          const uint64_t dbl = dbl0 + static_cast<uint64_t>(kk * (bstep >> 4));
+          umma_tf32(d, dal, dbh, idesc, kk > 0 ? 1u : 0u);
+          umma_tf32(d, dah, dbl, idesc, 1u);
+          umma_tf32(d, dah, dbh, idesc, 1u);
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                         smem_addr(&done[s]))
+                     : "memory");
+        last_bar = smem_addr(&done[s]);
+        last_parity = j / S;
+      }
+      // a wait ran out somewhere: let the newest MMAs finish (bounded) before the
+      // tensor memory is released
+      if (abort_flag && last_bar) mbar_wait(last_bar, static_cast<uint32_t>(last_parity & 1));
+    }
+  } else if (warp == kTcLoaderWarp) {
+    const float4 *rec_all = a.rec;
+    int j = 0;
+    for (int w = blockIdx.x; w < items && !abort_flag; w += gridDim.x, ++j) {
+      const int b = j & 1;
+      const TcItem it = tc_item(a, w);
+      if (j >= 2) wait(&rec_empty[b], (j - 2) >> 1);
+      if (abort_flag) break;
+      tile_atom_ranges_warp(a, home_x, home_y, ta[b], it.f, it.t, it.x0, it.y0);
+      __syncwarp();
+      if (lane == 0) {
+        const TileAtoms &tb = ta[b];
+        const int nrec = min(tb.cum[tb.nb], RB);
+        const uint32_t bar = smem_addr(&rec_full[b]);
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
+                     "r"(nrec * 16)
+                     : "memory");
+        const float4 *src = rec_all + static_cast<int64_t>(it.f) * a.M;
+        const uint32_t dst = smem_addr(recs + static_cast<size_t>(b) * RB);
+        for (int r = 0; r < tb.nb; ++r) {
+          const int lo = tb.cum[r], hi = min(tb.cum[r + 1], nrec);
+          if (hi > lo)
+            asm volatile(
+                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                    dst + static_cast<uint32_t>(lo) * 16),
+                "l"(src + tb.start[r]), "r"((hi - lo) * 16), "r"(bar)
+                : "memory");
+        }
+      }
+    }
+  } else {
+    // epilogue warps
+    const int quarter = warp & 3;
+    int j = 0;
+    for (int w = blockIdx.x; w < items && !abort_flag; w += gridDim.x, ++j) {
+      const int s = S == 2 ? (j & 1) : 0;
+      wait(&done[s], j / S);
+      if (abort_flag) break;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const TcItem it = tc_item(a, w);
+      const int64_t zplane = static_cast<int64_t>(a.ext[0]) * a.ext[1];
+      float2 *Zft = a.Z + (static_cast<int64_t>(it.f) * a.T + it.t) * a.nkz * zplane;
+      // with M = 64, row c of D sits in TMEM lane (c % 16) + 32 * (c / 16)
+      const int c = 16 * quarter + lane, lx = c >> 3, ly = c & 7;
+      const bool valid = lane < 16 && lx < it.cw && ly < it.ch;
+      const int64_t cell = static_cast<int64_t>(it.x0 + lx) * a.ext[1] + (it.y0 + ly);
+      const uint32_t lane_base = tmem + (static_cast<uint32_t>(32 * quarter) << 16) + static_cast<uint32_t>(s * N);
+      for (int c0 = 0; c0 < N; c0 += 8) {
+        uint32_t r[8];
+        asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                     : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+                       "=r"(r[6]), "=r"(r[7])
+                     : "r"(lane_base + c0));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (valid) {
+#pragma unroll
+          for (int jj = 0; jj < 4; ++jj) {
+            const int kz = c0 / 2 + jj;
+            if (kz < a.nkz)
+              Zft[kz * zplane + cell] = make_float2(__uint_as_float(r[2 * jj]), __uint_as_float(r[2 * jj + 1]));
+          }
+        }
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(smem_addr(&tmem_empty[s]));
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (warp == kTcMmaWarp)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(a.tcCols));
 }
 
 
@@ -1332,6 +1765,9 @@ struct SaxsPlan {
   bool adj_tiled_y = false, adj_tiled_z = false;
   size_t smem_yadj = 0, smem_zadj = 0;
   int spread_ctas = 1;  // resident CTAs of the persistent spreading kernel
+  bool use_tc = false;  // z-axis DFT on the tensor cores (k_spread_zdft_tc)
+  size_t smem_spread_tc = 0;
+  int tc_ctas = 1;
   int xc = 1;           // x values per shared-memory chunk in k_xdft_post
   bool profiling = false;
   std::vector<StageRecord> prof_pending;
@@ -1570,6 +2006,41 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
     pl->xc = static_cast<int>(std::min<size_t>(xc, a.ext[0]));
     pl->smem_xdft = fixed + static_cast<size_t>(pl->xc) * per_x;
   }
+  {
+    // tensor-core z-DFT: N = 2*nkz padded to 8 (<= 256), K = ez padded to 8, two
+    // operand stages when they fit, else one.  PYCUSAXS_ZDFT=simt keeps the FP32
+    // SIMT kernel.
+    const char *mode = std::getenv("PYCUSAXS_ZDFT");
+    const bool simt_only = mode && std::strcmp(mode, "simt") == 0;
+    const int N = round_up(2 * a.nkz, 8);
+    const int KT = round_up(a.ext[2], 8);
+    const int R = std::max(KT, round_up(a.n[2], 8));
+    const size_t avail = optin - static_smem(k_spread_zdft_tc);
+    const size_t b_bytes = 2 * static_cast<size_t>(KT) * N * sizeof(float);
+    const size_t stage_bytes = static_cast<size_t>(R + KT) * 64 * sizeof(float);
+    const size_t home_bytes = static_cast<size_t>(a.stiles[0] + a.stiles[1]) * sizeof(int4);
+    // two operand stages before larger record buffers; records beyond the
+    // staging buffer are read from global memory
+    int S = 0, RB = 0;
+    for (int s_try = 2; s_try >= 1 && S == 0; --s_try)
+      for (int rb = 1024; rb >= 128 && S == 0; rb /= 2)
+        if (b_bytes + s_try * stage_bytes + 2 * static_cast<size_t>(rb) * 16 + home_bytes <= avail) {
+          S = s_try;
+          RB = rb;
+        }
+    if (!simt_only && N <= 256 && S > 0) {
+      pl->use_tc = true;
+      a.tcN = N;
+      a.tcK = KT;
+      a.tcR = R;
+      a.tcS = S;
+      a.tcRB = RB;
+      int cols = 32;
+      while (cols < S * N) cols *= 2;
+      a.tcCols = cols;
+      pl->smem_spread_tc = b_bytes + S * stage_bytes + 2 * static_cast<size_t>(RB) * 16 + home_bytes;
+    }
+  }
   pl->smem_hist = a.num_bins <= kHistSmemBins ? 2 * sizeof(double) * a.num_bins : 0;
   pl->smem_bin = static_cast<size_t>(kThreads / 32) * a.T * sizeof(double);
   if (pl->smem_spread + static_smem(k_spread_zdft) > optin ||
@@ -1611,8 +2082,9 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
   ALLOC(d_modz, nn[2]);
   ALLOC(d_ff, 9 * a.T);
   int4 *d_hx = nullptr, *d_hy = nullptr;
-  float *d_twzs = nullptr;
+  float *d_twzs = nullptr, *d_twztc = nullptr;
   ALLOC(d_twzs, 2 * a.nkzp);
+  if (pl->use_tc) ALLOC(d_twztc, 2 * static_cast<size_t>(a.tcK) * a.tcN);
   ALLOC(d_hx, a.stiles[0]);
   ALLOC(d_hy, a.stiles[1]);
   ALLOC(d_geom, static_cast<size_t>(B) * kGeom);
@@ -1641,6 +2113,7 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
   a.modz = d_modz;
   a.ff = d_ff;
   a.twz_sum = d_twzs;
+  a.twz_tc = d_twztc;
   a.home_x = d_hx;
   a.home_y = d_hy;
   a.geom = d_geom;
@@ -1661,6 +2134,25 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
     }
     twzs[2 * k] = static_cast<float>(re);
     twzs[2 * k + 1] = static_cast<float>(im);
+  }
+  // the same z twiddles in the tensor-core B layout, split into a TF32 head and
+  // the exact remainder
+  std::vector<float> twtc(pl->use_tc ? 2 * static_cast<size_t>(a.tcK) * a.tcN : 0, 0.0f);
+  if (pl->use_tc) {
+    const size_t half = static_cast<size_t>(a.tcK) * a.tcN;
+    for (int z = 0; z < ez; ++z)
+      for (int n = 0; n < 2 * a.nkz; ++n) {
+        const float2 w = twz[z * a.nkzp + n / 2];
+        const float v = (n & 1) ? w.y : w.x;
+        uint32_t bits;
+        std::memcpy(&bits, &v, sizeof(bits));
+        bits &= 0xFFFFE000u;
+        float head;
+        std::memcpy(&head, &bits, sizeof(head));
+        const size_t o = static_cast<size_t>(z / 4) * (a.tcN / 8) * 32 + (n / 8) * 32 + (n % 8) * 4 + z % 4;
+        twtc[o] = head;
+        twtc[half + o] = v - head;
+      }
   }
   std::vector<float2> twy(static_cast<size_t>(ey) * a.nkyp, make_float2(0.f, 0.f));
   for (int y = 0; y < ey; ++y)
@@ -1697,6 +2189,7 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
       (rc = up(d_ff, pl->ff.data(), sizeof(float) * pl->ff.size())) ||
       (rc = up(d_hx, hxt.data(), sizeof(int4) * hxt.size())) ||
       (rc = up(d_twzs, twzs.data(), sizeof(float) * twzs.size())) ||
+      (rc = up(d_twztc, twtc.data(), sizeof(float) * twtc.size())) ||
       (rc = up(d_hy, hyt.data(), sizeof(int4) * hyt.size())) ||
       (rc = up(pl->d_geom0, g0, sizeof(g0)))) {
     destroy(pl);
@@ -1719,12 +2212,21 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
   if (e == cudaSuccess) e = raise_smem_limit(k_xdft_post);
   if (e == cudaSuccess) e = raise_smem_limit(k_hist<float>);
   if (e == cudaSuccess) e = raise_smem_limit(k_hist<double>);
+  if (e == cudaSuccess) e = raise_smem_limit(k_spread_zdft_tc);
   if (e == cudaSuccess) {
     int per_sm = 0, sms = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_spread_zdft, kThreads,
                                                       pl->smem_spread);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, pl->device);
     pl->spread_ctas = std::max(1, per_sm) * std::max(1, sms);
+    if (e == cudaSuccess && pl->use_tc) {
+      // resident CTAs whose tensor-memory allocations fit the SM's 512 columns together
+      int tc_per_sm = 0;
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tc_per_sm, k_spread_zdft_tc, kTcThreads,
+                                                        pl->smem_spread_tc);
+      tc_per_sm = std::min(std::max(1, tc_per_sm), 512 / a.tcCols);
+      pl->tc_ctas = tc_per_sm * std::max(1, sms);
+    }
   }
   if (e != cudaSuccess) {
     destroy(pl);
@@ -1768,6 +2270,19 @@ struct StageTimer {
   }
 };
 
+// Spreading + z-axis DFT of `items` work items: the tensor-core kernel when the
+// plan has it, else the FP32 SIMT kernel.
+int launch_spread(const SaxsPlan *pl, const DevArgs &a, int items, cudaStream_t st) {
+  if (pl->use_tc) {
+    k_spread_zdft_tc<<<std::max(1, std::min(items, pl->tc_ctas)), kTcThreads, pl->smem_spread_tc,
+                       st>>>(a, items);
+    return launch_check("k_spread_zdft_tc");
+  }
+  k_spread_zdft<<<std::max(1, std::min(items, pl->spread_ctas)), kThreads, pl->smem_spread, st>>>(
+      a, items);
+  return launch_check("k_spread_zdft");
+}
+
 // Enqueue the memsets and kernels of one batch of `nframes` frames whose
 // geometry is already in (or queued for) a.geom.  Host work free, so that it can
 // be captured in a CUDA graph.
@@ -1799,11 +2314,10 @@ int enqueue_batch(SaxsPlan *pl, const DevArgs &a, int nframes, cudaStream_t st, 
   }
   {
     const int items = a.stiles[0] * a.stiles[1] * a.T * nframes;
-    const int grid = std::max(1, std::min(items, pl->spread_ctas));
     tm.begin(kStSpread);
-    k_spread_zdft<<<grid, kThreads, pl->smem_spread, st>>>(a, items);
+    const int rc = launch_spread(pl, a, items, st);
     tm.end(kStSpread);
-    if (int rc = launch_check("k_spread_zdft")) return rc;
+    if (rc) return rc;
   }
   {
     dim3 gy((a.ext[0] + kYRows - 1) / kYRows, a.nkz, nframes * a.T);
@@ -2036,7 +2550,11 @@ int histogram(SaxsPlan *pl, double *hist, double *nhist, cudaStream_t st) {
     CUDA_TRY(cudaMemcpyAsync(hist, a.hist, nb * sizeof(double), cudaMemcpyDeviceToHost, st));
     CUDA_TRY(cudaMemcpyAsync(nhist, a.nhist, nb * sizeof(double), cudaMemcpyDeviceToHost, st));
   }
+  int status = 0;
+  CUDA_TRY(cudaMemcpyAsync(&status, a.status, sizeof(int), cudaMemcpyDeviceToHost, st));
   CUDA_TRY(cudaStreamSynchronize(st));
+  if (status != 0)
+    return fail(SAXS_E_CUDA, "tensor-core z-DFT: an MMA completion wait ran out; results are invalid");
   return SAXS_OK;
 }
 
@@ -2138,8 +2656,7 @@ int backward(SaxsPlan *pl, const float *xyz, const float *box, const double *dl,
     CUDA_TRY(cudaMemsetAsync(a.offsets, 0, sizeof(int) * (a.nbins + 1), st));
   }
   const int items = a.stiles[0] * a.stiles[1] * a.T;
-  k_spread_zdft<<<std::max(1, std::min(items, pl->spread_ctas)), kThreads, pl->smem_spread, st>>>(
-      a, items);
+  if (int rc = launch_spread(pl, a, items, st)) return rc;
   dim3 gy((a.ext[0] + kYRows - 1) / kYRows, a.nkz, a.T);
   k_ydft<<<gy, kThreads, pl->smem_ydft, st>>>(a);
   if (int rc = launch_check("backward recompute")) return rc;
@@ -2270,9 +2787,7 @@ int forward_into_scratch(SaxsPlan *pl, const float *xyz, const float *box, unsig
     CUDA_TRY(cudaMemsetAsync(a.offsets, 0, sizeof(int) * (a.nbins + 1), st));
   }
   const int items = a.stiles[0] * a.stiles[1] * a.T;
-  k_spread_zdft<<<std::max(1, std::min(items, pl->spread_ctas)), kThreads, pl->smem_spread, st>>>(
-      a, items);
-  if (int rc = launch_check("k_spread_zdft")) return rc;
+  if (int rc = launch_spread(pl, a, items, st)) return rc;
   dim3 gy((a.ext[0] + kYRows - 1) / kYRows, a.nkz, a.T);
   k_ydft<<<gy, kThreads, pl->smem_ydft, st>>>(a);
   if (int rc = launch_check("k_ydft")) return rc;
@@ -2312,7 +2827,7 @@ int saxs_plan_info(const SaxsPlan *pl, SaxsPlanInfo *info) {
   info->kbox[1] = a.nky;
   info->kbox[2] = a.nkz;
   info->kz_count = a.nkz;
-  info->path = 0;
+  info->path = pl->use_tc ? 1 : 0;
   info->device_bytes = pl->bytes;
   info->frames_accumulated = pl->frames;
   return SAXS_OK;

@@ -39,6 +39,7 @@ class PlanInfo:
     kbox: tuple
     device_bytes: int
     frames: int
+    path: int = 0  # 1: z-axis DFT on the tensor cores (tcgen05), 0: FP32 SIMT
 
 
 def entries_from_index(atom_index: dict, natoms: int | None = None):
@@ -120,7 +121,7 @@ class SaxsEngine:
         _native.check(self.lib.saxs_plan_info(self._plan, ctypes.byref(i)))
         return PlanInfo(tuple(i.grid), tuple(i.scaled_grid), float(i.bin_size), float(i.qcut),
                         int(i.num_bins), tuple(i.kbox), int(i.device_bytes),
-                        int(i.frames_accumulated))
+                        int(i.frames_accumulated), int(i.path))
 
     @property
     def frames(self) -> int:

@@ -1,0 +1,122 @@
+"""Tensor-core (tcgen05, 3xTF32) z-axis DFT vs the FP32 SIMT kernel and the FP64 oracle (GPU).
+
+Plans take the tensor-core kernel whenever its operands fit shared memory
+(``info.path == 1``); ``PYCUSAXS_ZDFT=simt`` at plan creation keeps the SIMT
+kernel.  Both must give identical bin counts and profiles within the 1e-4 tolerance of
+the FP64 oracle; the 3xTF32 products are accurate to ~2^-19, and
+TC_VS_SIMT_RTOL (2e-5 per bin) bounds the difference between the two kernels.
+"""
+import contextlib
+import os
+
+import numpy as np
+import pytest
+
+from helpers import assert_profiles_close, engine_hist, oracle_hist
+from pycusaxs_b200.synthetic import System, cubic_system
+
+pytestmark = pytest.mark.gpu
+
+TC_VS_SIMT_RTOL = 2e-5
+
+
+@contextlib.contextmanager
+def zdft_mode(mode):
+    old = os.environ.get("PYCUSAXS_ZDFT")
+    if mode is None:
+        os.environ.pop("PYCUSAXS_ZDFT", None)
+    else:
+        os.environ["PYCUSAXS_ZDFT"] = mode
+    try:
+        yield
+    finally:
+        if old is None:
+            os.environ.pop("PYCUSAXS_ZDFT", None)
+        else:
+            os.environ["PYCUSAXS_ZDFT"] = old
+
+
+def _both(system, grid, frames, expect_tc=True, **kw):
+    with zdft_mode(None):
+        h_tc, n_tc, e_tc = engine_hist(system, grid, frames, **kw)
+        path_tc = e_tc.info.path
+        e_tc.close()
+    with zdft_mode("simt"):
+        h_s, n_s, e_s = engine_hist(system, grid, frames, **kw)
+        path_s = e_s.info.path
+        e_s.close()
+    assert path_s == 0
+    assert path_tc == (1 if expect_tc else 0)
+    np.testing.assert_array_equal(n_tc, n_s)
+    sel = n_s > 0
+    sel[0] = False
+    diff = np.abs(h_tc[sel] - h_s[sel]) / np.abs(h_s[sel])
+    ho, no, _ = oracle_hist(system, grid, frames, **{k: v for k, v in kw.items() if k != "max_frames"})
+    err_tc = assert_profiles_close(h_tc, n_tc, ho, no)
+    err_s = assert_profiles_close(h_s, n_s, ho, no)
+    print(f"vs FP64 oracle: tensor cores {err_tc:.2e}, SIMT {err_s:.2e}; between them {diff.max():.2e}")
+    assert diff.max() <= TC_VS_SIMT_RTOL, diff.max()
+    return err_tc, float(diff.max())
+
+
+def _line_system(n, lengths, seed, elements=("C", "O")):
+    rng = np.random.default_rng(seed)
+    L = np.asarray(lengths, np.float64)
+    pos = (rng.uniform(0, 1, (n, 3)) * L).astype(np.float32)
+    el = np.array(elements, dtype=object)[rng.choice(len(elements), n)]
+    return System(el, pos, np.diag(L).astype(np.float32))
+
+
+def test_tc_small_cubic(cuda):
+    s = cubic_system(4000, 40.0, seed=11)
+    _both(s, (32, 32, 32), [s.positions], sigma=2.0, qcut=0.6)
+
+
+def test_tc_bench_sized_grid128(cuda):
+    # the trajectory workload's plan: grid 128, 256^3 supercell, q-cut 0.5
+    s = cubic_system(30_000, 120.0, seed=12)
+    _both(s, (128, 128, 128), [s.positions], sigma=2.0, qcut=0.5, bin_size=0.002)
+
+
+def test_tc_uneven_grid_z_not_multiple_of_8(cuda):
+    # z extent 44 -> K padded to 48 with zero twiddle rows
+    s = _line_system(3000, (30.0, 40.0, 44.0), 13, ("H", "C", "O", "N"))
+    _both(s, (24, 32, 44), [s.positions], sigma=2.5, qcut=0.9)
+
+
+def test_tc_order2_two_taps(cuda):
+    s = cubic_system(3000, 36.0, seed=14)
+    _both(s, (32, 32, 32), [s.positions], order=2, sigma=2.0, qcut=0.7)
+
+
+def test_tc_supercell_smaller_than_grid(cuda):
+    # scaled grid below the grid: the transform crops, spread rows exceed K
+    s = cubic_system(3000, 36.0, seed=15)
+    _both(s, (40, 40, 40), [s.positions], scaled_grid=(32, 32, 30), qcut=0.6)
+
+
+def test_tc_single_operand_stage_long_z(cuda):
+    # z extent 256, 17 kz values (N = 40): twiddles 80 KB + one 128 KB operand stage
+    # fit shared memory, two stages do not
+    s = _line_system(4000, (80.0, 80.0, 320.0), 16)
+    _both(s, (32, 32, 256), [s.positions], sigma=2.0, qcut=0.15)
+
+
+def test_tc_many_kz_wide_n(cuda):
+    # long z at the largest q-cut the grid allows (reset to ~1.55 /A): the full kz
+    # axis, 97 values, N = 200 with one operand stage
+    s = _line_system(1500, (16.0, 16.0, 192.0), 17)
+    _both(s, (16, 16, 96), [s.positions], sigma=2.0, qcut=3.5)
+
+
+def test_too_many_kz_keeps_simt(cuda):
+    # ~126 kz values over a 256-long z axis: the twiddle operands alone (2 x 256 x 256
+    # floats) exceed shared memory, so the plan keeps the SIMT kernel
+    s = _line_system(1200, (20.0, 20.0, 320.0), 18)
+    _both(s, (16, 16, 256), [s.positions], expect_tc=False, sigma=2.0, qcut=50.0)
+
+
+def test_tc_batched_frames(cuda):
+    s = cubic_system(5000, 40.0, seed=19, jitter=0.5, nframes=3)
+    frames = [s.frame(k) for k in range(3)]
+    _both(s, (32, 32, 32), frames, sigma=2.0, qcut=0.6, max_frames=3)
