@@ -82,6 +82,8 @@ struct DevArgs {
   int order, ntaps;
   int T, M;
   int tiles[2], stiles[2], nbins;
+  int bin_w;  // home-bin width (columns) of the atom counting sort: 4, or 8 when 4 would
+              // need more than four bins per spread tile and axis
   int kx_lo, nkx, ky_lo, nky, nkz, nkzp, nkxp, nkyp;
   int zc;  // z rows of twiddles k_spread_zdft holds in shared memory at once
   // tensor-core z-DFT (k_spread_zdft_tc): GEMM N, K, spread rows, stages, TMEM columns
@@ -201,7 +203,7 @@ __global__ void __launch_bounds__(kThreads) k_bin_atoms(DevArgs a) {
     if (xf < 0) xf += a.n[0];
     int yf = m[1] - a.order;
     if (yf < 0) yf += a.n[1];
-    const int bin = (t * a.tiles[1] + yf / kTile) * a.tiles[0] + xf / kTile;
+    const int bin = (t * a.tiles[1] + yf / a.bin_w) * a.tiles[0] + xf / a.bin_w;
     const int rank = atomicAdd(&a.counts[f * a.nbins + bin], 1);
     a.key[static_cast<int64_t>(f) * a.M + e] = make_int2(bin, rank);
     // Contribution of this atom to the z-border planes of its type's grid:
@@ -537,11 +539,11 @@ __global__ void __launch_bounds__(kThreads, 2) k_spread_zdft(DevArgs a, int item
 // exact FP32 remainder: A*B ~ Ah*Bh + Ah*Bl + Al*Bh, accumulated in FP32 in
 // tensor memory.  The dropped Al*Bl term and the TF32 rounding of the remainders
 // are below 2^-19 of each product.
-constexpr int kTcProducerWarps = 16;
+constexpr int kTcProducerWarps = 24;
 constexpr int kTcProducers = 32 * kTcProducerWarps;
-constexpr int kTcMmaWarp = 16;
-constexpr int kTcLoaderWarp = 17;
-constexpr int kTcThreads = 32 * 22;  // producers, MMA warp, loader warp, 4 epilogue warps
+constexpr int kTcMmaWarp = kTcProducerWarps;
+constexpr int kTcLoaderWarp = kTcProducerWarps + 1;
+constexpr int kTcThreads = 32 * (kTcProducerWarps + 6);  // producers, MMA, loader, 4 epilogue warps
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -570,21 +572,23 @@ __device__ __forceinline__ uint64_t global_ns() {
   return t;
 }
 
-// Bounded wait for the given phase parity of an mbarrier: gives up after 2^24
-// polls or 2 s, whichever comes first, and returns false.
+// Bounded wait for the given phase parity of an mbarrier: each try suspends the
+// thread until the phase completes or 0.1 ms pass (so waiting warps do not take
+// issue slots from working ones); gives up after 2^16 tries or 2 s, whichever
+// comes first, and returns false.
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
   const uint64_t t0 = global_ns();
-  for (int it = 0; it < (1 << 24); ++it) {
+  for (int it = 0; it < (1 << 16); ++it) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred P1;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2, %3;\n\t"
         "selp.b32 %0, 1, 0, P1;\n\t}\n"
         : "=r"(done)
-        : "r"(bar), "r"(parity)
+        : "r"(bar), "r"(parity), "r"(100000)
         : "memory");
     if (done) return true;
-    if ((it & 255) == 255 && global_ns() - t0 > 2000000000ull) return false;
+    if (global_ns() - t0 > 2000000000ull) return false;
   }
   return false;
 }
@@ -717,15 +721,15 @@ __device__ __forceinline__ TcItem tc_item(const DevArgs &a, int w) {
 }
 
 // Persistent, warp-specialized: grid = min(work items, resident CTAs), block
-// kTcThreads = 22 warps.  Work items as in k_spread_zdft, in the same order in
+// kTcThreads.  Work items as in k_spread_zdft, in the same order in
 // every role:
-//   warps 0-15  producers: zero the stage's A tile, spread the item's atoms
+//   producer warps (kTcProducerWarps): zero the stage's A tile, spread the item's atoms
 //               into it (shared-memory atomics), subtract the padding mean and
 //               split it into the TF32 head (in place) and remainder
-//   warp 16     one lane issues the 3xTF32 MMAs of an item into its TMEM stage
-//   warp 17     loader: home-tile record ranges of an item and bulk copies
+//   next warp   one lane issues the 3xTF32 MMAs of an item into its TMEM stage
+//   next warp   loader: home-tile record ranges of an item and bulk copies
 //               (cp.async.bulk) of its atom records into a staging buffer
-//   warps 18-21 epilogue: TMEM accumulator -> Z (warp w reads lane quarter w%4)
+//   last 4      epilogue: TMEM accumulator -> Z (warp w reads lane quarter w%4)
 // Hand-offs are mbarriers, every wait bounded:
 //   rec_full[b]   loader -> producers (records + ranges of buffer b landed)
 //   rec_empty[b]  producers -> loader (buffer b spread)
@@ -1819,24 +1823,29 @@ int dalloc(SaxsPlan *pl, T **ptr, size_t count) {
   return SAXS_OK;
 }
 
-// Distinct home tiles whose atoms can reach columns [c0, c0+cw) along an axis
-// of length n, for stencils of `order` taps that start at an atom's home column.
-std::vector<int4> home_tile_table(int ext, int n, int order) {
-  std::vector<int4> out;
+// Distinct home bins (width bin_w) whose atoms can reach the columns
+// [c0, c0+cw) of each spread tile along an axis of length n, for stencils of
+// `order` taps that start at an atom's home column.  Returns false when a tile
+// would need more than four bins.
+bool home_tile_table(int ext, int n, int order, int bin_w, std::vector<int4> *out) {
+  out->clear();
   for (int c0 = 0; c0 < ext; c0 += kTile) {
     const int cw = std::min(kTile, ext - c0);
     int h[4] = {-1, -1, -1, -1}, cnt = 0;
     for (int d = 0; d < cw + order - 1; ++d) {
       int x = (c0 - order + 1 + d) % n;
       if (x < 0) x += n;
-      const int t = x / kTile;
+      const int t = x / bin_w;
       bool seen = false;
       for (int k = 0; k < cnt; ++k) seen |= (h[k] == t);
-      if (!seen && cnt < 4) h[cnt++] = t;
+      if (!seen) {
+        if (cnt == 4) return false;
+        h[cnt++] = t;
+      }
     }
-    out.push_back(make_int4(h[0], h[1], h[2], h[3]));
+    out->push_back(make_int4(h[0], h[1], h[2], h[3]));
   }
-  return out;
+  return true;
 }
 
 void frame_geometry(const SaxsPlan *pl, const float box[9], float g[kGeom]) {
@@ -1936,8 +1945,21 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
   a.ntaps = ntaps;
   a.T = p.ntypes;
   a.M = p.nentries;
-  a.tiles[0] = (a.n[0] + kTile - 1) / kTile;
-  a.tiles[1] = (a.n[1] + kTile - 1) / kTile;
+  // home bins 4 columns wide cut the atoms an item visits without reaching its
+  // tile (about half with 8-wide bins, a sixth with 4-wide ones)
+  std::vector<int4> hxt, hyt;
+  a.bin_w = 4;
+  if (!home_tile_table(a.ext[0], a.n[0], a.order, 4, &hxt) ||
+      !home_tile_table(a.ext[1], a.n[1], a.order, 4, &hyt)) {
+    a.bin_w = 8;
+    if (!home_tile_table(a.ext[0], a.n[0], a.order, 8, &hxt) ||
+        !home_tile_table(a.ext[1], a.n[1], a.order, 8, &hyt)) {
+      destroy(pl);
+      return fail(SAXS_E_INVALID, "spline order too large for the spread tiles");
+    }
+  }
+  a.tiles[0] = (a.n[0] + a.bin_w - 1) / a.bin_w;
+  a.tiles[1] = (a.n[1] + a.bin_w - 1) / a.bin_w;
   a.stiles[0] = (a.ext[0] + kTile - 1) / kTile;
   a.stiles[1] = (a.ext[1] + kTile - 1) / kTile;
   a.nbins = a.T * a.tiles[0] * a.tiles[1];
@@ -2169,8 +2191,6 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
   saxs::bspline_moduli(nn[2], ndim, mz.data());
   float g0[kGeom];
   frame_geometry(pl, p.box0, g0);
-  const std::vector<int4> hxt = home_tile_table(ex, a.n[0], a.order);
-  const std::vector<int4> hyt = home_tile_table(ey, a.n[1], a.order);
 
   auto up = [&](void *dst, const void *src, size_t bytes) -> int {
     if (bytes == 0) return SAXS_OK;
