@@ -87,7 +87,7 @@ struct DevArgs {
   int kx_lo, nkx, ky_lo, nky, nkz, nkzp, nkxp, nkyp;
   int zc;  // z rows of twiddles k_spread_zdft holds in shared memory at once
   // tensor-core z-DFT (k_spread_zdft_tc): GEMM N, K, spread rows, stages, TMEM columns
-  int tcN, tcK, tcR, tcS, tcCols, tcRB;
+  int tcN, tcK, tcR, tcS, tcCols, tcRB, tcCap;
   int nf[3];
   int dz;
   float dq, qcut;
@@ -597,25 +597,76 @@ __device__ __forceinline__ float tf32_head(float v) {
   return __uint_as_float(__float_as_uint(v) & 0xFFFFE000u);
 }
 
-// Home-tile record ranges of one item (lane 4*ix + iy of the calling warp owns
-// home tile (hx[ix], hy[iy])), compacted and prefix-summed with shuffles; lane 0
-// writes them to `ta`.  Called by one whole warp.
-__device__ __forceinline__ void tile_atom_ranges_warp(const DevArgs &a, const int4 *home_x,
-                                                      const int4 *home_y, TileAtoms &ta, int f,
-                                                      int t, int x0, int y0) {
+// Shared-memory bytes per entry of the spreading pre-pass atom table (the plan
+// sizes the table, DevArgs::tcCap entries).
+constexpr int kTcAtomBytes = 3 * 16 + 16 + 2 * 4;  // wx, wy, wz (float4), z offsets (int4), lx, ly
+
+// What the loader publishes with an item's records: the home-bin record ranges,
+// the item's frame, type and tile, and its padding mean.
+struct TcSlot {
+  TileAtoms ta;
+  int f, t, x0, y0, cw, ch;
+  float mean;
+};
+
+// Grid-stride walk over work items w = ((f*T + t)*sy + ty)*sx + tx without
+// divisions after the first item: each step adds the grid size digit by digit.
+struct ItemIter {
+  int tx, ty, t, f;
+  int dtx, dty, dt, df;
+  int sx, sy, T;
+  __device__ __forceinline__ void init(const DevArgs &a, int w0, int g) {
+    sx = a.stiles[0];
+    sy = a.stiles[1];
+    T = a.T;
+    const int st = sx * sy;
+    tx = (w0 % st) % sx;
+    ty = (w0 % st) / sx;
+    t = (w0 / st) % T;
+    f = (w0 / st) / T;
+    dtx = (g % st) % sx;
+    dty = (g % st) / sx;
+    dt = (g / st) % T;
+    df = (g / st) / T;
+  }
+  __device__ __forceinline__ void next() {
+    tx += dtx;
+    int c = tx >= sx;
+    if (c) tx -= sx;
+    ty += dty + c;
+    c = ty >= sy;
+    if (c) ty -= sy;
+    t += dt + c;
+    c = t >= T;
+    if (c) t -= T;
+    f += df + c;
+  }
+};
+
+// Loader, first half: lane 4*iy + ix of the calling warp loads the record range
+// of home bin (hx[ix], hy[iy]) (bins adjacent in x are adjacent in memory).
+__device__ __forceinline__ void home_ranges_load(const DevArgs &a, const int4 *home_x,
+                                                 const int4 *home_y, int f, int t, int x0, int y0,
+                                                 int &s0, int &cnt, bool &valid) {
   const int lane = threadIdx.x & 31;
   const int4 hxv = home_x[x0 / kTile], hyv = home_y[y0 / kTile];
-  const int ix = (lane >> 2) & 3, iy = lane & 3;
+  const int iy = (lane >> 2) & 3, ix = lane & 3;
   const int hx = ix == 0 ? hxv.x : ix == 1 ? hxv.y : ix == 2 ? hxv.z : hxv.w;
   const int hy = iy == 0 ? hyv.x : iy == 1 ? hyv.y : iy == 2 ? hyv.z : hyv.w;
-  const bool valid = lane < 16 && hx >= 0 && hy >= 0;
-  int s0 = 0, cnt = 0;
+  valid = lane < 16 && hx >= 0 && hy >= 0;
+  s0 = 0;
+  cnt = 0;
   if (valid) {
     const int *off = a.offsets + static_cast<int64_t>(f) * (a.nbins + 1);
     const int bin = (t * a.tiles[1] + hy) * a.tiles[0] + hx;
     s0 = off[bin];
     cnt = off[bin + 1] - s0;
   }
+}
+
+// Loader, second half: compaction and prefix sum of the ranges into `ta`.
+__device__ __forceinline__ void home_ranges_publish(TileAtoms &ta, int s0, int cnt, bool valid) {
+  const int lane = threadIdx.x & 31;
   const unsigned bal = __ballot_sync(0xffffffffu, valid);
   const int pos = __popc(bal & ((1u << lane) - 1u));
   int inc = cnt;
@@ -624,72 +675,93 @@ __device__ __forceinline__ void tile_atom_ranges_warp(const DevArgs &a, const in
     const int v = __shfl_up_sync(0xffffffffu, inc, d);
     if (lane >= d) inc += v;
   }
-  // lane 0 gathers (pos, start, inclusive count) of the valid lanes and writes them
-  int nb = 0;
-  for (int l = 0; l < 16; ++l) {
-    const int sl = __shfl_sync(0xffffffffu, s0, l);
-    const int il = __shfl_sync(0xffffffffu, inc, l);
-    if ((bal >> l) & 1u) {
-      if (lane == 0) {
-        ta.start[nb] = sl;
-        ta.cum[nb + 1] = il;
-      }
-      ++nb;
-    }
+  if (valid) {
+    ta.start[pos] = s0;
+    ta.cum[pos + 1] = inc;
   }
   if (lane == 0) {
     ta.cum[0] = 0;
-    ta.nb = nb;
+    ta.nb = __popc(bal);
   }
-  (void)pos;
 }
 
-// Spreading of one column tile into the K-major A layout, one thread per
-// (atom, z tap): the four lanes of an atom write four different banks.  Records
-// [0, nrec_smem) come from the shared-memory copy, the rest from global memory.
-__device__ __forceinline__ void spread_tile_kmajor(const DevArgs &a, const TileAtoms &ta,
-                                                   const float4 *srec, int nrec_smem, float *A,
-                                                   int f, int x0, int y0, int cw, int ch, int tid,
-                                                   int nthreads) {
-  const float4 *rec = a.rec + static_cast<int64_t>(f) * a.M;
+// Shared-memory atom table of the spreading pre-pass (struct of arrays).
+struct AtomTab {
+  float4 *wx, *wy, *wz;  // B-spline weights of the four taps per axis
+  int4 *zo;              // A-tile offsets (z/4)*256 + z%4 of the four z taps
+  int *lx, *ly;          // tile column of each x / y tap, one byte each, 0xFF outside
+};
+
+// Spreading pre-pass: atom v0 + i (i < nv) -> weights, z offsets and in-tile tap
+// columns.  Records [0, nrec_smem) come from the staged copy, the rest from
+// global memory.
+__device__ __forceinline__ void spread_prepass(const DevArgs &a, const TileAtoms &ta,
+                                               const float4 *srec, int nrec_smem, int f, int v0,
+                                               int nv, const AtomTab &tab, int x0, int y0, int cw,
+                                               int ch, int tid) {
   const int P = a.order, nt = a.ntaps, nz = a.n[2];
-  const int total = ta.cum[ta.nb] * nt;
-  for (int k = tid; k < total; k += nthreads) {
-    const int v = nt == 4 ? (k >> 2) : k / nt;
-    const int r = k - v * nt;
+  for (int i = tid; i < nv; i += kTcProducers) {
+    const int v = v0 + i;
     float4 q;
     if (v < nrec_smem) {
       q = srec[v];
     } else {
       int j = 0;
       while (v >= ta.cum[j + 1]) ++j;
-      q = rec[ta.start[j] + (v - ta.cum[j])];
+      q = a.rec[static_cast<int64_t>(f) * a.M + ta.start[j] + (v - ta.cum[j])];
     }
     const int m0 = static_cast<int>(q.x), m1 = static_cast<int>(q.y), m2 = static_cast<int>(q.z);
     float wx[4], wy[4], wz[4];
     cubic_weights(q.x - static_cast<float>(m0), wx);
     cubic_weights(q.y - static_cast<float>(m1), wy);
     cubic_weights(q.z - static_cast<float>(m2), wz);
-    const float wzr = r == 0 ? wz[0] : r == 1 ? wz[1] : r == 2 ? wz[2] : wz[3];
-    int z = m2 - P + r;
-    if (z < 0) z += nz;
-    float *colz = A + (z >> 2) * 256 + (z & 3);
+    int lxp = 0, lyp = 0, zo[4];
 #pragma unroll
     for (int o = 0; o < 4; ++o) {
-      if (o >= nt) break;
-      int x = m0 - P + o;
-      if (x < 0) x += a.n[0];
-      const int lx = x - x0;
-      if (static_cast<unsigned>(lx) >= static_cast<unsigned>(cw)) continue;
-#pragma unroll
-      for (int p = 0; p < 4; ++p) {
-        if (p >= nt) break;
-        int y = m1 - P + p;
+      int bx = 0xFF, by = 0xFF, zz = 0;
+      if (o < nt) {
+        int x = m0 - P + o;
+        if (x < 0) x += a.n[0];
+        if (static_cast<unsigned>(x - x0) < static_cast<unsigned>(cw)) bx = x - x0;
+        int y = m1 - P + o;
         if (y < 0) y += a.n[1];
-        const int ly = y - y0;
-        if (static_cast<unsigned>(ly) >= static_cast<unsigned>(ch)) continue;
-        atomicAdd(colz + lx * 32 + ly * 4, (wx[o] * wy[p]) * wzr);
+        if (static_cast<unsigned>(y - y0) < static_cast<unsigned>(ch)) by = y - y0;
+        int z = m2 - P + o;
+        if (z < 0) z += nz;
+        zz = (z >> 2) * 256 + (z & 3);
       }
+      lxp |= bx << (8 * o);
+      lyp |= by << (8 * o);
+      zo[o] = zz;
+    }
+    tab.wx[i] = make_float4(wx[0], wx[1], wx[2], wx[3]);
+    tab.wy[i] = make_float4(wy[0], wy[1], wy[2], wy[3]);
+    tab.wz[i] = make_float4(wz[0], wz[1], wz[2], wz[3]);
+    tab.zo[i] = make_int4(zo[0], zo[1], zo[2], zo[3]);
+    tab.lx[i] = lxp;
+    tab.ly[i] = lyp;
+  }
+}
+
+// Spreading taps: one lane per (atom, y tap, z tap), four x taps each.  The 16
+// lanes of an atom write 16 different banks (bank = 4*ly + z%4).
+__device__ __forceinline__ void spread_taps(const AtomTab &tab, int nv, int nt, float *A, int tid) {
+  for (int u = tid; u < nv * 16; u += kTcProducers) {
+    const int i = u >> 4, p = (u >> 2) & 3, r = u & 3;
+    if (p >= nt || r >= nt) continue;
+    const int ly = (tab.ly[i] >> (8 * p)) & 0xFF;
+    const int lxp = tab.lx[i];
+    if (ly == 0xFF || lxp == -1) continue;
+    const float wy = reinterpret_cast<const float *>(&tab.wy[i])[p];
+    const float wz = reinterpret_cast<const float *>(&tab.wz[i])[r];
+    const int zo = reinterpret_cast<const int *>(&tab.zo[i])[r];
+    const float4 wx4 = tab.wx[i];
+    const float wx[4] = {wx4.x, wx4.y, wx4.z, wx4.w};
+    float *col = A + zo + ly * 4;
+#pragma unroll
+    for (int o = 0; o < 4; ++o) {
+      const int lx = (lxp >> (8 * o)) & 0xFF;
+      if (lx != 0xFF) atomicAdd(col + lx * 32, (wx[o] * wy) * wz);
     }
   }
 }
@@ -702,47 +774,44 @@ __device__ __forceinline__ void producers_sync() {
   asm volatile("bar.sync 1, %0;" ::"r"(kTcProducers) : "memory");
 }
 
-// Work item w -> (frame, type, tile origin, tile extent).
-struct TcItem {
-  int f, t, x0, y0, cw, ch;
-};
-
-__device__ __forceinline__ TcItem tc_item(const DevArgs &a, int w) {
-  const int st = a.stiles[0] * a.stiles[1];
-  TcItem it;
-  it.f = w / (a.T * st);
-  it.t = (w / st) % a.T;
-  const int tl = w % st;
-  it.x0 = (tl % a.stiles[0]) * kTile;
-  it.y0 = (tl / a.stiles[0]) * kTile;
-  it.cw = min(kTile, a.ext[0] - it.x0);
-  it.ch = min(kTile, a.ext[1] - it.y0);
-  return it;
+// Producer barrier that also returns the OR of `v` over the producers.
+__device__ __forceinline__ bool producers_sync_or(bool v) {
+  uint32_t out;
+  asm volatile(
+      "{\n\t.reg .pred pi, po;\n\t"
+      "setp.ne.u32 pi, %1, 0;\n\t"
+      "bar.red.or.pred po, 1, %2, pi;\n\t"
+      "selp.u32 %0, 1, 0, po;\n\t}\n"
+      : "=r"(out)
+      : "r"(static_cast<uint32_t>(v)), "r"(kTcProducers)
+      : "memory");
+  return out != 0;
 }
 
 // Persistent, warp-specialized: grid = min(work items, resident CTAs), block
-// kTcThreads.  Work items as in k_spread_zdft, in the same order in
-// every role:
-//   producer warps (kTcProducerWarps): zero the stage's A tile, spread the item's atoms
-//               into it (shared-memory atomics), subtract the padding mean and
-//               split it into the TF32 head (in place) and remainder
+// kTcThreads.  Work items as in k_spread_zdft, in the same order in every role:
+//   producer warps (kTcProducerWarps): zero the stage's A tile, spread the
+//               item's atoms into it (a per-atom pre-pass, then shared-memory
+//               atomics per tap), subtract the padding mean and split it into
+//               the TF32 head (in place) and remainder
 //   next warp   one lane issues the 3xTF32 MMAs of an item into its TMEM stage
-//   next warp   loader: home-tile record ranges of an item and bulk copies
-//               (cp.async.bulk) of its atom records into a staging buffer
+//   next warp   loader: home-bin record ranges, frame/type/tile and padding mean
+//               of an item, and bulk copies (cp.async.bulk) of its atom records
+//               into a staging buffer
 //   last 4      epilogue: TMEM accumulator -> Z (warp w reads lane quarter w%4)
 // Hand-offs are mbarriers, every wait bounded:
-//   rec_full[b]   loader -> producers (records + ranges of buffer b landed)
-//   rec_empty[b]  producers -> loader (buffer b spread)
+//   rec_full[b]   loader -> producers (records + item data of slot b landed)
+//   rec_empty[b]  producers -> loader (slot b spread)
 //   full[s]       producers -> MMA (stage s operands written)
 //   done[s]       MMA commit -> epilogue (accumulator ready) and producers
 //                 (stage s operands free again)
 //   tmem_empty[s] epilogue -> MMA (TMEM stage s read out)
 // Dynamic shared memory: Bh, Bl (tcK x tcN floats each), tcS stages of
-// A32 (tcR x 64) + Al (tcK x 64), two record buffers of tcRB float4, and the
-// home-tile tables (stiles[0] + stiles[1] int4).
+// A32 (tcR x 64) + Al (tcK x 64), two record buffers of tcRB float4, the
+// home-bin tables (stiles[0] + stiles[1] int4) and the atom table.
 __global__ void __launch_bounds__(kTcThreads, 1) k_spread_zdft_tc(DevArgs a, int items) {
   extern __shared__ __align__(16) unsigned char smem[];  // no-swizzle operands need 16 B
-  __shared__ TileAtoms ta[2];
+  __shared__ TcSlot slot[2];
   __shared__ __align__(8) uint64_t bars[10];
   __shared__ uint32_t tmem_slot;
   __shared__ volatile int abort_flag;
@@ -754,6 +823,14 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_spread_zdft_tc(DevArgs a, int
   float4 *recs = reinterpret_cast<float4 *>(stages + static_cast<size_t>(S) * (R + KT) * 64);
   int4 *home_x = reinterpret_cast<int4 *>(recs + 2 * RB);
   int4 *home_y = home_x + a.stiles[0];
+  AtomTab tab;
+  tab.wx = reinterpret_cast<float4 *>(home_y + a.stiles[1]);
+  const int cap = a.tcCap;
+  tab.wy = tab.wx + cap;
+  tab.wz = tab.wy + cap;
+  tab.zo = reinterpret_cast<int4 *>(tab.wz + cap);
+  tab.lx = reinterpret_cast<int *>(tab.zo + cap);
+  tab.ly = tab.lx + cap;
   uint64_t *rec_full = bars, *rec_empty = bars + 2, *full = bars + 4, *done = bars + 6,
            *tmem_empty = bars + 8;
   {
@@ -797,26 +874,33 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_spread_zdft_tc(DevArgs a, int
       const int b = j & 1, s = S == 2 ? (j & 1) : 0;
       float *A32 = stages + static_cast<size_t>(s) * (R + KT) * 64;
       float *Al = A32 + static_cast<size_t>(R) * 64;
-      const TcItem it = tc_item(a, w);
       if (j >= S) wait(&done[s], (j - S) / S);  // the stage's previous MMAs are finished
       {
         float4 *t4 = reinterpret_cast<float4 *>(A32);
         for (int i = tid; i < R * 16; i += kTcProducers) t4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
       }
       wait(&rec_full[b], j >> 1);
-      producers_sync();
-      if (!abort_flag) {
-        const int nrec = min(ta[b].cum[ta[b].nb], RB);
-        spread_tile_kmajor(a, ta[b], recs + static_cast<size_t>(b) * RB, nrec, A32, it.f, it.x0,
-                           it.y0, it.cw, it.ch, tid, kTcProducers);
+      // one decision for all producers: the spreading below has barriers inside
+      const bool skip = producers_sync_or(abort_flag != 0);
+      const TcSlot &sl = slot[b];
+      const float mean = sl.mean;
+      if (!skip) {
+        const int nvis = sl.ta.cum[sl.ta.nb];
+        const int nrec = min(nvis, RB);
+        for (int v0 = 0; v0 < nvis; v0 += cap) {
+          const int nv = min(cap, nvis - v0);
+          if (v0 > 0) producers_sync();  // the previous chunk's taps have read the table
+          spread_prepass(a, sl.ta, recs + static_cast<size_t>(b) * RB, nrec, sl.f, v0, nv, tab, sl.x0,
+                         sl.y0, sl.cw, sl.ch, tid);
+          producers_sync();
+          spread_taps(tab, nv, a.ntaps, A32, tid);
+        }
       }
       producers_sync();
       if (tid == 0) mbar_arrive(smem_addr(&rec_empty[b]));
       {
         // padding mean applied before the TF32 split: the tensor cores see
         // g - mean (rows z >= ez meet zero twiddles)
-        const float mean = static_cast<float>(
-            a.border[static_cast<int64_t>(it.f) * a.T + it.t] / a.border_count);
         float4 *h4 = reinterpret_cast<float4 *>(A32);
         float4 *l4 = reinterpret_cast<float4 *>(Al);
         for (int i = tid; i < KT * 16; i += kTcProducers) {
@@ -879,51 +963,74 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_spread_zdft_tc(DevArgs a, int
       if (abort_flag && last_bar) mbar_wait(last_bar, static_cast<uint32_t>(last_parity & 1));
     }
   } else if (warp == kTcLoaderWarp) {
-    const float4 *rec_all = a.rec;
+    ItemIter it;
+    it.init(a, blockIdx.x, gridDim.x);
     int j = 0;
-    for (int w = blockIdx.x; w < items && !abort_flag; w += gridDim.x, ++j) {
+    for (int w = blockIdx.x; w < items; w += gridDim.x, ++j, it.next()) {
       const int b = j & 1;
-      const TcItem it = tc_item(a, w);
+      const int x0 = it.tx * kTile, y0 = it.ty * kTile;
+      int s0, cnt;
+      bool valid;
+      // the range and mean loads are issued before the wait for the slot
+      home_ranges_load(a, home_x, home_y, it.f, it.t, x0, y0, s0, cnt, valid);
+      const double bsum = a.border[static_cast<int64_t>(it.f) * a.T + it.t];
       if (j >= 2) wait(&rec_empty[b], (j - 2) >> 1);
-      if (abort_flag) break;
-      tile_atom_ranges_warp(a, home_x, home_y, ta[b], it.f, it.t, it.x0, it.y0);
+      if (__any_sync(0xffffffffu, abort_flag != 0)) break;
+      TcSlot &sl = slot[b];
+      home_ranges_publish(sl.ta, s0, cnt, valid);
+      if (lane == 0) {
+        sl.f = it.f;
+        sl.t = it.t;
+        sl.x0 = x0;
+        sl.y0 = y0;
+        sl.cw = min(kTile, a.ext[0] - x0);
+        sl.ch = min(kTile, a.ext[1] - y0);
+        sl.mean = static_cast<float>(bsum / a.border_count);
+      }
       __syncwarp();
       if (lane == 0) {
-        const TileAtoms &tb = ta[b];
+        const TileAtoms &tb = sl.ta;
         const int nrec = min(tb.cum[tb.nb], RB);
         const uint32_t bar = smem_addr(&rec_full[b]);
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
                      "r"(nrec * 16)
                      : "memory");
-        const float4 *src = rec_all + static_cast<int64_t>(it.f) * a.M;
+        const float4 *src = a.rec + static_cast<int64_t>(it.f) * a.M;
         const uint32_t dst = smem_addr(recs + static_cast<size_t>(b) * RB);
-        for (int r = 0; r < tb.nb; ++r) {
-          const int lo = tb.cum[r], hi = min(tb.cum[r + 1], nrec);
+        // one bulk copy per run of ranges that are contiguous in global memory
+        int r = 0;
+        while (r < tb.nb && tb.cum[r] < nrec) {
+          int e = r;
+          while (e + 1 < tb.nb && tb.start[e + 1] == tb.start[e] + (tb.cum[e + 1] - tb.cum[e])) ++e;
+          const int lo = tb.cum[r], hi = min(tb.cum[e + 1], nrec);
           if (hi > lo)
             asm volatile(
                 "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
                     dst + static_cast<uint32_t>(lo) * 16),
                 "l"(src + tb.start[r]), "r"((hi - lo) * 16), "r"(bar)
                 : "memory");
+          r = e + 1;
         }
       }
     }
   } else {
     // epilogue warps
     const int quarter = warp & 3;
+    ItemIter it;
+    it.init(a, blockIdx.x, gridDim.x);
+    const int64_t zplane = static_cast<int64_t>(a.ext[0]) * a.ext[1];
     int j = 0;
-    for (int w = blockIdx.x; w < items && !abort_flag; w += gridDim.x, ++j) {
+    for (int w = blockIdx.x; w < items; w += gridDim.x, ++j, it.next()) {
       const int s = S == 2 ? (j & 1) : 0;
       wait(&done[s], j / S);
-      if (abort_flag) break;
+      if (__any_sync(0xffffffffu, abort_flag != 0)) break;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const TcItem it = tc_item(a, w);
-      const int64_t zplane = static_cast<int64_t>(a.ext[0]) * a.ext[1];
+      const int x0 = it.tx * kTile, y0 = it.ty * kTile;
       float2 *Zft = a.Z + (static_cast<int64_t>(it.f) * a.T + it.t) * a.nkz * zplane;
       // with M = 64, row c of D sits in TMEM lane (c % 16) + 32 * (c / 16)
       const int c = 16 * quarter + lane, lx = c >> 3, ly = c & 7;
-      const bool valid = lane < 16 && lx < it.cw && ly < it.ch;
-      const int64_t cell = static_cast<int64_t>(it.x0 + lx) * a.ext[1] + (it.y0 + ly);
+      const bool valid = lane < 16 && lx < min(kTile, a.ext[0] - x0) && ly < min(kTile, a.ext[1] - y0);
+      const int64_t cell = static_cast<int64_t>(x0 + lx) * a.ext[1] + (y0 + ly);
       const uint32_t lane_base = tmem + (static_cast<uint32_t>(32 * quarter) << 16) + static_cast<uint32_t>(s * N);
       for (int c0 = 0; c0 < N; c0 += 8) {
         uint32_t r[8];
@@ -2041,15 +2148,19 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
     const size_t b_bytes = 2 * static_cast<size_t>(KT) * N * sizeof(float);
     const size_t stage_bytes = static_cast<size_t>(R + KT) * 64 * sizeof(float);
     const size_t home_bytes = static_cast<size_t>(a.stiles[0] + a.stiles[1]) * sizeof(int4);
-    // two operand stages before larger record buffers; records beyond the
-    // staging buffer are read from global memory
-    int S = 0, RB = 0;
+    // two operand stages before larger record buffers before a larger atom
+    // table; records beyond the staging buffer are read from global memory,
+    // atoms beyond the table are spread in further chunks
+    int S = 0, RB = 0, CAP = 0;
     for (int s_try = 2; s_try >= 1 && S == 0; --s_try)
       for (int rb = 1024; rb >= 128 && S == 0; rb /= 2)
-        if (b_bytes + s_try * stage_bytes + 2 * static_cast<size_t>(rb) * 16 + home_bytes <= avail) {
-          S = s_try;
-          RB = rb;
-        }
+        for (int cap = 256; cap >= 64 && S == 0; cap /= 2)
+          if (b_bytes + s_try * stage_bytes + 2 * static_cast<size_t>(rb) * 16 + home_bytes +
+                  static_cast<size_t>(cap) * kTcAtomBytes <= avail) {
+            S = s_try;
+            RB = rb;
+            CAP = cap;
+          }
     if (!simt_only && N <= 256 && S > 0) {
       pl->use_tc = true;
       a.tcN = N;
@@ -2057,10 +2168,12 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
       a.tcR = R;
       a.tcS = S;
       a.tcRB = RB;
+      a.tcCap = CAP;
       int cols = 32;
       while (cols < S * N) cols *= 2;
       a.tcCols = cols;
-      pl->smem_spread_tc = b_bytes + S * stage_bytes + 2 * static_cast<size_t>(RB) * 16 + home_bytes;
+      pl->smem_spread_tc = b_bytes + S * stage_bytes + 2 * static_cast<size_t>(RB) * 16 + home_bytes +
+                           static_cast<size_t>(CAP) * kTcAtomBytes;
     }
   }
   pl->smem_hist = a.num_bins <= kHistSmemBins ? 2 * sizeof(double) * a.num_bins : 0;
