@@ -88,6 +88,8 @@ struct DevArgs {
   int zc;  // z rows of twiddles k_spread_zdft holds in shared memory at once
   // tensor-core z-DFT (k_spread_zdft_tc): GEMM N, K, spread rows, stages, TMEM columns
   int tcN, tcK, tcR, tcS, tcCols, tcRB, tcCap;
+  // tensor-core y-axis DFT (k_ydft_tc): GEMM N', K chunks, stages, TMEM columns
+  int ytcN, ytcChunks, ytcS, ytcCols;
   int nf[3];
   int dz;
   float dq, qcut;
@@ -106,6 +108,7 @@ struct DevArgs {
   const float *ff;    // [T][9]
   const float *twz_sum; // [2*nkzp]: sum over z < ez of the z twiddles (re, im)
   const float *twz_tc;  // [2][tcK x tcN]: z twiddles as TF32 head / remainder, K-major
+  const float *twy_tc;  // [chunk][2][ytcN x 2*kYtcChunk]: y-DFT B' operand, head / remainder
   const int4 *home_x; // per spread tile along x: home tiles whose atoms reach it (-1 padded)
   const int4 *home_y;
   int2 *key;
@@ -1128,6 +1131,230 @@ __global__ void __launch_bounds__(kThreads) k_ydft(DevArgs a) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Tensor-core y-axis DFT (tcgen05, 3xTF32)
+// ---------------------------------------------------------------------------
+//
+// Per z-transformed plane (frame, type, kz) and block of 128 x rows, the y-axis
+// DFT is the real GEMM  D[x][n'] = sum_k' A[x][k'] B'[k'][n']  with
+//   A[x][2y + c] = component c (0 re, 1 im) of Z[x][y]  (the plane's own memory
+//                  layout read as floats), K' = 2*ey,
+//   B'[2y + c][2ky + d] = { Wr, Wi ; -Wi, Wr }[c][d] of W[y][ky], the y twiddles,
+//   D[x][2ky + d] = component d of Y[ky][x],  N' = 2*nky padded to 16.
+// K is streamed in chunks of kYtcChunk y values.  Operands are K-major,
+// no-swizzle (core matrices of 8 rows x 16 B): A element (x, k') at
+// (k'/4)*512 + (x/8)*32 + (x%8)*4 + k'%4 floats (LBO 2048 B, SBO 128 B); B'
+// element (n', k') at (k'/4)*(N'/8)*32 + (n'/8)*32 + (n'%8)*4 + k'%4 (LBO N'*16
+// B, SBO 128 B).  Both are split into a TF32 head and remainder like the z-axis
+// DFT's operands.
+constexpr int kYtcChunk = 16;                  // y values per K chunk (K' = 32)
+constexpr int kYtcProducerWarps = 8;
+constexpr int kYtcProducers = 32 * kYtcProducerWarps;
+constexpr int kYtcMmaWarp = kYtcProducerWarps;
+constexpr int kYtcLoaderWarp = kYtcProducerWarps + 1;
+constexpr int kYtcThreads = 32 * (kYtcProducerWarps + 6);  // producers, MMA, loader, 4 epilogue
+constexpr int kYtcMaxStages = 4;
+
+// Persistent, warp-specialized: grid = min(items, resident CTAs), block
+// kYtcThreads; an item is (plane, block of 128 x rows), planes ordered
+// (frame, type, kz) like Z and Y.  Barriers (all waits bounded):
+//   afull[st] producers -> MMA (A chunk of stage st split and written)
+//   bfull[st] loader bulk copy -> MMA (B' chunk landed)
+//   empty[st] MMA commit -> producers and loader (stage st read)
+//   dfull[d]  MMA commit -> epilogue (accumulator d complete)
+//   dempty[d] epilogue -> MMA (accumulator d read out)
+// Dynamic shared memory: ytcS stages of { A head, A remainder (128 x K'),
+// B' head, B' remainder (N' x K') } floats.
+__global__ void __launch_bounds__(kYtcThreads, 1) k_ydft_tc(DevArgs a, int items) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ __align__(8) uint64_t bars[3 * kYtcMaxStages + 4];
+  __shared__ uint32_t tmem_slot;
+  __shared__ volatile int abort_flag;
+  const int N = a.ytcN, NS = a.ytcS, NC = a.ytcChunks;
+  const int KP = 2 * kYtcChunk;                      // K' per chunk
+  const int a_floats = 128 * KP, b_floats = N * KP;  // per head or remainder
+  const int stage_floats = 2 * a_floats + 2 * b_floats;
+  const int ex = a.ext[0], ey = a.ext[1];
+  const int xblocks = (ex + 127) / 128;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  float *stages = reinterpret_cast<float *>(smem);
+  uint64_t *afull = bars, *bfull = bars + kYtcMaxStages, *empty = bars + 2 * kYtcMaxStages,
+           *dfull = bars + 3 * kYtcMaxStages, *dempty = dfull + 2;
+  if (warp == kYtcMmaWarp) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_addr(&tmem_slot)),
+                 "r"(a.ytcCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+  }
+  if (tid == 0) {
+    for (int i = 0; i < NS; ++i) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&afull[i])), "r"(kYtcProducerWarps));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&bfull[i])), "r"(1));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&empty[i])), "r"(1));
+    }
+    for (int d = 0; d < 2; ++d) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&dfull[d])), "r"(1));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&dempty[d])), "r"(4));
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    abort_flag = 0;
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_slot;
+
+  auto wait = [&](uint64_t *bar, int parity) {
+    if (abort_flag) return;
+    if (!mbar_wait(smem_addr(bar), static_cast<uint32_t>(parity & 1))) {
+      abort_flag = 1;
+      atomicExch(a.status, 1);
+    }
+  };
+
+  if (warp < kYtcProducerWarps) {
+    int g = 0;
+    for (int w = blockIdx.x; w < items; w += gridDim.x) {
+      const int64_t plane = w / xblocks;
+      const int xb = (w % xblocks) * 128;
+      const float2 *Zp = a.Z + plane * ex * ey;
+      for (int c = 0; c < NC; ++c, ++g) {
+        const int st = g % NS;
+        if (g >= NS) wait(&empty[st], g / NS - 1);
+        float *ah = stages + static_cast<size_t>(st) * stage_floats;
+        float *al = ah + a_floats;
+        // 128 rows x 8 float4 (two complex values each); 8 lanes per row
+        for (int i = tid; i < 128 * (kYtcChunk / 2); i += kYtcProducers) {
+          const int x = i >> 3, q = i & 7;
+          const int gx = xb + x, y = c * kYtcChunk + 2 * q;
+          float2 u0 = make_float2(0.f, 0.f), u1 = make_float2(0.f, 0.f);
+          if (gx < ex) {
+            const float2 *row = Zp + static_cast<int64_t>(gx) * ey;
+            if (y < ey) u0 = row[y];
+            if (y + 1 < ey) u1 = row[y + 1];
+          }
+          const float4 v = make_float4(u0.x, u0.y, u1.x, u1.y);
+          const float4 h = make_float4(tf32_head(v.x), tf32_head(v.y), tf32_head(v.z), tf32_head(v.w));
+          const int o = q * 512 + (x >> 3) * 32 + (x & 7) * 4;
+          *reinterpret_cast<float4 *>(ah + o) = h;
+          *reinterpret_cast<float4 *>(al + o) = make_float4(v.x - h.x, v.y - h.y, v.z - h.z, v.w - h.w);
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncwarp();
+        if (lane == 0) mbar_arrive(smem_addr(&afull[st]));
+      }
+    }
+  } else if (warp == kYtcLoaderWarp) {
+    if (lane == 0) {
+      const uint32_t bytes = static_cast<uint32_t>(2 * b_floats * sizeof(float));
+      int g = 0;
+      for (int w = blockIdx.x; w < items && !abort_flag; w += gridDim.x) {
+        for (int c = 0; c < NC; ++c, ++g) {
+          const int st = g % NS;
+          if (g >= NS) wait(&empty[st], g / NS - 1);
+          if (abort_flag) break;
+          const uint32_t bar = smem_addr(&bfull[st]);
+          const uint32_t dst = smem_addr(stages + static_cast<size_t>(st) * stage_floats + 2 * a_floats);
+          asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+                       : "memory");
+          asm volatile(
+              "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+              "l"(a.twy_tc + static_cast<size_t>(c) * 2 * b_floats), "r"(bytes), "r"(bar)
+              : "memory");
+        }
+      }
+    }
+  } else if (warp == kYtcMmaWarp) {
+    if (lane == 0) {
+      // kind::tf32: D f32, A and B tf32, both K-major, N >> 3 at bit 17, M = 128
+      const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) |
+                             (static_cast<uint32_t>(N >> 3) << 17) | (static_cast<uint32_t>(128 >> 4) << 24);
+      int g = 0, i = 0;
+      uint32_t last_bar = 0;
+      int last_parity = 0;
+      for (int w = blockIdx.x; w < items && !abort_flag; w += gridDim.x, ++i) {
+        const int d = i & 1;
+        if (i >= 2) wait(&dempty[d], (i - 2) >> 1);
+        const uint32_t dcol = tmem + static_cast<uint32_t>(d * N);
+        for (int c = 0; c < NC; ++c, ++g) {
+          const int st = g % NS;
+          wait(&afull[st], g / NS);
+          wait(&bfull[st], g / NS);
+          if (abort_flag) break;
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const float *ah = stages + static_cast<size_t>(st) * stage_floats;
+          const uint64_t dah0 = umma_desc(smem_addr(ah), 2048, 128);
+          const uint64_t dal0 = umma_desc(smem_addr(ah + a_floats), 2048, 128);
+          const uint64_t dbh0 = umma_desc(smem_addr(ah + 2 * a_floats), N * 16, 128);
+          const uint64_t dbl0 = umma_desc(smem_addr(ah + 2 * a_floats + b_floats), N * 16, 128);
+          // one k step (8 of K'): A advances 4096 B (+256), B' N*32 B (+N*2)
+          for (int kk = 0; kk < KP / 8; ++kk) {
+            const uint64_t dah = dah0 + static_cast<uint64_t>(kk * 256);
+            const uint64_t dal = dal0 + static_cast<uint64_t>(kk * 256);
+            const uint64_t dbh = dbh0 + static_cast<uint64_t>(kk * 2 * N);
+            const uint64_t dbl = dbl0 + static_cast<uint64_t>(kk * 2 * N);
+            umma_tf32(dcol, dal, dbh, idesc, (c > 0 || kk > 0) ? 1u : 0u);
+            umma_tf32(dcol, dah, dbl, idesc, 1u);
+            umma_tf32(dcol, dah, dbh, idesc, 1u);
+          }
+          asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                           smem_addr(&empty[st]))
+                       : "memory");
+          last_bar = smem_addr(&empty[st]);
+          last_parity = g / NS;
+        }
+        if (abort_flag) break;
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                         smem_addr(&dfull[d]))
+                     : "memory");
+      }
+      if (abort_flag && last_bar) mbar_wait(last_bar, static_cast<uint32_t>(last_parity & 1));
+    }
+  } else {
+    // epilogue: warp w reads TMEM lanes 32*(w%4).. = x rows of the block
+    const int quarter = warp & 3;
+    int i = 0;
+    for (int w = blockIdx.x; w < items; w += gridDim.x, ++i) {
+      const int d = i & 1;
+      wait(&dfull[d], i >> 1);
+      if (__any_sync(0xffffffffu, abort_flag != 0)) break;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const int64_t plane = w / xblocks;
+      const int x = (w % xblocks) * 128 + 32 * quarter + lane;
+      float2 *Yp = a.Y + plane * a.nky * ex;
+      const uint32_t lane_base = tmem + (static_cast<uint32_t>(32 * quarter) << 16) + static_cast<uint32_t>(d * N);
+      for (int c0 = 0; c0 < N; c0 += 16) {
+        uint32_t r[16];
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+            "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+              "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+              "=r"(r[14]), "=r"(r[15])
+            : "r"(lane_base + c0));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (x < ex) {
+#pragma unroll
+          for (int jj = 0; jj < 8; ++jj) {
+            const int ky = c0 / 2 + jj;
+            if (ky < a.nky)
+              Yp[static_cast<int64_t>(ky) * ex + x] =
+                  make_float2(__uint_as_float(r[2 * jj]), __uint_as_float(r[2 * jj + 1]));
+          }
+        }
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(smem_addr(&dempty[d]));
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (warp == kYtcMmaWarp)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(a.ytcCols));
+}
+
 // grid (ceil(nky/4), nkz, frames), block 256: x-axis DFT, form factors, type
 // sum, modulus.  Dynamic shared memory, for an x chunk of `xc` values:
 // twx xc*nkxp | Y rows T*xc | F T*nkxp (all float2).
@@ -1879,6 +2106,9 @@ struct SaxsPlan {
   bool use_tc = false;  // z-axis DFT on the tensor cores (k_spread_zdft_tc)
   size_t smem_spread_tc = 0;
   int tc_ctas = 1;
+  bool use_ytc = false;  // y-axis DFT on the tensor cores (k_ydft_tc)
+  size_t smem_ydft_tc = 0;
+  int ytc_ctas = 1;
   int xc = 1;           // x values per shared-memory chunk in k_xdft_post
   bool profiling = false;
   std::vector<StageRecord> prof_pending;
@@ -2176,6 +2406,26 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
                            static_cast<size_t>(CAP) * kTcAtomBytes;
     }
   }
+  {
+    // tensor-core y-DFT: N' = 2*nky padded to 16 (<= 256), two to four K-chunk
+    // stages.  PYCUSAXS_YDFT=simt keeps the FP32 SIMT kernel.
+    const char *mode = std::getenv("PYCUSAXS_YDFT");
+    const bool simt_only = mode && std::strcmp(mode, "simt") == 0;
+    const int N = round_up(2 * a.nky, 16);
+    const size_t stage_bytes = (2 * 128 + 2 * static_cast<size_t>(N)) * 2 * kYtcChunk * sizeof(float);
+    const size_t avail = optin - static_smem(k_ydft_tc);
+    const int S = static_cast<int>(std::min<size_t>(kYtcMaxStages, avail / stage_bytes));
+    if (!simt_only && N <= 256 && S >= 2) {
+      pl->use_ytc = true;
+      a.ytcN = N;
+      a.ytcChunks = (a.ext[1] + kYtcChunk - 1) / kYtcChunk;
+      a.ytcS = S;
+      int cols = 32;
+      while (cols < 2 * N) cols *= 2;
+      a.ytcCols = cols;
+      pl->smem_ydft_tc = S * stage_bytes;
+    }
+  }
   pl->smem_hist = a.num_bins <= kHistSmemBins ? 2 * sizeof(double) * a.num_bins : 0;
   pl->smem_bin = static_cast<size_t>(kThreads / 32) * a.T * sizeof(double);
   if (pl->smem_spread + static_smem(k_spread_zdft) > optin ||
@@ -2217,9 +2467,10 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
   ALLOC(d_modz, nn[2]);
   ALLOC(d_ff, 9 * a.T);
   int4 *d_hx = nullptr, *d_hy = nullptr;
-  float *d_twzs = nullptr, *d_twztc = nullptr;
+  float *d_twzs = nullptr, *d_twztc = nullptr, *d_twytc = nullptr;
   ALLOC(d_twzs, 2 * a.nkzp);
   if (pl->use_tc) ALLOC(d_twztc, 2 * static_cast<size_t>(a.tcK) * a.tcN);
+  if (pl->use_ytc) ALLOC(d_twytc, static_cast<size_t>(a.ytcChunks) * 2 * a.ytcN * 2 * kYtcChunk);
   ALLOC(d_hx, a.stiles[0]);
   ALLOC(d_hy, a.stiles[1]);
   ALLOC(d_geom, static_cast<size_t>(B) * kGeom);
@@ -2249,6 +2500,7 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
   a.ff = d_ff;
   a.twz_sum = d_twzs;
   a.twz_tc = d_twztc;
+  a.twy_tc = d_twytc;
   a.home_x = d_hx;
   a.home_y = d_hy;
   a.geom = d_geom;
@@ -2297,6 +2549,38 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
   for (int x = 0; x < ex; ++x)
     for (int k = 0; k < a.nkx; ++k)
       saxs::twiddle(a.kx_lo + k, x, nn[0], &twx[x * a.nkxp + k].x, &twx[x * a.nkxp + k].y);
+  // the y twiddles as the y-DFT's B' operand: per K chunk, head block then
+  // remainder block, each N' x 2*kYtcChunk K-major
+  std::vector<float> twytc(pl->use_ytc ? static_cast<size_t>(a.ytcChunks) * 2 * a.ytcN * 2 * kYtcChunk : 0,
+                           0.0f);
+  if (pl->use_ytc) {
+    const int KP = 2 * kYtcChunk, Np = a.ytcN;
+    const size_t blk = static_cast<size_t>(Np) * KP;
+    for (int c = 0; c < a.ytcChunks; ++c)
+      for (int yy = 0; yy < kYtcChunk; ++yy) {
+        const int y = c * kYtcChunk + yy;
+        if (y >= ey) continue;
+        for (int ky = 0; ky < a.nky; ++ky) {
+          const float2 w = twy[static_cast<size_t>(y) * a.nkyp + ky];
+          // B'[2y + cz][2ky + d]: {Wr, Wi ; -Wi, Wr}[cz][d]
+          const float vals[2][2] = {{w.x, w.y}, {-w.y, w.x}};
+          for (int cz = 0; cz < 2; ++cz)
+            for (int d = 0; d < 2; ++d) {
+              const int kp = 2 * yy + cz, np = 2 * ky + d;
+              const float v = vals[cz][d];
+              uint32_t bits;
+              std::memcpy(&bits, &v, sizeof(bits));
+              bits &= 0xFFFFE000u;
+              float head;
+              std::memcpy(&head, &bits, sizeof(head));
+              const size_t o = static_cast<size_t>(c) * 2 * blk + static_cast<size_t>(kp / 4) * (Np / 8) * 32 +
+                               (np / 8) * 32 + (np % 8) * 4 + kp % 4;
+              twytc[o] = head;
+              twytc[o + blk] = v - head;
+            }
+        }
+      }
+  }
   const int ndim = std::max(nn[0], std::max(nn[1], nn[2]));
   std::vector<float> mx(nn[0]), my(nn[1]), mz(nn[2]);
   saxs::bspline_moduli(nn[0], ndim, mx.data());
@@ -2323,6 +2607,7 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
       (rc = up(d_hx, hxt.data(), sizeof(int4) * hxt.size())) ||
       (rc = up(d_twzs, twzs.data(), sizeof(float) * twzs.size())) ||
       (rc = up(d_twztc, twtc.data(), sizeof(float) * twtc.size())) ||
+      (rc = up(d_twytc, twytc.data(), sizeof(float) * twytc.size())) ||
       (rc = up(d_hy, hyt.data(), sizeof(int4) * hyt.size())) ||
       (rc = up(pl->d_geom0, g0, sizeof(g0)))) {
     destroy(pl);
@@ -2346,6 +2631,7 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
   if (e == cudaSuccess) e = raise_smem_limit(k_hist<float>);
   if (e == cudaSuccess) e = raise_smem_limit(k_hist<double>);
   if (e == cudaSuccess) e = raise_smem_limit(k_spread_zdft_tc);
+  if (e == cudaSuccess) e = raise_smem_limit(k_ydft_tc);
   if (e == cudaSuccess) {
     int per_sm = 0, sms = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_spread_zdft, kThreads,
@@ -2359,6 +2645,12 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
                                                         pl->smem_spread_tc);
       tc_per_sm = std::min(std::max(1, tc_per_sm), 512 / a.tcCols);
       pl->tc_ctas = tc_per_sm * std::max(1, sms);
+    }
+    if (e == cudaSuccess && pl->use_ytc) {
+      int per = 0;
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_ydft_tc, kYtcThreads, pl->smem_ydft_tc);
+      per = std::min(std::max(1, per), 512 / a.ytcCols);
+      pl->ytc_ctas = per * std::max(1, sms);
     }
   }
   if (e != cudaSuccess) {
@@ -2416,6 +2708,19 @@ int launch_spread(const SaxsPlan *pl, const DevArgs &a, int items, cudaStream_t 
   return launch_check("k_spread_zdft");
 }
 
+// y-axis DFT of `planes` z-transformed planes: the tensor-core kernel when the
+// plan has it, else the FP32 SIMT kernel.
+int launch_ydft(const SaxsPlan *pl, const DevArgs &a, int planes, cudaStream_t st) {
+  if (pl->use_ytc) {
+    const int items = planes * ((a.ext[0] + 127) / 128);
+    k_ydft_tc<<<std::max(1, std::min(items, pl->ytc_ctas)), kYtcThreads, pl->smem_ydft_tc, st>>>(a, items);
+    return launch_check("k_ydft_tc");
+  }
+  dim3 gy((a.ext[0] + kYRows - 1) / kYRows, a.nkz, planes / a.nkz);
+  k_ydft<<<gy, kThreads, pl->smem_ydft, st>>>(a);
+  return launch_check("k_ydft");
+}
+
 // Enqueue the memsets and kernels of one batch of `nframes` frames whose
 // geometry is already in (or queued for) a.geom.  Host work free, so that it can
 // be captured in a CUDA graph.
@@ -2453,11 +2758,10 @@ int enqueue_batch(SaxsPlan *pl, const DevArgs &a, int nframes, cudaStream_t st, 
     if (rc) return rc;
   }
   {
-    dim3 gy((a.ext[0] + kYRows - 1) / kYRows, a.nkz, nframes * a.T);
     tm.begin(kStYdft);
-    k_ydft<<<gy, kThreads, pl->smem_ydft, st>>>(a);
+    const int rc = launch_ydft(pl, a, nframes * a.T * a.nkz, st);
     tm.end(kStYdft);
-    if (int rc = launch_check("k_ydft")) return rc;
+    if (rc) return rc;
   }
   {
     dim3 gx((a.nky + kXRows - 1) / kXRows, a.nkz, nframes);
@@ -2790,9 +3094,7 @@ int backward(SaxsPlan *pl, const float *xyz, const float *box, const double *dl,
   }
   const int items = a.stiles[0] * a.stiles[1] * a.T;
   if (int rc = launch_spread(pl, a, items, st)) return rc;
-  dim3 gy((a.ext[0] + kYRows - 1) / kYRows, a.nkz, a.T);
-  k_ydft<<<gy, kThreads, pl->smem_ydft, st>>>(a);
-  if (int rc = launch_check("backward recompute")) return rc;
+  if (int rc = launch_ydft(pl, a, a.T * a.nkz, st)) return rc;
   // adjoint passes
   dim3 gx((a.nky + kXRows - 1) / kXRows, a.nkz, 1);
   k_xdft_grad<<<gx, kThreads, pl->smem_xdft, st>>>(a, j, pl->xc);
@@ -2921,9 +3223,7 @@ int forward_into_scratch(SaxsPlan *pl, const float *xyz, const float *box, unsig
   }
   const int items = a.stiles[0] * a.stiles[1] * a.T;
   if (int rc = launch_spread(pl, a, items, st)) return rc;
-  dim3 gy((a.ext[0] + kYRows - 1) / kYRows, a.nkz, a.T);
-  k_ydft<<<gy, kThreads, pl->smem_ydft, st>>>(a);
-  if (int rc = launch_check("k_ydft")) return rc;
+  if (int rc = launch_ydft(pl, a, a.T * a.nkz, st)) return rc;
   dim3 gx((a.nky + kXRows - 1) / kXRows, a.nkz, 1);
   k_xdft_post<<<gx, kThreads, pl->smem_xdft, st>>>(a, pl->xc);
   if (int rc = launch_check("k_xdft_post")) return rc;
@@ -2960,7 +3260,7 @@ int saxs_plan_info(const SaxsPlan *pl, SaxsPlanInfo *info) {
   info->kbox[1] = a.nky;
   info->kbox[2] = a.nkz;
   info->kz_count = a.nkz;
-  info->path = pl->use_tc ? 1 : 0;
+  info->path = (pl->use_tc ? 1 : 0) | (pl->use_ytc ? 2 : 0);
   info->device_bytes = pl->bytes;
   info->frames_accumulated = pl->frames;
   return SAXS_OK;

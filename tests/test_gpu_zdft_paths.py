@@ -1,9 +1,10 @@
-"""Tensor-core (tcgen05, 3xTF32) z-axis DFT vs the FP32 SIMT kernel and the FP64 oracle (GPU).
+"""Tensor-core (tcgen05, 3xTF32) z- and y-axis DFTs vs the FP32 SIMT kernels and the FP64 oracle (GPU).
 
-Plans take the tensor-core kernel whenever its operands fit shared memory
-(``info.path == 1``); ``PYCUSAXS_ZDFT=simt`` at plan creation keeps the SIMT
-kernel.  Both must give identical bin counts and profiles within the 1e-4 tolerance of
-the FP64 oracle; the 3xTF32 products are accurate to ~2^-19, and
+Plans take a tensor-core kernel whenever its operands fit shared memory
+(``info.path`` bit 0 for the z-axis DFT, bit 1 for the y-axis DFT);
+``PYCUSAXS_ZDFT=simt`` / ``PYCUSAXS_YDFT=simt`` at plan creation keep the SIMT
+kernel.  Both must give identical bin counts and profiles within the 1e-4
+tolerance of the FP64 oracle; the 3xTF32 products are accurate to ~2^-19, and
 TC_VS_SIMT_RTOL (2e-5 per bin) bounds the difference between the two kernels.
 """
 import contextlib
@@ -21,32 +22,33 @@ TC_VS_SIMT_RTOL = 2e-5
 
 
 @contextlib.contextmanager
-def zdft_mode(mode):
-    old = os.environ.get("PYCUSAXS_ZDFT")
+def dft_mode(var, mode):
+    old = os.environ.get(var)
     if mode is None:
-        os.environ.pop("PYCUSAXS_ZDFT", None)
+        os.environ.pop(var, None)
     else:
-        os.environ["PYCUSAXS_ZDFT"] = mode
+        os.environ[var] = mode
     try:
         yield
     finally:
         if old is None:
-            os.environ.pop("PYCUSAXS_ZDFT", None)
+            os.environ.pop(var, None)
         else:
-            os.environ["PYCUSAXS_ZDFT"] = old
+            os.environ[var] = old
 
 
-def _both(system, grid, frames, expect_tc=True, **kw):
-    with zdft_mode(None):
+def _both(system, grid, frames, expect_tc=True, axis="z", **kw):
+    var, bit = ("PYCUSAXS_ZDFT", 1) if axis == "z" else ("PYCUSAXS_YDFT", 2)
+    with dft_mode(var, None):
         h_tc, n_tc, e_tc = engine_hist(system, grid, frames, **kw)
         path_tc = e_tc.info.path
         e_tc.close()
-    with zdft_mode("simt"):
+    with dft_mode(var, "simt"):
         h_s, n_s, e_s = engine_hist(system, grid, frames, **kw)
         path_s = e_s.info.path
         e_s.close()
-    assert path_s == 0
-    assert path_tc == (1 if expect_tc else 0)
+    assert path_s & bit == 0
+    assert (path_tc & bit) == (bit if expect_tc else 0)
     np.testing.assert_array_equal(n_tc, n_s)
     sel = n_s > 0
     sel[0] = False
@@ -120,3 +122,41 @@ def test_tc_batched_frames(cuda):
     s = cubic_system(5000, 40.0, seed=19, jitter=0.5, nframes=3)
     frames = [s.frame(k) for k in range(3)]
     _both(s, (32, 32, 32), frames, sigma=2.0, qcut=0.6, max_frames=3)
+
+
+# -- y-axis DFT -------------------------------------------------------------
+
+
+def test_ytc_small_cubic_fewer_rows_than_block(cuda):
+    # x extent 32 of a 128-row block: the rows beyond it are zero
+    s = cubic_system(4000, 40.0, seed=21)
+    _both(s, (32, 32, 32), [s.positions], axis="y", sigma=2.0, qcut=0.6)
+
+
+def test_ytc_bench_sized_grid128(cuda):
+    s = cubic_system(30_000, 120.0, seed=22)
+    _both(s, (128, 128, 128), [s.positions], axis="y", sigma=2.0, qcut=0.5, bin_size=0.002)
+
+
+def test_ytc_y_extent_not_multiple_of_chunk(cuda):
+    # y extent 40: the last K chunk holds 8 y values and 8 zero rows
+    s = _line_system(3000, (30.0, 40.0, 44.0), 23, ("H", "C", "O", "N"))
+    _both(s, (24, 40, 44), [s.positions], axis="y", sigma=2.5, qcut=0.9)
+
+
+def test_ytc_two_x_blocks(cuda):
+    # x extent 160: two blocks of 128 rows, the second one partly empty
+    s = _line_system(3000, (160.0, 40.0, 40.0), 24, ("C", "N", "O"))
+    _both(s, (160, 32, 32), [s.positions], axis="y", sigma=2.0, qcut=0.4)
+
+
+def test_ytc_full_ky_axis_keeps_simt(cuda):
+    # q-cut at the grid's limit on a long y axis: 2*nky > 256 columns, SIMT kernel
+    s = _line_system(1500, (16.0, 192.0, 16.0), 25)
+    _both(s, (16, 96, 16), [s.positions], axis="y", expect_tc=False, sigma=2.0, qcut=3.5)
+
+
+def test_ytc_batched_frames(cuda):
+    s = cubic_system(5000, 40.0, seed=26, jitter=0.5, nframes=3)
+    frames = [s.frame(k) for k in range(3)]
+    _both(s, (32, 32, 32), frames, axis="y", sigma=2.0, qcut=0.6, max_frames=3)
