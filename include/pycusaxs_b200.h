@@ -70,8 +70,8 @@ typedef struct SaxsPlanInfo {
   int num_bins;         /* int(qcut/bin_size)+1 (saxsKernel.cu:247)                */
   int kbox[3];          /* k-points evaluated per axis (x, y: signed range; z: 0..)*/
   int kz_count;
-  int path;             /* pruned separable DFT; bit 0: z-axis DFT on tcgen05       */
-                        /* (3xTF32), bit 1: y-axis DFT on tcgen05; else FP32 SIMT   */
+  int path;             /* pruned separable DFT; bits 0, 1, 2: z-, y-, x-axis DFT   */
+                        /* on tcgen05 (3xTF32); a clear bit: that pass in FP32 SIMT */
   size_t device_bytes;  /* device memory held by the plan                          */
   int frames_accumulated;
 } SaxsPlanInfo;

@@ -30,6 +30,7 @@
 // padded transform is F = DFT(g - mean over the corner block) + mean*nn^3 at
 // k = 0, evaluated exactly by three pruned DFT passes that never touch the
 // zero region.
+#include <cuda.h>  // CUtensorMap and its enums (the encoder is fetched at run time)
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -88,8 +89,7 @@ struct DevArgs {
   int zc;  // z rows of twiddles k_spread_zdft holds in shared memory at once
   // tensor-core z-DFT (k_spread_zdft_tc): GEMM N, K, spread rows, stages, TMEM columns
   int tcN, tcK, tcR, tcS, tcCols, tcRB, tcCap;
-  // tensor-core y-axis DFT (k_ydft_tc): GEMM N', K chunks, stages, TMEM columns
-  int ytcN, ytcChunks, ytcS, ytcCols;
+  int xtcTP;  // tensor-core x-axis DFT: rows per ky (types padded to 8 or 16)
   int nf[3];
   int dz;
   float dq, qcut;
@@ -108,7 +108,6 @@ struct DevArgs {
   const float *ff;    // [T][9]
   const float *twz_sum; // [2*nkzp]: sum over z < ez of the z twiddles (re, im)
   const float *twz_tc;  // [2][tcK x tcN]: z twiddles as TF32 head / remainder, K-major
-  const float *twy_tc;  // [chunk][2][ytcN x 2*kYtcChunk]: y-DFT B' operand, head / remainder
   const int4 *home_x; // per spread tile along x: home tiles whose atoms reach it (-1 padded)
   const int4 *home_y;
   int2 *key;
@@ -1132,63 +1131,111 @@ __global__ void __launch_bounds__(kThreads) k_ydft(DevArgs a) {
 }
 
 // ---------------------------------------------------------------------------
-// Tensor-core y-axis DFT (tcgen05, 3xTF32)
+// Tensor-core y- and x-axis DFTs (tcgen05, 3xTF32)
 // ---------------------------------------------------------------------------
 //
-// Per z-transformed plane (frame, type, kz) and block of 128 x rows, the y-axis
-// DFT is the real GEMM  D[x][n'] = sum_k' A[x][k'] B'[k'][n']  with
-//   A[x][2y + c] = component c (0 re, 1 im) of Z[x][y]  (the plane's own memory
-//                  layout read as floats), K' = 2*ey,
-//   B'[2y + c][2ky + d] = { Wr, Wi ; -Wi, Wr }[c][d] of W[y][ky], the y twiddles,
-//   D[x][2ky + d] = component d of Y[ky][x],  N' = 2*nky padded to 16.
-// K is streamed in chunks of kYtcChunk y values.  Operands are K-major,
-// no-swizzle (core matrices of 8 rows x 16 B): A element (x, k') at
-// (k'/4)*512 + (x/8)*32 + (x%8)*4 + k'%4 floats (LBO 2048 B, SBO 128 B); B'
+// Both passes are real GEMMs  D[r][n'] = sum_k' A[r][k'] B'[k'][n']  over blocks
+// of 128 rows, with complex data read as real:
+//   A[r][2u + c] = component c (0 re, 1 im) of the row's complex values at u
+//                  (each row is contiguous in memory, so A is that memory read
+//                  as floats), K' = 2 * (extent of u),
+//   B'[2u + c][2k + d] = { Wr, Wi ; -Wi, Wr }[c][d] of the twiddle W[u][k],
+//   D[r][2k + d] = component d of the transformed row at k,  N' = 2 * (number
+//                  of k) padded to 16.
+// y pass: rows are the x rows of one z-transformed plane Z[x][y] (u = y, k =
+//   ky), 128 per item; the epilogue writes Y[ky][x].
+// x pass: rows are (ky, type) pairs of one (frame, kz), row = (ky - ky0) * TP +
+//   type with the types padded to TP (8 or 16), u = x, k = kx; the epilogue
+//   applies the form factors, sums the types with shuffles across the TP lanes
+//   of a ky, squares and multiplies by the B-spline moduli (the SIMT kernel's
+//   k_xdft_post), writing ibox[kz][ky][kx].
+// K is streamed in chunks of kDtcChunk values of u: per chunk the loader warp
+// issues one tensor copy (cp.async.bulk.tensor, no multicast) of the 128 rows
+// x 32 floats into a raw staging tile (rows outside the data zero-filled by the
+// tensor map) and one bulk copy of the B' chunk.  Operands are K-major,
+// no-swizzle (core matrices of 8 rows x 16 B): A element (r, k') at
+// (k'/4)*512 + (r/8)*32 + (r%8)*4 + k'%4 floats (LBO 2048 B, SBO 128 B); B'
 // element (n', k') at (k'/4)*(N'/8)*32 + (n'/8)*32 + (n'%8)*4 + k'%4 (LBO N'*16
 // B, SBO 128 B).  Both are split into a TF32 head and remainder like the z-axis
 // DFT's operands.
-constexpr int kYtcChunk = 16;                  // y values per K chunk (K' = 32)
-constexpr int kYtcProducerWarps = 8;
-constexpr int kYtcProducers = 32 * kYtcProducerWarps;
-constexpr int kYtcMmaWarp = kYtcProducerWarps;
-constexpr int kYtcLoaderWarp = kYtcProducerWarps + 1;
-constexpr int kYtcThreads = 32 * (kYtcProducerWarps + 6);  // producers, MMA, loader, 4 epilogue
-constexpr int kYtcMaxStages = 4;
+constexpr int kDtcChunk = 16;                  // u values per K chunk (K' = 32)
+constexpr int kDtcProducerWarps = 8;
+constexpr int kDtcProducers = 32 * kDtcProducerWarps;
+constexpr int kDtcMmaWarp = kDtcProducerWarps;
+constexpr int kDtcLoaderWarp = kDtcProducerWarps + 1;
+constexpr int kDtcThreads = 32 * (kDtcProducerWarps + 6);  // producers, MMA, loader, 4 epilogue
+constexpr int kDtcMaxStages = 4;
+
+// One pass's GEMM shape: N', K chunks, stages, TMEM columns, B' table.
+struct DtcShape {
+  int N, chunks, S, cols;
+  const float *B;  // [chunk][2][N' x 2*kDtcChunk]: head block then remainder block
+};
+
+// Tensor copy of chunk c of item w's 128 rows into `dst` (y pass: 3-D map
+// {2*ey floats, ex rows, planes}; x pass: 5-D map {2*ex floats, type, ky, kz,
+// frame} whose box {32, TP, 128/TP, 1, 1} lands rows in (ky, type) order).
+template <bool kX>
+__device__ __forceinline__ void dtc_tensor_copy(const DevArgs &a, const CUtensorMap *map, int w, int c,
+                                                uint32_t dst, uint32_t bar) {
+  const uint64_t m = reinterpret_cast<uint64_t>(map);
+  const int u0 = c * 2 * kDtcChunk;
+  if (!kX) {
+    const int xblocks = (a.ext[0] + 127) / 128;
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, "
+        "%4}], [%5];" ::"r"(dst),
+        "l"(m), "r"(u0), "r"((w % xblocks) * 128), "r"(w / xblocks), "r"(bar)
+        : "memory");
+  } else {
+    const int kyb = 128 / a.xtcTP;
+    const int nblk = (a.nky + kyb - 1) / kyb;
+    const int f = w / (a.nkz * nblk), kz = (w / nblk) % a.nkz;
+    asm volatile(
+        "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, "
+        "%4, %5, %6}], [%7];" ::"r"(dst),
+        "l"(m), "r"(u0), "r"(0), "r"((w % nblk) * kyb), "r"(kz), "r"(f), "r"(bar)
+        : "memory");
+  }
+}
 
 // Persistent, warp-specialized: grid = min(items, resident CTAs), block
-// kYtcThreads; an item is (plane, block of 128 x rows), planes ordered
-// (frame, type, kz) like Z and Y.  Barriers (all waits bounded):
+// kDtcThreads.  Items: y pass (plane, block of 128 x rows), planes ordered
+// (frame, type, kz) like Z and Y; x pass (frame, kz, block of 128/TP ky).
+// Barriers (all waits bounded):
+//   bfull[st] loader copies -> producers and MMA (raw A rows and B' landed)
 //   afull[st] producers -> MMA (A chunk of stage st split and written)
-//   bfull[st] loader bulk copy -> MMA (B' chunk landed)
-//   empty[st] MMA commit -> producers and loader (stage st read)
+//   empty[st] MMA commit -> loader (stage st read)
 //   dfull[d]  MMA commit -> epilogue (accumulator d complete)
 //   dempty[d] epilogue -> MMA (accumulator d read out)
-// Dynamic shared memory: ytcS stages of { A head, A remainder (128 x K'),
-// B' head, B' remainder (N' x K') } floats.
-__global__ void __launch_bounds__(kYtcThreads, 1) k_ydft_tc(DevArgs a, int items) {
+// Dynamic shared memory: S stages of { A head, A remainder (128 x K'), B' head,
+// B' remainder (N' x K'), raw A rows (128 x K') } floats.
+template <bool kX>
+__global__ void __launch_bounds__(kDtcThreads, 1)
+    k_dft_tc(DevArgs a, DtcShape sh, const __grid_constant__ CUtensorMap amap, int items) {
   extern __shared__ __align__(16) unsigned char smem[];
-  __shared__ __align__(8) uint64_t bars[3 * kYtcMaxStages + 4];
+  __shared__ __align__(8) uint64_t bars[3 * kDtcMaxStages + 4];
   __shared__ uint32_t tmem_slot;
   __shared__ volatile int abort_flag;
-  const int N = a.ytcN, NS = a.ytcS, NC = a.ytcChunks;
-  const int KP = 2 * kYtcChunk;                      // K' per chunk
+  const int N = sh.N, NS = sh.S, NC = sh.chunks;
+  const int KP = 2 * kDtcChunk;                      // K' per chunk
   const int a_floats = 128 * KP, b_floats = N * KP;  // per head or remainder
-  const int stage_floats = 2 * a_floats + 2 * b_floats;
-  const int ex = a.ext[0], ey = a.ext[1];
-  const int xblocks = (ex + 127) / 128;
+  const int stage_floats = 3 * a_floats + 2 * b_floats;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  float *stages = reinterpret_cast<float *>(smem);
-  uint64_t *afull = bars, *bfull = bars + kYtcMaxStages, *empty = bars + 2 * kYtcMaxStages,
-           *dfull = bars + 3 * kYtcMaxStages, *dempty = dfull + 2;
-  if (warp == kYtcMmaWarp) {
+  // tensor copies need a 128-byte aligned destination: the stages start at the
+  // first 128-byte boundary of the dynamic shared memory (128 bytes reserved)
+  float *stages = reinterpret_cast<float *>(smem + ((128u - (smem_addr(smem) & 127u)) & 127u));
+  uint64_t *afull = bars, *bfull = bars + kDtcMaxStages, *empty = bars + 2 * kDtcMaxStages,
+           *dfull = bars + 3 * kDtcMaxStages, *dempty = dfull + 2;
+  if (warp == kDtcMmaWarp) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      smem_addr(&tmem_slot)),
-                 "r"(a.ytcCols));
+                 "r"(sh.cols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
   }
   if (tid == 0) {
     for (int i = 0; i < NS; ++i) {
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&afull[i])), "r"(kYtcProducerWarps));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&afull[i])), "r"(kDtcProducerWarps));
       asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&bfull[i])), "r"(1));
       asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&empty[i])), "r"(1));
     }
@@ -1212,30 +1259,22 @@ __global__ void __launch_bounds__(kYtcThreads, 1) k_ydft_tc(DevArgs a, int items
     }
   };
 
-  if (warp < kYtcProducerWarps) {
+  if (warp < kDtcProducerWarps) {
+    // split the raw 128 x K' rows into head and remainder, K-major: 8 lanes per
+    // row read 128 contiguous bytes
     int g = 0;
     for (int w = blockIdx.x; w < items; w += gridDim.x) {
-      const int64_t plane = w / xblocks;
-      const int xb = (w % xblocks) * 128;
-      const float2 *Zp = a.Z + plane * ex * ey;
       for (int c = 0; c < NC; ++c, ++g) {
         const int st = g % NS;
-        if (g >= NS) wait(&empty[st], g / NS - 1);
+        wait(&bfull[st], g / NS);
         float *ah = stages + static_cast<size_t>(st) * stage_floats;
         float *al = ah + a_floats;
-        // 128 rows x 8 float4 (two complex values each); 8 lanes per row
-        for (int i = tid; i < 128 * (kYtcChunk / 2); i += kYtcProducers) {
-          const int x = i >> 3, q = i & 7;
-          const int gx = xb + x, y = c * kYtcChunk + 2 * q;
-          float2 u0 = make_float2(0.f, 0.f), u1 = make_float2(0.f, 0.f);
-          if (gx < ex) {
-            const float2 *row = Zp + static_cast<int64_t>(gx) * ey;
-            if (y < ey) u0 = row[y];
-            if (y + 1 < ey) u1 = row[y + 1];
-          }
-          const float4 v = make_float4(u0.x, u0.y, u1.x, u1.y);
+        const float *raw = ah + 2 * a_floats + 2 * b_floats;
+        for (int i = tid; i < 128 * (KP / 4); i += kDtcProducers) {
+          const int r = i >> 3, q = i & 7;
+          const float4 v = *reinterpret_cast<const float4 *>(raw + r * KP + 4 * q);
           const float4 h = make_float4(tf32_head(v.x), tf32_head(v.y), tf32_head(v.z), tf32_head(v.w));
-          const int o = q * 512 + (x >> 3) * 32 + (x & 7) * 4;
+          const int o = q * 512 + (r >> 3) * 32 + (r & 7) * 4;
           *reinterpret_cast<float4 *>(ah + o) = h;
           *reinterpret_cast<float4 *>(al + o) = make_float4(v.x - h.x, v.y - h.y, v.z - h.z, v.w - h.w);
         }
@@ -1244,9 +1283,10 @@ __global__ void __launch_bounds__(kYtcThreads, 1) k_ydft_tc(DevArgs a, int items
         if (lane == 0) mbar_arrive(smem_addr(&afull[st]));
       }
     }
-  } else if (warp == kYtcLoaderWarp) {
+  } else if (warp == kDtcLoaderWarp) {
     if (lane == 0) {
-      const uint32_t bytes = static_cast<uint32_t>(2 * b_floats * sizeof(float));
+      const uint32_t bbytes = static_cast<uint32_t>(2 * b_floats * sizeof(float));
+      const uint32_t abytes = static_cast<uint32_t>(a_floats * sizeof(float));
       int g = 0;
       for (int w = blockIdx.x; w < items && !abort_flag; w += gridDim.x) {
         for (int c = 0; c < NC; ++c, ++g) {
@@ -1254,17 +1294,19 @@ __global__ void __launch_bounds__(kYtcThreads, 1) k_ydft_tc(DevArgs a, int items
           if (g >= NS) wait(&empty[st], g / NS - 1);
           if (abort_flag) break;
           const uint32_t bar = smem_addr(&bfull[st]);
-          const uint32_t dst = smem_addr(stages + static_cast<size_t>(st) * stage_floats + 2 * a_floats);
-          asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+          float *sb = stages + static_cast<size_t>(st) * stage_floats;
+          asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bbytes + abytes)
                        : "memory");
           asm volatile(
-              "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
-              "l"(a.twy_tc + static_cast<size_t>(c) * 2 * b_floats), "r"(bytes), "r"(bar)
+              "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                  smem_addr(sb + 2 * a_floats)),
+              "l"(sh.B + static_cast<size_t>(c) * 2 * b_floats), "r"(bbytes), "r"(bar)
               : "memory");
+          dtc_tensor_copy<kX>(a, &amap, w, c, smem_addr(sb + 2 * a_floats + 2 * b_floats), bar);
         }
       }
     }
-  } else if (warp == kYtcMmaWarp) {
+  } else if (warp == kDtcMmaWarp) {
     if (lane == 0) {
       // kind::tf32: D f32, A and B tf32, both K-major, N >> 3 at bit 17, M = 128
       const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) |
@@ -1278,8 +1320,8 @@ __global__ void __launch_bounds__(kYtcThreads, 1) k_ydft_tc(DevArgs a, int items
         const uint32_t dcol = tmem + static_cast<uint32_t>(d * N);
         for (int c = 0; c < NC; ++c, ++g) {
           const int st = g % NS;
-          wait(&afull[st], g / NS);
           wait(&bfull[st], g / NS);
+          wait(&afull[st], g / NS);
           if (abort_flag) break;
           asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
           const float *ah = stages + static_cast<size_t>(st) * stage_floats;
@@ -1311,35 +1353,94 @@ __global__ void __launch_bounds__(kYtcThreads, 1) k_ydft_tc(DevArgs a, int items
       if (abort_flag && last_bar) mbar_wait(last_bar, static_cast<uint32_t>(last_parity & 1));
     }
   } else {
-    // epilogue: warp w reads TMEM lanes 32*(w%4).. = x rows of the block
+    // epilogue: warp w reads TMEM lanes 32*(w%4).. = rows of the block
     const int quarter = warp & 3;
+    const int r = 32 * quarter + lane;
     int i = 0;
     for (int w = blockIdx.x; w < items; w += gridDim.x, ++i) {
       const int d = i & 1;
       wait(&dfull[d], i >> 1);
       if (__any_sync(0xffffffffu, abort_flag != 0)) break;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const int64_t plane = w / xblocks;
-      const int x = (w % xblocks) * 128 + 32 * quarter + lane;
-      float2 *Yp = a.Y + plane * a.nky * ex;
       const uint32_t lane_base = tmem + (static_cast<uint32_t>(32 * quarter) << 16) + static_cast<uint32_t>(d * N);
-      for (int c0 = 0; c0 < N; c0 += 16) {
-        uint32_t r[16];
-        asm volatile(
-            "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-            "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-              "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-              "=r"(r[14]), "=r"(r[15])
-            : "r"(lane_base + c0));
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        if (x < ex) {
+      if (!kX) {
+        const int ex = a.ext[0];
+        const int xblocks = (ex + 127) / 128;
+        const int64_t plane = w / xblocks;
+        const int x = (w % xblocks) * 128 + r;
+        float2 *Yp = a.Y + plane * a.nky * ex;
+        for (int c0 = 0; c0 < N; c0 += 16) {
+          uint32_t v[16];
+          asm volatile(
+              "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+              "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+              : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+                "=r"(v[14]), "=r"(v[15])
+              : "r"(lane_base + c0));
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+          if (x < ex) {
+#pragma unroll
+            for (int jj = 0; jj < 8; ++jj) {
+              const int ky = c0 / 2 + jj;
+              if (ky < a.nky)
+                Yp[static_cast<int64_t>(ky) * ex + x] =
+                    make_float2(__uint_as_float(v[2 * jj]), __uint_as_float(v[2 * jj + 1]));
+            }
+          }
+        }
+      } else {
+        const int tp = a.xtcTP, kyb = 128 / tp;
+        const int nblk = (a.nky + kyb - 1) / kyb;
+        const int f = w / (a.nkz * nblk), kz = (w / nblk) % a.nkz;
+        const int ky = (w % nblk) * kyb + r / tp, t = r % tp;
+        const bool row_ok = t < a.T && ky < a.nky;
+        const float *ocs = a.geom + f * kGeom + 9;
+        const int ka = signed_k(kz, a.nn[2], a.nf[2]);
+        const int ja = a.ky_lo + min(ky, a.nky - 1);
+        const float mean = row_ok ? static_cast<float>(a.border[static_cast<int64_t>(f) * a.T + t] /
+                                                       a.border_count)
+                                  : 0.0f;
+        const float *ff = a.ff + 9 * (t < a.T ? t : 0);
+        const int jw = ja < 0 ? ja + a.nn[1] : ja;
+        const float mzy = a.mody[jw] * a.modz[kz];
+        float *ib = a.ibox + ((static_cast<int64_t>(f) * a.nkz + kz) * a.nky + ky) * a.nkx;
+        for (int c0 = 0; c0 < N; c0 += 16) {
+          uint32_t v[16];
+          asm volatile(
+              "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+              "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+              : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+                "=r"(v[14]), "=r"(v[15])
+              : "r"(lane_base + c0));
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
           for (int jj = 0; jj < 8; ++jj) {
-            const int ky = c0 / 2 + jj;
-            if (ky < a.nky)
-              Yp[static_cast<int64_t>(ky) * ex + x] =
-                  make_float2(__uint_as_float(r[2 * jj]), __uint_as_float(r[2 * jj + 1]));
+            const int kx = c0 / 2 + jj;
+            const int ia = a.kx_lo + min(kx, a.nkx - 1);
+            const float mw = kpoint_q(ocs, ia, ja, ka);
+            const bool inside = row_ok && kx < a.nkx && !(mw > a.qcut);
+            float2 F = make_float2(__uint_as_float(v[2 * jj]), __uint_as_float(v[2 * jj + 1]));
+            // the padding mean's constant over the whole supercell lands at k = 0
+            if (ka == 0 && ja == 0 && ia == 0)
+              F.x += static_cast<float>(static_cast<double>(mean) * a.nn3);
+            float2 A = make_float2(0.f, 0.f);
+            if (inside) {
+              const float q = mw / (4.0 * M_PI);
+              const float ft = form_factor(ff, q * q);
+              A.x = ft * F.x;
+              A.y = ft * F.y;
+            }
+            // type sum across the tp lanes of this ky
+            for (int o = 1; o < tp; o <<= 1) {
+              A.x += __shfl_xor_sync(0xffffffffu, A.x, o);
+              A.y += __shfl_xor_sync(0xffffffffu, A.y, o);
+            }
+            if (t == 0 && ky < a.nky && kx < a.nkx) {
+              const int iw = ia < 0 ? ia + a.nn[0] : ia;
+              ib[kx] = !(mw > a.qcut) ? (A.x * A.x + A.y * A.y) * (a.modx[iw] * mzy) : 0.0f;
+            }
           }
         }
       }
@@ -1351,8 +1452,8 @@ __global__ void __launch_bounds__(kYtcThreads, 1) k_ydft_tc(DevArgs a, int items
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  if (warp == kYtcMmaWarp)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(a.ytcCols));
+  if (warp == kDtcMmaWarp)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(sh.cols));
 }
 
 // grid (ceil(nky/4), nkz, frames), block 256: x-axis DFT, form factors, type
@@ -2106,9 +2207,11 @@ struct SaxsPlan {
   bool use_tc = false;  // z-axis DFT on the tensor cores (k_spread_zdft_tc)
   size_t smem_spread_tc = 0;
   int tc_ctas = 1;
-  bool use_ytc = false;  // y-axis DFT on the tensor cores (k_ydft_tc)
-  size_t smem_ydft_tc = 0;
-  int ytc_ctas = 1;
+  bool use_ytc = false;  // y-axis DFT on the tensor cores (k_dft_tc<false>)
+  bool use_xtc = false;  // x-axis DFT + post on the tensor cores (k_dft_tc<true>)
+  DtcShape yshape{}, xshape{};
+  size_t smem_ydft_tc = 0, smem_xdft_tc = 0;
+  int ytc_ctas = 1, xtc_ctas = 1;
   int xc = 1;           // x values per shared-memory chunk in k_xdft_post
   bool profiling = false;
   std::vector<StageRecord> prof_pending;
@@ -2220,6 +2323,58 @@ void destroy(SaxsPlan *pl) {
   if (pl->ring.host) cudaFreeHost(pl->ring.host);
   cudaSetDevice(prev);
   delete pl;
+}
+
+// GEMM shape of a tensor-core DFT pass over `extent` values of u to `nk` values
+// of k: N' = 2*nk padded to 16 (at most 256), two to four K-chunk stages in
+// `avail` bytes of shared memory.  Returns false when the pass does not fit.
+bool dtc_shape(int nk, int extent, size_t avail, DtcShape *sh, size_t *smem) {
+  const int N = round_up(2 * nk, 16);
+  const size_t stage_bytes = (3 * 128 + 2 * static_cast<size_t>(N)) * 2 * kDtcChunk * sizeof(float);
+  const int S = static_cast<int>(std::min<size_t>(kDtcMaxStages, (avail - 128) / stage_bytes));
+  if (N > 256 || S < 2) return false;
+  sh->N = N;
+  sh->chunks = (extent + kDtcChunk - 1) / kDtcChunk;
+  sh->S = S;
+  int cols = 32;
+  while (cols < 2 * N) cols *= 2;
+  sh->cols = cols;
+  *smem = S * stage_bytes + 128;  // + alignment slack of the stage base
+  return true;
+}
+
+// B' operand of a tensor-core DFT pass from twiddles tw[u * stride + k] (u <
+// extent, k < nk): per K chunk a head block then a remainder block, each N' x
+// 2*kDtcChunk K-major, B'[2u + c][2k + d] = {Wr, Wi ; -Wi, Wr}[c][d].
+std::vector<float> dtc_bprime(const std::vector<float2> &tw, int stride, int extent, int nk,
+                              const DtcShape &sh) {
+  const int KP = 2 * kDtcChunk, Np = sh.N;
+  const size_t blk = static_cast<size_t>(Np) * KP;
+  std::vector<float> out(static_cast<size_t>(sh.chunks) * 2 * blk, 0.0f);
+  for (int c = 0; c < sh.chunks; ++c)
+    for (int uu = 0; uu < kDtcChunk; ++uu) {
+      const int u = c * kDtcChunk + uu;
+      if (u >= extent) continue;
+      for (int k = 0; k < nk; ++k) {
+        const float2 w = tw[static_cast<size_t>(u) * stride + k];
+        const float vals[2][2] = {{w.x, w.y}, {-w.y, w.x}};
+        for (int cz = 0; cz < 2; ++cz)
+          for (int d = 0; d < 2; ++d) {
+            const int kp = 2 * uu + cz, np = 2 * k + d;
+            const float v = vals[cz][d];
+            uint32_t bits;
+            std::memcpy(&bits, &v, sizeof(bits));
+            bits &= 0xFFFFE000u;
+            float head;
+            std::memcpy(&head, &bits, sizeof(head));
+            const size_t o = static_cast<size_t>(c) * 2 * blk + static_cast<size_t>(kp / 4) * (Np / 8) * 32 +
+                             (np / 8) * 32 + (np % 8) * 4 + kp % 4;
+            out[o] = head;
+            out[o + blk] = v - head;
+          }
+      }
+    }
+  return out;
 }
 
 int create(const SaxsParams *prm, SaxsPlan **out) {
@@ -2407,24 +2562,19 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
     }
   }
   {
-    // tensor-core y-DFT: N' = 2*nky padded to 16 (<= 256), two to four K-chunk
-    // stages.  PYCUSAXS_YDFT=simt keeps the FP32 SIMT kernel.
-    const char *mode = std::getenv("PYCUSAXS_YDFT");
-    const bool simt_only = mode && std::strcmp(mode, "simt") == 0;
-    const int N = round_up(2 * a.nky, 16);
-    const size_t stage_bytes = (2 * 128 + 2 * static_cast<size_t>(N)) * 2 * kYtcChunk * sizeof(float);
-    const size_t avail = optin - static_smem(k_ydft_tc);
-    const int S = static_cast<int>(std::min<size_t>(kYtcMaxStages, avail / stage_bytes));
-    if (!simt_only && N <= 256 && S >= 2) {
-      pl->use_ytc = true;
-      a.ytcN = N;
-      a.ytcChunks = (a.ext[1] + kYtcChunk - 1) / kYtcChunk;
-      a.ytcS = S;
-      int cols = 32;
-      while (cols < 2 * N) cols *= 2;
-      a.ytcCols = cols;
-      pl->smem_ydft_tc = S * stage_bytes;
-    }
+    // tensor-core y- and x-axis DFTs when their shapes fit; the x pass needs at
+    // most 16 types.  PYCUSAXS_YDFT=simt / PYCUSAXS_XDFT=simt keep the FP32
+    // SIMT kernels.
+    const char *ym = std::getenv("PYCUSAXS_YDFT");
+    const char *xm = std::getenv("PYCUSAXS_XDFT");
+    // the tensor maps need row strides that are multiples of 16 bytes: even extents
+    if (!(ym && std::strcmp(ym, "simt") == 0) && a.ext[1] % 2 == 0)
+      pl->use_ytc = dtc_shape(a.nky, a.ext[1], optin - static_smem(k_dft_tc<false>), &pl->yshape,
+                              &pl->smem_ydft_tc);
+    a.xtcTP = a.T <= 8 ? 8 : 16;
+    if (!(xm && std::strcmp(xm, "simt") == 0) && a.T <= 16 && a.ext[0] % 2 == 0)
+      pl->use_xtc = dtc_shape(a.nkx, a.ext[0], optin - static_smem(k_dft_tc<true>), &pl->xshape,
+                              &pl->smem_xdft_tc);
   }
   pl->smem_hist = a.num_bins <= kHistSmemBins ? 2 * sizeof(double) * a.num_bins : 0;
   pl->smem_bin = static_cast<size_t>(kThreads / 32) * a.T * sizeof(double);
@@ -2467,10 +2617,11 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
   ALLOC(d_modz, nn[2]);
   ALLOC(d_ff, 9 * a.T);
   int4 *d_hx = nullptr, *d_hy = nullptr;
-  float *d_twzs = nullptr, *d_twztc = nullptr, *d_twytc = nullptr;
+  float *d_twzs = nullptr, *d_twztc = nullptr, *d_twytc = nullptr, *d_twxtc = nullptr;
   ALLOC(d_twzs, 2 * a.nkzp);
   if (pl->use_tc) ALLOC(d_twztc, 2 * static_cast<size_t>(a.tcK) * a.tcN);
-  if (pl->use_ytc) ALLOC(d_twytc, static_cast<size_t>(a.ytcChunks) * 2 * a.ytcN * 2 * kYtcChunk);
+  if (pl->use_ytc) ALLOC(d_twytc, static_cast<size_t>(pl->yshape.chunks) * 4 * pl->yshape.N * kDtcChunk);
+  if (pl->use_xtc) ALLOC(d_twxtc, static_cast<size_t>(pl->xshape.chunks) * 4 * pl->xshape.N * kDtcChunk);
   ALLOC(d_hx, a.stiles[0]);
   ALLOC(d_hy, a.stiles[1]);
   ALLOC(d_geom, static_cast<size_t>(B) * kGeom);
@@ -2500,7 +2651,8 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
   a.ff = d_ff;
   a.twz_sum = d_twzs;
   a.twz_tc = d_twztc;
-  a.twy_tc = d_twytc;
+  pl->yshape.B = d_twytc;
+  pl->xshape.B = d_twxtc;
   a.home_x = d_hx;
   a.home_y = d_hy;
   a.geom = d_geom;
@@ -2549,38 +2701,10 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
   for (int x = 0; x < ex; ++x)
     for (int k = 0; k < a.nkx; ++k)
       saxs::twiddle(a.kx_lo + k, x, nn[0], &twx[x * a.nkxp + k].x, &twx[x * a.nkxp + k].y);
-  // the y twiddles as the y-DFT's B' operand: per K chunk, head block then
-  // remainder block, each N' x 2*kYtcChunk K-major
-  std::vector<float> twytc(pl->use_ytc ? static_cast<size_t>(a.ytcChunks) * 2 * a.ytcN * 2 * kYtcChunk : 0,
-                           0.0f);
-  if (pl->use_ytc) {
-    const int KP = 2 * kYtcChunk, Np = a.ytcN;
-    const size_t blk = static_cast<size_t>(Np) * KP;
-    for (int c = 0; c < a.ytcChunks; ++c)
-      for (int yy = 0; yy < kYtcChunk; ++yy) {
-        const int y = c * kYtcChunk + yy;
-        if (y >= ey) continue;
-        for (int ky = 0; ky < a.nky; ++ky) {
-          const float2 w = twy[static_cast<size_t>(y) * a.nkyp + ky];
-          // B'[2y + cz][2ky + d]: {Wr, Wi ; -Wi, Wr}[cz][d]
-          const float vals[2][2] = {{w.x, w.y}, {-w.y, w.x}};
-          for (int cz = 0; cz < 2; ++cz)
-            for (int d = 0; d < 2; ++d) {
-              const int kp = 2 * yy + cz, np = 2 * ky + d;
-              const float v = vals[cz][d];
-              uint32_t bits;
-              std::memcpy(&bits, &v, sizeof(bits));
-              bits &= 0xFFFFE000u;
-              float head;
-              std::memcpy(&head, &bits, sizeof(head));
-              const size_t o = static_cast<size_t>(c) * 2 * blk + static_cast<size_t>(kp / 4) * (Np / 8) * 32 +
-                               (np / 8) * 32 + (np % 8) * 4 + kp % 4;
-              twytc[o] = head;
-              twytc[o + blk] = v - head;
-            }
-        }
-      }
-  }
+  const std::vector<float> twytc =
+      pl->use_ytc ? dtc_bprime(twy, a.nkyp, ey, a.nky, pl->yshape) : std::vector<float>();
+  const std::vector<float> twxtc =
+      pl->use_xtc ? dtc_bprime(twx, a.nkxp, ex, a.nkx, pl->xshape) : std::vector<float>();
   const int ndim = std::max(nn[0], std::max(nn[1], nn[2]));
   std::vector<float> mx(nn[0]), my(nn[1]), mz(nn[2]);
   saxs::bspline_moduli(nn[0], ndim, mx.data());
@@ -2608,6 +2732,7 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
       (rc = up(d_twzs, twzs.data(), sizeof(float) * twzs.size())) ||
       (rc = up(d_twztc, twtc.data(), sizeof(float) * twtc.size())) ||
       (rc = up(d_twytc, twytc.data(), sizeof(float) * twytc.size())) ||
+      (rc = up(d_twxtc, twxtc.data(), sizeof(float) * twxtc.size())) ||
       (rc = up(d_hy, hyt.data(), sizeof(int4) * hyt.size())) ||
       (rc = up(pl->d_geom0, g0, sizeof(g0)))) {
     destroy(pl);
@@ -2631,7 +2756,8 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
   if (e == cudaSuccess) e = raise_smem_limit(k_hist<float>);
   if (e == cudaSuccess) e = raise_smem_limit(k_hist<double>);
   if (e == cudaSuccess) e = raise_smem_limit(k_spread_zdft_tc);
-  if (e == cudaSuccess) e = raise_smem_limit(k_ydft_tc);
+  if (e == cudaSuccess) e = raise_smem_limit(k_dft_tc<false>);
+  if (e == cudaSuccess) e = raise_smem_limit(k_dft_tc<true>);
   if (e == cudaSuccess) {
     int per_sm = 0, sms = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_spread_zdft, kThreads,
@@ -2648,9 +2774,15 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
     }
     if (e == cudaSuccess && pl->use_ytc) {
       int per = 0;
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_ydft_tc, kYtcThreads, pl->smem_ydft_tc);
-      per = std::min(std::max(1, per), 512 / a.ytcCols);
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_dft_tc<false>, kDtcThreads, pl->smem_ydft_tc);
+      per = std::min(std::max(1, per), 512 / pl->yshape.cols);
       pl->ytc_ctas = per * std::max(1, sms);
+    }
+    if (e == cudaSuccess && pl->use_xtc) {
+      int per = 0;
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_dft_tc<true>, kDtcThreads, pl->smem_xdft_tc);
+      per = std::min(std::max(1, per), 512 / pl->xshape.cols);
+      pl->xtc_ctas = per * std::max(1, sms);
     }
   }
   if (e != cudaSuccess) {
@@ -2708,17 +2840,82 @@ int launch_spread(const SaxsPlan *pl, const DevArgs &a, int items, cudaStream_t 
   return launch_check("k_spread_zdft");
 }
 
+// cuTensorMapEncodeTiled, fetched from the driver once (no link to libcuda).
+using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *,
+                                   CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
+                                   CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      p = nullptr;
+    }
+    return reinterpret_cast<EncodeTiledFn>(p);
+  }();
+  return fn;
+}
+
+// Float32 tiled tensor map over `base` (no swizzle, zero fill outside).
+int encode_map(CUtensorMap *m, const void *base, int rank, const cuuint64_t *dims, const cuuint64_t *strides,
+               const cuuint32_t *box) {
+  EncodeTiledFn fn = encode_tiled();
+  if (!fn) return fail(SAXS_E_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+  const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+  const CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, static_cast<cuuint32_t>(rank), const_cast<void *>(base),
+                        dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(SAXS_E_CUDA, "tensor map encoding failed (" + std::to_string(r) + ")");
+  return SAXS_OK;
+}
+
 // y-axis DFT of `planes` z-transformed planes: the tensor-core kernel when the
 // plan has it, else the FP32 SIMT kernel.
 int launch_ydft(const SaxsPlan *pl, const DevArgs &a, int planes, cudaStream_t st) {
   if (pl->use_ytc) {
     const int items = planes * ((a.ext[0] + 127) / 128);
-    k_ydft_tc<<<std::max(1, std::min(items, pl->ytc_ctas)), kYtcThreads, pl->smem_ydft_tc, st>>>(a, items);
-    return launch_check("k_ydft_tc");
+    // Z[plane][x][y] as {2*ey floats, x, plane}
+    const cuuint64_t ex = a.ext[0], ey = a.ext[1];
+    const cuuint64_t dims[3] = {2 * ey, ex, static_cast<cuuint64_t>(planes)};
+    const cuuint64_t strides[2] = {8 * ey, 8 * ey * ex};
+    const cuuint32_t box[3] = {2 * kDtcChunk, 128, 1};
+    CUtensorMap map;
+    if (int rc = encode_map(&map, a.Z, 3, dims, strides, box)) return rc;
+    k_dft_tc<false><<<std::max(1, std::min(items, pl->ytc_ctas)), kDtcThreads, pl->smem_ydft_tc, st>>>(
+        a, pl->yshape, map, items);
+    return launch_check("k_dft_tc<y>");
   }
   dim3 gy((a.ext[0] + kYRows - 1) / kYRows, a.nkz, planes / a.nkz);
   k_ydft<<<gy, kThreads, pl->smem_ydft, st>>>(a);
   return launch_check("k_ydft");
+}
+
+// x-axis DFT, form factors, type sum and moduli of `nframes` frames into ibox:
+// the tensor-core kernel when the plan has it, else the FP32 SIMT kernel.
+int launch_xdft(const SaxsPlan *pl, const DevArgs &a, int nframes, cudaStream_t st) {
+  if (pl->use_xtc) {
+    const int kyb = 128 / a.xtcTP;
+    const int items = nframes * a.nkz * ((a.nky + kyb - 1) / kyb);
+    // Y[f][t][kz][ky][x] as {2*ex floats, t, ky, kz, f}
+    const cuuint64_t ex = a.ext[0];
+    const cuuint64_t dims[5] = {2 * ex, static_cast<cuuint64_t>(a.T), static_cast<cuuint64_t>(a.nky),
+                                static_cast<cuuint64_t>(a.nkz), static_cast<cuuint64_t>(nframes)};
+    const cuuint64_t row = 8 * ex;
+    const cuuint64_t strides[4] = {row * a.nky * a.nkz, row, row * a.nky, row * a.nky * a.nkz * a.T};
+    const cuuint32_t box[5] = {2 * kDtcChunk, static_cast<cuuint32_t>(a.xtcTP), static_cast<cuuint32_t>(kyb), 1, 1};
+    CUtensorMap map;
+    if (int rc = encode_map(&map, a.Y, 5, dims, strides, box)) return rc;
+    k_dft_tc<true><<<std::max(1, std::min(items, pl->xtc_ctas)), kDtcThreads, pl->smem_xdft_tc, st>>>(
+        a, pl->xshape, map, items);
+    return launch_check("k_dft_tc<x>");
+  }
+  dim3 gx((a.nky + kXRows - 1) / kXRows, a.nkz, nframes);
+  k_xdft_post<<<gx, kThreads, pl->smem_xdft, st>>>(a, pl->xc);
+  return launch_check("k_xdft_post");
 }
 
 // Enqueue the memsets and kernels of one batch of `nframes` frames whose
@@ -2764,11 +2961,10 @@ int enqueue_batch(SaxsPlan *pl, const DevArgs &a, int nframes, cudaStream_t st, 
     if (rc) return rc;
   }
   {
-    dim3 gx((a.nky + kXRows - 1) / kXRows, a.nkz, nframes);
     tm.begin(kStXdft);
-    k_xdft_post<<<gx, kThreads, pl->smem_xdft, st>>>(a, pl->xc);
+    const int rc = launch_xdft(pl, a, nframes, st);
     tm.end(kStXdft);
-    if (int rc = launch_check("k_xdft_post")) return rc;
+    if (rc) return rc;
   }
   tm.begin(kStHist);
   if (pl->ensemble == SAXS_NPT) {
@@ -3224,9 +3420,7 @@ int forward_into_scratch(SaxsPlan *pl, const float *xyz, const float *box, unsig
   const int items = a.stiles[0] * a.stiles[1] * a.T;
   if (int rc = launch_spread(pl, a, items, st)) return rc;
   if (int rc = launch_ydft(pl, a, a.T * a.nkz, st)) return rc;
-  dim3 gx((a.nky + kXRows - 1) / kXRows, a.nkz, 1);
-  k_xdft_post<<<gx, kThreads, pl->smem_xdft, st>>>(a, pl->xc);
-  if (int rc = launch_check("k_xdft_post")) return rc;
+  if (int rc = launch_xdft(pl, a, 1, st)) return rc;
   dim3 gh(a.nkz, 1);
   k_hist<float><<<gh, kThreads, pl->smem_hist, st>>>(a, a.ibox, a.geom, kGeom, 1.0, hist, nhist);
   return launch_check("k_hist");
@@ -3260,7 +3454,7 @@ int saxs_plan_info(const SaxsPlan *pl, SaxsPlanInfo *info) {
   info->kbox[1] = a.nky;
   info->kbox[2] = a.nkz;
   info->kz_count = a.nkz;
-  info->path = (pl->use_tc ? 1 : 0) | (pl->use_ytc ? 2 : 0);
+  info->path = (pl->use_tc ? 1 : 0) | (pl->use_ytc ? 2 : 0) | (pl->use_xtc ? 4 : 0);
   info->device_bytes = pl->bytes;
   info->frames_accumulated = pl->frames;
   return SAXS_OK;

@@ -152,13 +152,15 @@ class SaxsEngine:
                 e - s, b[s:e].ctypes.data_as(_native.c_float_p),
                 ctypes.c_void_p(self.stream.cuda_stream)))
 
-    def forward_host(self, xyz, boxes) -> None:
+    def forward_host(self, xyz, boxes, chunk: int | None = None) -> None:
         """Process frames held in host memory, (B, natoms, 3) or (natoms, 3).
 
         ``xyz`` is a numpy array or a CPU torch tensor.  A pinned tensor is
         copied straight to the device; anything else goes through a pinned
         staging buffer first.  Host-to-device copies run on a copy stream,
-        double-buffered against the compute stream.
+        double-buffered against the compute stream, in sub-batches of ``chunk``
+        frames (default: a quarter of the call's frames, at most max_frames) so
+        that the copy of one sub-batch overlaps the kernels of the previous one.
         """
         torch = self._torch
         pinned = isinstance(xyz, torch.Tensor) and xyz.device.type == "cpu" and xyz.is_pinned()
@@ -181,8 +183,9 @@ class SaxsEngine:
             raise ValueError("positions must have shape (B, natoms, 3)")
         st = self._staging_buffers(x.shape[1])
         B = self.max_frames
-        for s in range(0, nf, B):
-            e = min(nf, s + B)
+        step = min(B, max(1, -(-nf // 4))) if chunk is None else max(1, min(B, int(chunk)))
+        for s in range(0, nf, step):
+            e = min(nf, s + step)
             slot = st["next"]
             st["next"] ^= 1
             dev = st["dev"][slot]

@@ -1,9 +1,9 @@
-"""Tensor-core (tcgen05, 3xTF32) z- and y-axis DFTs vs the FP32 SIMT kernels and the FP64 oracle (GPU).
+"""Tensor-core (tcgen05, 3xTF32) z-, y- and x-axis DFTs vs the FP32 SIMT kernels and the FP64 oracle (GPU).
 
 Plans take a tensor-core kernel whenever its operands fit shared memory
-(``info.path`` bit 0 for the z-axis DFT, bit 1 for the y-axis DFT);
-``PYCUSAXS_ZDFT=simt`` / ``PYCUSAXS_YDFT=simt`` at plan creation keep the SIMT
-kernel.  Both must give identical bin counts and profiles within the 1e-4
+(``info.path`` bits 0, 1, 2 for the z-, y- and x-axis DFTs);
+``PYCUSAXS_ZDFT=simt`` / ``PYCUSAXS_YDFT=simt`` / ``PYCUSAXS_XDFT=simt`` at plan
+creation keep the SIMT kernel.  Both must give identical bin counts and profiles within the 1e-4
 tolerance of the FP64 oracle; the 3xTF32 products are accurate to ~2^-19, and
 TC_VS_SIMT_RTOL (2e-5 per bin) bounds the difference between the two kernels.
 """
@@ -37,8 +37,11 @@ def dft_mode(var, mode):
             os.environ[var] = old
 
 
+_AXES = {"z": ("PYCUSAXS_ZDFT", 1), "y": ("PYCUSAXS_YDFT", 2), "x": ("PYCUSAXS_XDFT", 4)}
+
+
 def _both(system, grid, frames, expect_tc=True, axis="z", **kw):
-    var, bit = ("PYCUSAXS_ZDFT", 1) if axis == "z" else ("PYCUSAXS_YDFT", 2)
+    var, bit = _AXES[axis]
     with dft_mode(var, None):
         h_tc, n_tc, e_tc = engine_hist(system, grid, frames, **kw)
         path_tc = e_tc.info.path
@@ -160,3 +163,50 @@ def test_ytc_batched_frames(cuda):
     s = cubic_system(5000, 40.0, seed=26, jitter=0.5, nframes=3)
     frames = [s.frame(k) for k in range(3)]
     _both(s, (32, 32, 32), frames, axis="y", sigma=2.0, qcut=0.6, max_frames=3)
+
+
+# -- x-axis DFT (with form factors, type sum and moduli) --------------------
+
+
+def test_xtc_small_cubic(cuda):
+    s = cubic_system(4000, 40.0, seed=31)
+    _both(s, (32, 32, 32), [s.positions], axis="x", sigma=2.0, qcut=0.6)
+
+
+def test_xtc_bench_sized_grid128(cuda):
+    s = cubic_system(30_000, 120.0, seed=32)
+    _both(s, (128, 128, 128), [s.positions], axis="x", sigma=2.0, qcut=0.5, bin_size=0.002)
+
+
+def test_xtc_x_extent_not_multiple_of_chunk(cuda):
+    s = _line_system(3000, (30.0, 40.0, 44.0), 33, ("H", "C", "O", "N"))
+    _both(s, (24, 40, 44), [s.positions], axis="x", sigma=2.5, qcut=0.9)
+
+
+def test_xtc_ten_types_sixteen_rows_per_ky(cuda):
+    els = ("H", "C", "N", "O", "P", "S", "Na", "Cl", "K", "Mg")
+    s = _line_system(5000, (40.0, 40.0, 40.0), 34, els)
+    _both(s, (32, 32, 32), [s.positions], axis="x", sigma=2.0, qcut=0.7)
+
+
+def test_xtc_seventeen_types_keep_simt(cuda):
+    els = ("H", "C", "N", "O", "P", "S", "Na", "Cl", "K", "Mg", "Ca", "F", "Br", "I", "Fe", "Zn", "Cu")
+    s = _line_system(5000, (40.0, 40.0, 40.0), 35, els)
+    _both(s, (32, 32, 32), [s.positions], axis="x", expect_tc=False, sigma=2.0, qcut=0.7)
+
+
+def test_xtc_triclinic(cuda):
+    from pycusaxs_b200.synthetic import triclinic_slab_system
+    s = triclinic_slab_system(5000, 40.0, 40.0, 32.0, 80.0, seed=36)
+    _both(s, (32, 32, 32), [s.positions], axis="x", sigma=2.0, qcut=0.7)
+
+
+def test_xtc_full_kx_axis_keeps_simt(cuda):
+    s = _line_system(1500, (192.0, 16.0, 16.0), 37)
+    _both(s, (96, 16, 16), [s.positions], axis="x", expect_tc=False, sigma=2.0, qcut=3.5)
+
+
+def test_xtc_batched_frames(cuda):
+    s = cubic_system(5000, 40.0, seed=38, jitter=0.5, nframes=3)
+    frames = [s.frame(k) for k in range(3)]
+    _both(s, (32, 32, 32), frames, axis="x", sigma=2.0, qcut=0.6, max_frames=3)
