@@ -568,6 +568,16 @@ __device__ __forceinline__ void umma_tf32(uint32_t tmem_d, uint64_t da, uint64_t
       "l"(da), "l"(db), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
 }
 
+// The same with A read from tensor memory (row m of A in lane m, K along columns).
+__device__ __forceinline__ void umma_tf32_ts(uint32_t tmem_d, uint32_t tmem_a, uint64_t db, uint32_t idesc,
+                                             uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
+      "r"(tmem_a), "l"(db), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+
 __device__ __forceinline__ uint64_t global_ns() {
   uint64_t t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -1150,17 +1160,16 @@ __global__ void __launch_bounds__(kThreads) k_ydft(DevArgs a) {
 //   of a ky, squares and multiplies by the B-spline moduli (the SIMT kernel's
 //   k_xdft_post), writing ibox[kz][ky][kx].
 // K is streamed in chunks of kDtcChunk values of u: per chunk the loader warp
-// issues one tensor copy (cp.async.bulk.tensor, no multicast) of the 128 rows
-// x 32 floats into a raw staging tile (rows outside the data zero-filled by the
-// tensor map) and one bulk copy of the B' chunk.  Operands are K-major,
-// no-swizzle (core matrices of 8 rows x 16 B): A element (r, k') at
-// (k'/4)*512 + (r/8)*32 + (r%8)*4 + k'%4 floats (LBO 2048 B, SBO 128 B); B'
-// element (n', k') at (k'/4)*(N'/8)*32 + (n'/8)*32 + (n'%8)*4 + k'%4 (LBO N'*16
-// B, SBO 128 B).  Both are split into a TF32 head and remainder like the z-axis
-// DFT's operands.
+// issues one tensor copy (cp.async.bulk.tensor, no multicast, 128-byte swizzle)
+// of the 128 rows x 32 floats into a raw staging tile (rows outside the data
+// zero-filled by the tensor map) and one bulk copy of the B' chunk.  The
+// producers split the raw rows into a TF32 head and remainder and store them to
+// tensor memory, where the MMA reads A: row r of A is TMEM lane r, element k'
+// column a0 + k'.  B' stays in shared memory, K-major no-swizzle (core matrices
+// of 8 rows x 16 B): element (n', k') at (k'/4)*(N'/8)*32 + (n'/8)*32 + (n'%8)*4
+// + k'%4 floats (LBO N'*16 B, SBO 128 B), split on the host.
 constexpr int kDtcChunk = 16;                  // u values per K chunk (K' = 32)
 constexpr int kDtcProducerWarps = 8;
-constexpr int kDtcProducers = 32 * kDtcProducerWarps;
 constexpr int kDtcMmaWarp = kDtcProducerWarps;
 constexpr int kDtcLoaderWarp = kDtcProducerWarps + 1;
 constexpr int kDtcThreads = 32 * (kDtcProducerWarps + 6);  // producers, MMA, loader, 4 epilogue
@@ -1172,7 +1181,9 @@ struct DtcShape {
   const float *B;  // [chunk][2][N' x 2*kDtcChunk]: head block then remainder block
 };
 
-// Tensor copy of chunk c of item w's 128 rows into `dst` (y pass: 3-D map
+// Tensor copy of chunk c of item w's 128 rows into `dst`, 1024-byte aligned
+// (128-byte swizzle: the 16-byte piece j of row r lands at piece j ^ (r % 8) of
+// the row) (y pass: 3-D map
 // {2*ey floats, ex rows, planes}; x pass: 5-D map {2*ex floats, type, ky, kz,
 // frame} whose box {32, TP, 128/TP, 1, 1} lands rows in (ky, type) order).
 template <bool kX>
@@ -1208,8 +1219,10 @@ __device__ __forceinline__ void dtc_tensor_copy(const DevArgs &a, const CUtensor
 //   empty[st] MMA commit -> loader (stage st read)
 //   dfull[d]  MMA commit -> epilogue (accumulator d complete)
 //   dempty[d] epilogue -> MMA (accumulator d read out)
-// Dynamic shared memory: S stages of { A head, A remainder (128 x K'), B' head,
-// B' remainder (N' x K'), raw A rows (128 x K') } floats.
+// Dynamic shared memory: S stages of { raw A rows (128 x K'), B' head, B'
+// remainder (N' x K') } floats, 1024-byte aligned.  Tensor memory (512
+// columns): accumulators d at columns d*N', A stage st at 2N' + 64*st (head) and
+// + 32 (remainder).
 template <bool kX>
 __global__ void __launch_bounds__(kDtcThreads, 1)
     k_dft_tc(DevArgs a, DtcShape sh, const __grid_constant__ CUtensorMap amap, int items) {
@@ -1219,12 +1232,12 @@ __global__ void __launch_bounds__(kDtcThreads, 1)
   __shared__ volatile int abort_flag;
   const int N = sh.N, NS = sh.S, NC = sh.chunks;
   const int KP = 2 * kDtcChunk;                      // K' per chunk
-  const int a_floats = 128 * KP, b_floats = N * KP;  // per head or remainder
-  const int stage_floats = 3 * a_floats + 2 * b_floats;
+  const int a_floats = 128 * KP, b_floats = N * KP;  // raw A tile; B' head or remainder
+  const int stage_floats = a_floats + 2 * b_floats;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  // tensor copies need a 128-byte aligned destination: the stages start at the
-  // first 128-byte boundary of the dynamic shared memory (128 bytes reserved)
-  float *stages = reinterpret_cast<float *>(smem + ((128u - (smem_addr(smem) & 127u)) & 127u));
+  // swizzled tensor copies need a 1024-byte aligned destination: the stages
+  // start at the first 1024-byte boundary of the dynamic shared memory
+  float *stages = reinterpret_cast<float *>(smem + ((1024u - (smem_addr(smem) & 1023u)) & 1023u));
   uint64_t *afull = bars, *bfull = bars + kDtcMaxStages, *empty = bars + 2 * kDtcMaxStages,
            *dfull = bars + 3 * kDtcMaxStages, *dempty = dfull + 2;
   if (warp == kDtcMmaWarp) {
@@ -1260,25 +1273,48 @@ __global__ void __launch_bounds__(kDtcThreads, 1)
   };
 
   if (warp < kDtcProducerWarps) {
-    // split the raw 128 x K' rows into head and remainder, K-major: 8 lanes per
-    // row read 128 contiguous bytes
+    // warp w owns TMEM lane quarter w % 4 (rows 32*(w%4) + lane) and K' columns
+    // 16*(w/4) .. +15 of each chunk: four 16-byte reads of its row (swizzled
+    // pieces, conflict-free across the 8 rows of a 1024-byte block), split, two
+    // 16-column stores to tensor memory
+    static_assert(kDtcProducerWarps == 8 && kDtcChunk == 16, "8 producer warps cover 128 rows x 32 columns");
+    const int quarter = warp & 3, half = warp >> 2;
+    const int r = 32 * quarter + lane;
+    const uint32_t lane_off = static_cast<uint32_t>(32 * quarter) << 16;
     int g = 0;
     for (int w = blockIdx.x; w < items; w += gridDim.x) {
       for (int c = 0; c < NC; ++c, ++g) {
         const int st = g % NS;
+        if (g >= NS) wait(&empty[st], g / NS - 1);  // the stage's MMAs have read its TMEM columns
         wait(&bfull[st], g / NS);
-        float *ah = stages + static_cast<size_t>(st) * stage_floats;
-        float *al = ah + a_floats;
-        const float *raw = ah + 2 * a_floats + 2 * b_floats;
-        for (int i = tid; i < 128 * (KP / 4); i += kDtcProducers) {
-          const int r = i >> 3, q = i & 7;
-          const float4 v = *reinterpret_cast<const float4 *>(raw + r * KP + 4 * q);
-          const float4 h = make_float4(tf32_head(v.x), tf32_head(v.y), tf32_head(v.z), tf32_head(v.w));
-          const int o = q * 512 + (r >> 3) * 32 + (r & 7) * 4;
-          *reinterpret_cast<float4 *>(ah + o) = h;
-          *reinterpret_cast<float4 *>(al + o) = make_float4(v.x - h.x, v.y - h.y, v.z - h.z, v.w - h.w);
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const float *raw = stages + static_cast<size_t>(st) * stage_floats;
+        uint32_t hi[16], lo[16];
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj) {
+          const int j = 4 * half + jj;
+          const float4 v = *reinterpret_cast<const float4 *>(raw + r * KP + 4 * (j ^ (r & 7)));
+          const float vv[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            const float h = tf32_head(vv[e]);
+            hi[4 * jj + e] = __float_as_uint(h);
+            lo[4 * jj + e] = __float_as_uint(vv[e] - h);
+          }
         }
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        const uint32_t col = tmem + lane_off + static_cast<uint32_t>(2 * N + 64 * st + 16 * half);
+        asm volatile(
+            "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], "
+            "{%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(col),
+            "r"(hi[0]), "r"(hi[1]), "r"(hi[2]), "r"(hi[3]), "r"(hi[4]), "r"(hi[5]), "r"(hi[6]), "r"(hi[7]),
+            "r"(hi[8]), "r"(hi[9]), "r"(hi[10]), "r"(hi[11]), "r"(hi[12]), "r"(hi[13]), "r"(hi[14]), "r"(hi[15]));
+        asm volatile(
+            "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], "
+            "{%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(col + 32),
+            "r"(lo[0]), "r"(lo[1]), "r"(lo[2]), "r"(lo[3]), "r"(lo[4]), "r"(lo[5]), "r"(lo[6]), "r"(lo[7]),
+            "r"(lo[8]), "r"(lo[9]), "r"(lo[10]), "r"(lo[11]), "r"(lo[12]), "r"(lo[13]), "r"(lo[14]), "r"(lo[15]));
+        asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         __syncwarp();
         if (lane == 0) mbar_arrive(smem_addr(&afull[st]));
       }
@@ -1299,10 +1335,10 @@ __global__ void __launch_bounds__(kDtcThreads, 1)
                        : "memory");
           asm volatile(
               "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                  smem_addr(sb + 2 * a_floats)),
+                  smem_addr(sb + a_floats)),
               "l"(sh.B + static_cast<size_t>(c) * 2 * b_floats), "r"(bbytes), "r"(bar)
               : "memory");
-          dtc_tensor_copy<kX>(a, &amap, w, c, smem_addr(sb + 2 * a_floats + 2 * b_floats), bar);
+          dtc_tensor_copy<kX>(a, &amap, w, c, smem_addr(sb), bar);
         }
       }
     }
@@ -1324,20 +1360,18 @@ __global__ void __launch_bounds__(kDtcThreads, 1)
           wait(&afull[st], g / NS);
           if (abort_flag) break;
           asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-          const float *ah = stages + static_cast<size_t>(st) * stage_floats;
-          const uint64_t dah0 = umma_desc(smem_addr(ah), 2048, 128);
-          const uint64_t dal0 = umma_desc(smem_addr(ah + a_floats), 2048, 128);
-          const uint64_t dbh0 = umma_desc(smem_addr(ah + 2 * a_floats), N * 16, 128);
-          const uint64_t dbl0 = umma_desc(smem_addr(ah + 2 * a_floats + b_floats), N * 16, 128);
-          // one k step (8 of K'): A advances 4096 B (+256), B' N*32 B (+N*2)
+          const float *sb = stages + static_cast<size_t>(st) * stage_floats;
+          const uint64_t dbh0 = umma_desc(smem_addr(sb + a_floats), N * 16, 128);
+          const uint64_t dbl0 = umma_desc(smem_addr(sb + a_floats + b_floats), N * 16, 128);
+          const uint32_t ah0 = tmem + static_cast<uint32_t>(2 * N + 64 * st);
+          // one k step (8 of K'): A advances 8 TMEM columns, B' N*32 B (+N*2)
           for (int kk = 0; kk < KP / 8; ++kk) {
-            const uint64_t dah = dah0 + static_cast<uint64_t>(kk * 256);
-            const uint64_t dal = dal0 + static_cast<uint64_t>(kk * 256);
+            const uint32_t ah = ah0 + 8 * kk, al = ah + 32;
             const uint64_t dbh = dbh0 + static_cast<uint64_t>(kk * 2 * N);
             const uint64_t dbl = dbl0 + static_cast<uint64_t>(kk * 2 * N);
-            umma_tf32(dcol, dal, dbh, idesc, (c > 0 || kk > 0) ? 1u : 0u);
-            umma_tf32(dcol, dah, dbl, idesc, 1u);
-            umma_tf32(dcol, dah, dbh, idesc, 1u);
+            umma_tf32_ts(dcol, al, dbh, idesc, (c > 0 || kk > 0) ? 1u : 0u);
+            umma_tf32_ts(dcol, ah, dbl, idesc, 1u);
+            umma_tf32_ts(dcol, ah, dbh, idesc, 1u);
           }
           asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                            smem_addr(&empty[st]))
@@ -2330,16 +2364,15 @@ void destroy(SaxsPlan *pl) {
 // `avail` bytes of shared memory.  Returns false when the pass does not fit.
 bool dtc_shape(int nk, int extent, size_t avail, DtcShape *sh, size_t *smem) {
   const int N = round_up(2 * nk, 16);
-  const size_t stage_bytes = (3 * 128 + 2 * static_cast<size_t>(N)) * 2 * kDtcChunk * sizeof(float);
-  const int S = static_cast<int>(std::min<size_t>(kDtcMaxStages, (avail - 128) / stage_bytes));
+  const size_t stage_bytes = (128 + 2 * static_cast<size_t>(N)) * 2 * kDtcChunk * sizeof(float);
+  // tensor memory: two accumulators of N' columns and 64 columns of A per stage
+  const int S = std::min({kDtcMaxStages, static_cast<int>((avail - 1024) / stage_bytes), (512 - 2 * N) / 64});
   if (N > 256 || S < 2) return false;
   sh->N = N;
   sh->chunks = (extent + kDtcChunk - 1) / kDtcChunk;
   sh->S = S;
-  int cols = 32;
-  while (cols < 2 * N) cols *= 2;
-  sh->cols = cols;
-  *smem = S * stage_bytes + 128;  // + alignment slack of the stage base
+  sh->cols = 512;
+  *smem = S * stage_bytes + 1024;  // + alignment slack of the stage base
   return true;
 }
 
@@ -2860,14 +2893,14 @@ EncodeTiledFn encode_tiled() {
   return fn;
 }
 
-// Float32 tiled tensor map over `base` (no swizzle, zero fill outside).
+// Float32 tiled tensor map over `base` (128-byte swizzle, zero fill outside).
 int encode_map(CUtensorMap *m, const void *base, int rank, const cuuint64_t *dims, const cuuint64_t *strides,
                const cuuint32_t *box) {
   EncodeTiledFn fn = encode_tiled();
   if (!fn) return fail(SAXS_E_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
   const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
   const CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, static_cast<cuuint32_t>(rank), const_cast<void *>(base),
-                        dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                        dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return fail(SAXS_E_CUDA, "tensor map encoding failed (" + std::to_string(r) + ")");
   return SAXS_OK;
