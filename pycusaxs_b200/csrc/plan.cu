@@ -710,9 +710,9 @@ struct AtomTab {
 __device__ __forceinline__ void spread_prepass(const DevArgs &a, const TileAtoms &ta,
                                                const float4 *srec, int nrec_smem, int f, int v0,
                                                int nv, const AtomTab &tab, int x0, int y0, int cw,
-                                               int ch, int tid) {
+                                               int ch, int tid, int nthreads) {
   const int P = a.order, nt = a.ntaps, nz = a.n[2];
-  for (int i = tid; i < nv; i += kTcProducers) {
+  for (int i = tid; i < nv; i += nthreads) {
     const int v = v0 + i;
     float4 q;
     if (v < nrec_smem) {
@@ -757,8 +757,9 @@ __device__ __forceinline__ void spread_prepass(const DevArgs &a, const TileAtoms
 
 // Spreading taps: one lane per (atom, y tap, z tap), four x taps each.  The 16
 // lanes of an atom write 16 different banks (bank = 4*ly + z%4).
-__device__ __forceinline__ void spread_taps(const AtomTab &tab, int nv, int nt, float *A, int tid) {
-  for (int u = tid; u < nv * 16; u += kTcProducers) {
+__device__ __forceinline__ void spread_taps(const AtomTab &tab, int nv, int nt, float *A, int tid,
+                                            int nthreads) {
+  for (int u = tid; u < nv * 16; u += nthreads) {
     const int i = u >> 4, p = (u >> 2) & 3, r = u & 3;
     if (p >= nt || r >= nt) continue;
     const int ly = (tab.ly[i] >> (8 * p)) & 0xFF;
@@ -782,20 +783,21 @@ __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 
-__device__ __forceinline__ void producers_sync() {
-  asm volatile("bar.sync 1, %0;" ::"r"(kTcProducers) : "memory");
+// Named barrier `id` over `count` producer threads.
+__device__ __forceinline__ void producers_sync(int id, int count) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
 }
 
-// Producer barrier that also returns the OR of `v` over the producers.
-__device__ __forceinline__ bool producers_sync_or(bool v) {
+// The same barrier, also returning the OR of `v` over its threads.
+__device__ __forceinline__ bool producers_sync_or(bool v, int id, int count) {
   uint32_t out;
   asm volatile(
       "{\n\t.reg .pred pi, po;\n\t"
       "setp.ne.u32 pi, %1, 0;\n\t"
-      "bar.red.or.pred po, 1, %2, pi;\n\t"
+      "bar.red.or.pred po, %2, %3, pi;\n\t"
       "selp.u32 %0, 1, 0, po;\n\t}\n"
       : "=r"(out)
-      : "r"(static_cast<uint32_t>(v)), "r"(kTcProducers)
+      : "r"(static_cast<uint32_t>(v)), "r"(id), "r"(count)
       : "memory");
   return out != 0;
 }
@@ -805,7 +807,11 @@ __device__ __forceinline__ bool producers_sync_or(bool v) {
 //   producer warps (kTcProducerWarps): zero the stage's A tile, spread the
 //               item's atoms into it (a per-atom pre-pass, then shared-memory
 //               atomics per tap), subtract the padding mean and split it into
-//               the TF32 head (in place) and remainder
+//               the TF32 head (in place) and remainder.  With two operand
+//               stages they form two groups that take alternate items (group g:
+//               items j = g mod 2, stage and record slot g, named barrier 1 + g,
+//               its own atom table), so one group's barriers and waits overlap
+//               the other group's work
 //   next warp   one lane issues the 3xTF32 MMAs of an item into its TMEM stage
 //   next warp   loader: home-bin record ranges, frame/type/tile and padding mean
 //               of an item, and bulk copies (cp.async.bulk) of its atom records
@@ -820,7 +826,8 @@ __device__ __forceinline__ bool producers_sync_or(bool v) {
 //   tmem_empty[s] epilogue -> MMA (TMEM stage s read out)
 // Dynamic shared memory: Bh, Bl (tcK x tcN floats each), tcS stages of
 // A32 (tcR x 64) + Al (tcK x 64), two record buffers of tcRB float4, the
-// home-bin tables (stiles[0] + stiles[1] int4) and the atom table.
+// home-bin tables (stiles[0] + stiles[1] int4) and one atom table per producer
+// group.
 __global__ void __launch_bounds__(kTcThreads, 1) k_spread_zdft_tc(DevArgs a, int items) {
   extern __shared__ __align__(16) unsigned char smem[];  // no-swizzle operands need 16 B
   __shared__ TcSlot slot[2];
@@ -835,9 +842,14 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_spread_zdft_tc(DevArgs a, int
   float4 *recs = reinterpret_cast<float4 *>(stages + static_cast<size_t>(S) * (R + KT) * 64);
   int4 *home_x = reinterpret_cast<int4 *>(recs + 2 * RB);
   int4 *home_y = home_x + a.stiles[0];
-  AtomTab tab;
-  tab.wx = reinterpret_cast<float4 *>(home_y + a.stiles[1]);
+  // producer groups: two when there are two operand stages
+  const int G = S == 2 ? 2 : 1;
+  const int group = warp < kTcProducerWarps ? warp / (kTcProducerWarps / G) : 0;
+  const int gthreads = kTcProducers / G, gtid = tid - group * gthreads;
   const int cap = a.tcCap;
+  AtomTab tab;
+  tab.wx = reinterpret_cast<float4 *>(reinterpret_cast<unsigned char *>(home_y + a.stiles[1]) +
+                                      static_cast<size_t>(group) * cap * kTcAtomBytes);
   tab.wy = tab.wx + cap;
   tab.wz = tab.wy + cap;
   tab.zo = reinterpret_cast<int4 *>(tab.wz + cap);
@@ -859,7 +871,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_spread_zdft_tc(DevArgs a, int
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
   }
   if (tid == 0) {
-    const int counts[10] = {1, 1, 1, 1, kTcProducerWarps, kTcProducerWarps, 1, 1, 4, 4};
+    const int counts[10] = {1, 1, 1, 1, kTcProducerWarps / G, kTcProducerWarps / G, 1, 1, 4, 4};
     for (int i = 0; i < 10; ++i)
       asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&bars[i])), "r"(counts[i]));
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -881,19 +893,19 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_spread_zdft_tc(DevArgs a, int
   };
 
   if (warp < kTcProducerWarps) {
-    int j = 0;
-    for (int w = blockIdx.x; w < items; w += gridDim.x, ++j) {
+    const int bar_id = 1 + group;
+    for (int j = group, w = blockIdx.x + group * gridDim.x; w < items; j += G, w += G * gridDim.x) {
       const int b = j & 1, s = S == 2 ? (j & 1) : 0;
       float *A32 = stages + static_cast<size_t>(s) * (R + KT) * 64;
       float *Al = A32 + static_cast<size_t>(R) * 64;
       if (j >= S) wait(&done[s], (j - S) / S);  // the stage's previous MMAs are finished
       {
         float4 *t4 = reinterpret_cast<float4 *>(A32);
-        for (int i = tid; i < R * 16; i += kTcProducers) t4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int i = gtid; i < R * 16; i += gthreads) t4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
       }
       wait(&rec_full[b], j >> 1);
       // one decision for all producers: the spreading below has barriers inside
-      const bool skip = producers_sync_or(abort_flag != 0);
+      const bool skip = producers_sync_or(abort_flag != 0, bar_id, gthreads);
       const TcSlot &sl = slot[b];
       const float mean = sl.mean;
       if (!skip) {
@@ -901,21 +913,21 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_spread_zdft_tc(DevArgs a, int
         const int nrec = min(nvis, RB);
         for (int v0 = 0; v0 < nvis; v0 += cap) {
           const int nv = min(cap, nvis - v0);
-          if (v0 > 0) producers_sync();  // the previous chunk's taps have read the table
+          if (v0 > 0) producers_sync(bar_id, gthreads);  // the previous chunk's taps have read the table
           spread_prepass(a, sl.ta, recs + static_cast<size_t>(b) * RB, nrec, sl.f, v0, nv, tab, sl.x0,
-                         sl.y0, sl.cw, sl.ch, tid);
-          producers_sync();
-          spread_taps(tab, nv, a.ntaps, A32, tid);
+                         sl.y0, sl.cw, sl.ch, gtid, gthreads);
+          producers_sync(bar_id, gthreads);
+          spread_taps(tab, nv, a.ntaps, A32, gtid, gthreads);
         }
       }
-      producers_sync();
-      if (tid == 0) mbar_arrive(smem_addr(&rec_empty[b]));
+      producers_sync(bar_id, gthreads);
+      if (gtid == 0) mbar_arrive(smem_addr(&rec_empty[b]));
       {
         // padding mean applied before the TF32 split: the tensor cores see
         // g - mean (rows z >= ez meet zero twiddles)
         float4 *h4 = reinterpret_cast<float4 *>(A32);
         float4 *l4 = reinterpret_cast<float4 *>(Al);
-        for (int i = tid; i < KT * 16; i += kTcProducers) {
+        for (int i = gtid; i < KT * 16; i += gthreads) {
           float4 v = h4[i];
           v.x -= mean;
           v.y -= mean;
@@ -1429,13 +1441,17 @@ __global__ void __launch_bounds__(kDtcThreads, 1)
         const int f = w / (a.nkz * nblk), kz = (w / nblk) % a.nkz;
         const int ky = (w % nblk) * kyb + r / tp, t = r % tp;
         const bool row_ok = t < a.T && ky < a.nky;
-        const float *ocs = a.geom + f * kGeom + 9;
+        float ocs[9];
+#pragma unroll
+        for (int q = 0; q < 9; ++q) ocs[q] = a.geom[f * kGeom + 9 + q];
         const int ka = signed_k(kz, a.nn[2], a.nf[2]);
         const int ja = a.ky_lo + min(ky, a.nky - 1);
         const float mean = row_ok ? static_cast<float>(a.border[static_cast<int64_t>(f) * a.T + t] /
                                                        a.border_count)
                                   : 0.0f;
-        const float *ff = a.ff + 9 * (t < a.T ? t : 0);
+        float ff[9];
+#pragma unroll
+        for (int q = 0; q < 9; ++q) ff[q] = a.ff[9 * (t < a.T ? t : 0) + q];
         const int jw = ja < 0 ? ja + a.nn[1] : ja;
         const float mzy = a.mody[jw] * a.modz[kz];
         float *ib = a.ibox + ((static_cast<int64_t>(f) * a.nkz + kz) * a.nky + ky) * a.nkx;
@@ -2569,12 +2585,13 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
     // two operand stages before larger record buffers before a larger atom
     // table; records beyond the staging buffer are read from global memory,
     // atoms beyond the table are spread in further chunks
+    // (one atom table per producer group: two groups with two stages)
     int S = 0, RB = 0, CAP = 0;
     for (int s_try = 2; s_try >= 1 && S == 0; --s_try)
-      for (int rb = 1024; rb >= 128 && S == 0; rb /= 2)
-        for (int cap = 256; cap >= 64 && S == 0; cap /= 2)
+      for (int cap = 256; cap >= 64 && S == 0; cap /= 2)
+        for (int rb = 1024; rb >= 128 && S == 0; rb /= 2)
           if (b_bytes + s_try * stage_bytes + 2 * static_cast<size_t>(rb) * 16 + home_bytes +
-                  static_cast<size_t>(cap) * kTcAtomBytes <= avail) {
+                  static_cast<size_t>(s_try) * cap * kTcAtomBytes <= avail) {
             S = s_try;
             RB = rb;
             CAP = cap;
@@ -2591,7 +2608,7 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
       while (cols < S * N) cols *= 2;
       a.tcCols = cols;
       pl->smem_spread_tc = b_bytes + S * stage_bytes + 2 * static_cast<size_t>(RB) * 16 + home_bytes +
-                           static_cast<size_t>(CAP) * kTcAtomBytes;
+                           static_cast<size_t>(S) * CAP * kTcAtomBytes;
     }
   }
   {
