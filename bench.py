@@ -59,34 +59,88 @@ def parse():
 
 
 class ClockSampler:
-    """nvidia-smi SM clocks and throttle reasons, sampled every 200 ms."""
+    """SM clock and clock-event (throttle) reasons of the bench GPU, read through NVML
+    every 2 ms from a thread while the timed region runs (reading only; nothing is
+    set).  Falls back to `nvidia-smi -lms 200` when NVML cannot be loaded."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"),
+               ("hw_power_brake_slowdown", "nvmlClocksEventReasonHwPowerBrakeSlowdown"))
 
     def __init__(self, index: int):
         self.index = index
+        self.samples: list[tuple[float, int]] = []
+        self.smax = None
+        self._stop = threading.Event()
+        self._thread = None
+        self._nvml = None
+        self._handle = None
         self.proc = None
         self.lines: list[str] = []
 
+    def _open_nvml(self):
+        import pynvml
+        import torch
+
+        pynvml.nvmlInit()
+        try:
+            props = torch.cuda.get_device_properties(self.index)
+            bus = "%08x:%02x:%02x.0" % (props.pci_domain_id, props.pci_bus_id, props.pci_device_id)
+            handle = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            handle = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+        self._nvml, self._handle = pynvml, handle
+        self.smax = float(pynvml.nvmlDeviceGetMaxClockInfo(handle, pynvml.NVML_CLOCK_SM))
+
+    def _poll(self):
+        nv, h = self._nvml, self._handle
+        while True:
+            try:
+                self.samples.append((float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)),
+                                     int(nv.nvmlDeviceGetCurrentClocksEventReasons(h))))
+            except Exception:
+                pass
+            if self._stop.wait(0.002):
+                break
+
     def start(self):
         try:
+            self._open_nvml()
+            self._thread = threading.Thread(target=self._poll, daemon=True)
+            self._thread.start()
+            t0 = time.time()
+            while not self.samples and time.time() - t0 < 1.0:  # first sample before the timed region
+                time.sleep(0.001)
+            return
+        except Exception:
+            self._nvml = None
+        try:
             self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                ["nvidia-smi", f"--id={self.index}",
+                 "--query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap",
                  "--format=csv,noheader,nounits", "-lms", "200"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            threading.Thread(target=self._read, daemon=True).start()
+            threading.Thread(target=lambda: self.lines.extend(l.strip() for l in self.proc.stdout),
+                             daemon=True).start()
         except OSError:
             self.proc = None
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
-
     def stop(self) -> dict:
+        if self._nvml is not None:
+            self._stop.set()
+            self._thread.join(timeout=2)
+            nv = self._nvml
+            reasons = sorted({name for name, const in self.REASONS
+                              for _, bits in self.samples if bits & getattr(nv, const, 0)})
+            sm = [c for c, _ in self.samples]
+            return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.smax,
+                    "reasons": reasons, "samples": len(sm), "source": "nvml, 2 ms"}
         if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clock sampling unavailable"]}
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
@@ -96,19 +150,19 @@ class ClockSampler:
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in self.lines:
             parts = [p.strip() for p in line.split(",")]
-            if len(parts) < 9:
+            if len(parts) < 6:
                 continue
             try:
-                sm.append(float(parts[1]))
-                smax.append(float(parts[2]))
+                sm.append(float(parts[0]))
+                smax.append(float(parts[1]))
             except ValueError:
                 continue
-            for n, v in zip(names, parts[5:9]):
+            for n, v in zip(names, parts[2:6]):
                 if v.lower().startswith("active"):
                     reasons.add(n)
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": max(smax) if smax else None, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": "nvidia-smi, 200 ms"}
 
 
 def dist_setup(args):
@@ -229,11 +283,25 @@ def bench_ours(args):
     per_launch_s = dom_ms / 1e3 / max(dom_launches, 1)
     frames_per_launch = frames_timed / max(dom_launches, 1)
     achieved = algo_bytes.get(dom, 0) * frames_per_launch / per_launch_s / 1e9
-    roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": hbm,
-                "unit": "GB/s", "frac": round(achieved / hbm, 4), "traffic": None,
+    # the kernel that ran for each stage: plan path bits 0/1/2 = z/y/x DFT on tcgen05
+    path = info.path
+    kernel_of = {"k_spread_zdft": "k_spread_zdft_tc" if path & 1 else "k_spread_zdft",
+                 "k_ydft": "k_dft_tc<y>" if path & 2 else "k_ydft",
+                 "k_xdft_post": "k_dft_tc<x>" if path & 4 else "k_xdft_post"}
+    tensor = bool({"k_spread_zdft": 1, "k_ydft": 2, "k_xdft_post": 4}.get(dom, 0) & path)
+    roofline = {"bound": "hbm", "kernel": kernel_of.get(dom, dom), "achieved": round(achieved, 1),
+                "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4), "traffic": None,
                 "peak_source": "measured" if peaks else "fallback"}
     if dom in algo_flops:
-        roofline["fp32_tflops"] = round(algo_flops[dom] * frames_per_launch / per_launch_s / 1e12, 2)
+        useful = algo_flops[dom] * frames_per_launch / per_launch_s / 1e12
+        if tensor:
+            # 3xTF32: three TF32 MMAs per product; dense TF32 peak = half the bf16 one
+            tf32_peak = float(peaks.get("bf16_tflops", 1590.0)) / 2
+            roofline["tensor"] = {"useful_tflops": round(useful, 2), "issued_tflops": round(3 * useful, 2),
+                                  "tf32_peak_tflops": tf32_peak,
+                                  "issued_frac": round(3 * useful / tf32_peak, 4)}
+        else:
+            roofline["fp32_tflops"] = round(useful, 2)
     stage_share = {k: round(v[0] / max(sum(x[0] for x in prof.values()), 1e-9), 4)
                    for k, v in prof.items()}
 
@@ -290,7 +358,9 @@ def bench_ours(args):
                                "(256^3 supercell), qcut 0.5/A, 100 frames per step, npt",
                    "frames_per_step_per_gpu": FRAMES, "batch": B, "l2": "flushed between steps",
                    "kbox": [nkx, nky, nkz], "plain_path_frames_per_s": round(plain, 1) if plain else None,
-                   "stage_share": stage_share, "parallelism": f"frames sharded over {world} GPU(s)",
+                   "stage_share": stage_share,
+                   "stage_kernels": {k: kernel_of.get(k, k) for k in stage_share},
+                   "parallelism": f"frames sharded over {world} GPU(s)",
                    "adjoint": adj, "multi_system": multi},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": ck,
         "gpu_launches": int(launches),

@@ -1184,7 +1184,12 @@ constexpr int kDtcChunk = 16;                  // u values per K chunk (K' = 32)
 constexpr int kDtcProducerWarps = 8;
 constexpr int kDtcMmaWarp = kDtcProducerWarps;
 constexpr int kDtcLoaderWarp = kDtcProducerWarps + 1;
-constexpr int kDtcThreads = 32 * (kDtcProducerWarps + 6);  // producers, MMA, loader, 4 epilogue
+// epilogue warps: 4 for the y pass (stores only), 12 for the x pass (form factors
+// per element), a multiple of 4 so each TMEM lane quarter has the same number
+template <bool kX>
+__host__ __device__ constexpr int dtc_epi_warps() { return kX ? 12 : 4; }
+template <bool kX>
+__host__ __device__ constexpr int dtc_threads() { return 32 * (kDtcProducerWarps + 2 + dtc_epi_warps<kX>()); }
 constexpr int kDtcMaxStages = 4;
 
 // One pass's GEMM shape: N', K chunks, stages, TMEM columns, B' table.
@@ -1223,7 +1228,7 @@ __device__ __forceinline__ void dtc_tensor_copy(const DevArgs &a, const CUtensor
 }
 
 // Persistent, warp-specialized: grid = min(items, resident CTAs), block
-// kDtcThreads.  Items: y pass (plane, block of 128 x rows), planes ordered
+// dtc_threads<kX>() (producers, MMA warp, loader warp, epilogue warps).  Items: y pass (plane, block of 128 x rows), planes ordered
 // (frame, type, kz) like Z and Y; x pass (frame, kz, block of 128/TP ky).
 // Barriers (all waits bounded):
 //   bfull[st] loader copies -> producers and MMA (raw A rows and B' landed)
@@ -1236,7 +1241,7 @@ __device__ __forceinline__ void dtc_tensor_copy(const DevArgs &a, const CUtensor
 // columns): accumulators d at columns d*N', A stage st at 2N' + 64*st (head) and
 // + 32 (remainder).
 template <bool kX>
-__global__ void __launch_bounds__(kDtcThreads, 1)
+__global__ void __launch_bounds__(dtc_threads<kX>(), 1)
     k_dft_tc(DevArgs a, DtcShape sh, const __grid_constant__ CUtensorMap amap, int items) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ __align__(8) uint64_t bars[3 * kDtcMaxStages + 4];
@@ -1266,7 +1271,7 @@ __global__ void __launch_bounds__(kDtcThreads, 1)
     }
     for (int d = 0; d < 2; ++d) {
       asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&dfull[d])), "r"(1));
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&dempty[d])), "r"(4));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&dempty[d])), "r"(dtc_epi_warps<kX>()));
     }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     abort_flag = 0;
@@ -1399,8 +1404,11 @@ __global__ void __launch_bounds__(kDtcThreads, 1)
       if (abort_flag && last_bar) mbar_wait(last_bar, static_cast<uint32_t>(last_parity & 1));
     }
   } else {
-    // epilogue: warp w reads TMEM lanes 32*(w%4).. = rows of the block
+    // epilogue: warp w reads TMEM lanes 32*(w%4).. = rows of the block; the
+    // epilogue warps of one lane quarter take every EQ-th 16-column group
+    constexpr int EQ = dtc_epi_warps<kX>() / 4;
     const int quarter = warp & 3;
+    const int eslot = (warp - (kDtcLoaderWarp + 1)) / 4;
     const int r = 32 * quarter + lane;
     int i = 0;
     for (int w = blockIdx.x; w < items; w += gridDim.x, ++i) {
@@ -1415,7 +1423,7 @@ __global__ void __launch_bounds__(kDtcThreads, 1)
         const int64_t plane = w / xblocks;
         const int x = (w % xblocks) * 128 + r;
         float2 *Yp = a.Y + plane * a.nky * ex;
-        for (int c0 = 0; c0 < N; c0 += 16) {
+        for (int c0 = 16 * eslot; c0 < N; c0 += 16 * EQ) {
           uint32_t v[16];
           asm volatile(
               "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
@@ -1455,7 +1463,7 @@ __global__ void __launch_bounds__(kDtcThreads, 1)
         const int jw = ja < 0 ? ja + a.nn[1] : ja;
         const float mzy = a.mody[jw] * a.modz[kz];
         float *ib = a.ibox + ((static_cast<int64_t>(f) * a.nkz + kz) * a.nky + ky) * a.nkx;
-        for (int c0 = 0; c0 < N; c0 += 16) {
+        for (int c0 = 16 * eslot; c0 < N; c0 += 16 * EQ) {
           uint32_t v[16];
           asm volatile(
               "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
@@ -2824,13 +2832,15 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
     }
     if (e == cudaSuccess && pl->use_ytc) {
       int per = 0;
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_dft_tc<false>, kDtcThreads, pl->smem_ydft_tc);
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_dft_tc<false>, dtc_threads<false>(),
+                                                        pl->smem_ydft_tc);
       per = std::min(std::max(1, per), 512 / pl->yshape.cols);
       pl->ytc_ctas = per * std::max(1, sms);
     }
     if (e == cudaSuccess && pl->use_xtc) {
       int per = 0;
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_dft_tc<true>, kDtcThreads, pl->smem_xdft_tc);
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_dft_tc<true>, dtc_threads<true>(),
+                                                        pl->smem_xdft_tc);
       per = std::min(std::max(1, per), 512 / pl->xshape.cols);
       pl->xtc_ctas = per * std::max(1, sms);
     }
@@ -2935,7 +2945,7 @@ int launch_ydft(const SaxsPlan *pl, const DevArgs &a, int planes, cudaStream_t s
     const cuuint32_t box[3] = {2 * kDtcChunk, 128, 1};
     CUtensorMap map;
     if (int rc = encode_map(&map, a.Z, 3, dims, strides, box)) return rc;
-    k_dft_tc<false><<<std::max(1, std::min(items, pl->ytc_ctas)), kDtcThreads, pl->smem_ydft_tc, st>>>(
+    k_dft_tc<false><<<std::max(1, std::min(items, pl->ytc_ctas)), dtc_threads<false>(), pl->smem_ydft_tc, st>>>(
         a, pl->yshape, map, items);
     return launch_check("k_dft_tc<y>");
   }
@@ -2959,7 +2969,7 @@ int launch_xdft(const SaxsPlan *pl, const DevArgs &a, int nframes, cudaStream_t 
     const cuuint32_t box[5] = {2 * kDtcChunk, static_cast<cuuint32_t>(a.xtcTP), static_cast<cuuint32_t>(kyb), 1, 1};
     CUtensorMap map;
     if (int rc = encode_map(&map, a.Y, 5, dims, strides, box)) return rc;
-    k_dft_tc<true><<<std::max(1, std::min(items, pl->xtc_ctas)), kDtcThreads, pl->smem_xdft_tc, st>>>(
+    k_dft_tc<true><<<std::max(1, std::min(items, pl->xtc_ctas)), dtc_threads<true>(), pl->smem_xdft_tc, st>>>(
         a, pl->xshape, map, items);
     return launch_check("k_dft_tc<x>");
   }
