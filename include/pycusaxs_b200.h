@@ -182,6 +182,26 @@ int saxs_profile_enable(SaxsPlan *plan, int enable);
  * launches_out (may be NULL).  Clears the pending records. */
 int saxs_profile_read(SaxsPlan *plan, double *ms_out, int *launches_out);
 
+/* ---- trajectory readers without MDAnalysis ----
+ * The reference reads every frame through MDAnalysis (pycusaxs/topology.py:52-75
+ * Universe(tpr, xtc), 536-577 read_frame/get_box, 621-737 iter_frames_stream),
+ * converting GROMACS nanometres to Angstrom.  These read GROMACS TRR and
+ * CHARMM/NAMD DCD files natively into caller buffers: positions (natoms x 3,
+ * Angstrom) and the box as three row vectors (Angstrom; zeros when the file has
+ * no box).  Errors go to saxs_last_error(). */
+#define SAXS_TRAJ_AUTO 0 /* by file extension (.trr / .dcd) */
+#define SAXS_TRAJ_TRR 1
+#define SAXS_TRAJ_DCD 2
+typedef struct SaxsTraj SaxsTraj;
+
+/* Open and index a trajectory (frame byte offsets, atom count). */
+int saxs_traj_open(const char *path, int format, SaxsTraj **out);
+int saxs_traj_info(const SaxsTraj *traj, int *natoms, long long *nframes);
+/* Frame `frame` (0-based) into xyz[3*natoms], box[9]; time_ps may be NULL.
+ * Reads use pread: concurrent calls on one handle (other frames) are safe. */
+int saxs_traj_read(SaxsTraj *traj, long long frame, float *xyz, float *box, double *time_ps);
+void saxs_traj_close(SaxsTraj *traj);
+
 /* ---- setup numerics, exposed so that tests can pin them against the reference ---- */
 
 /* Nearest 2^a 3^b 5^c 7^d to round(n*sigma), ties to the smaller

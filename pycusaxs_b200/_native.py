@@ -27,6 +27,7 @@ EXPORTED = (
     "saxs_reset", "saxs_debug_kbox_intensity", "saxs_debug_border_sums", "saxs_backward",
     "saxs_graph_create", "saxs_graph_launch", "saxs_graph_destroy",
     "saxs_forward_noalloc", "saxs_profile_stages", "saxs_profile_stage_name", "saxs_profile_enable", "saxs_profile_read",
+    "saxs_traj_open", "saxs_traj_info", "saxs_traj_read", "saxs_traj_close",
     "saxs_closest_product", "saxs_cell_oc", "saxs_histogram_parameters", "saxs_bspline_moduli",
     "saxs_last_error", "saxs_version",
 )
@@ -132,6 +133,14 @@ def load(path: os.PathLike | str | None = None) -> ctypes.CDLL:
     lib.saxs_profile_enable.restype = ctypes.c_int
     lib.saxs_profile_read.argtypes = [vp, c_double_p, c_int_p]
     lib.saxs_profile_read.restype = ctypes.c_int
+    lib.saxs_traj_open.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(vp)]
+    lib.saxs_traj_open.restype = ctypes.c_int
+    lib.saxs_traj_info.argtypes = [vp, c_int_p, ctypes.POINTER(ctypes.c_longlong)]
+    lib.saxs_traj_info.restype = ctypes.c_int
+    lib.saxs_traj_read.argtypes = [vp, ctypes.c_longlong, c_float_p, c_float_p, c_double_p]
+    lib.saxs_traj_read.restype = ctypes.c_int
+    lib.saxs_traj_close.argtypes = [vp]
+    lib.saxs_traj_close.restype = None
     lib.saxs_closest_product.argtypes = [ctypes.c_int, ctypes.c_float]
     lib.saxs_closest_product.restype = ctypes.c_int64
     lib.saxs_cell_oc.argtypes = [c_float_p, c_float_p]

@@ -18,7 +18,7 @@ LIBDIR = PKG / "lib"
 LIBNAME = "libpycusaxs_b200.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-SOURCES = ["setup.cpp", "plan.cu", "noalloc.cu"]
+SOURCES = ["setup.cpp", "plan.cu", "noalloc.cu", "trajectory.cpp"]
 
 
 def nvcc() -> str:

@@ -83,12 +83,27 @@ def invoke_cuda_backend(required_params: Dict[str, Any], advanced_params: Dict[s
     return [result.get("summary", "cuda backend returned no summary")]
 
 
+# topology / trajectory formats read without MDAnalysis (pycusaxs_b200.trajectory)
+NATIVE_TOPOLOGY = (".gro", ".pdb")
+NATIVE_TRAJECTORY = (".trr", ".dcd", ".gro")
+
+
 def _default_topology_factory(topology_path: str, trajectory_path: str):
+    """GRO/PDB topology with a TRR/DCD/GRO trajectory: the native readers; anything
+    else (TPR, XTC, ...): the reference's MDAnalysis-backed Topology."""
+    if (Path(topology_path).suffix.lower() in NATIVE_TOPOLOGY
+            and Path(trajectory_path).suffix.lower() in NATIVE_TRAJECTORY):
+        from .trajectory import FileTopology
+
+        return FileTopology(topology_path, trajectory_path)
     try:
         from pycusaxs.topology import Topology  # the reference's MDAnalysis-backed loader
     except ImportError as exc:
         raise ImportError("an MDAnalysis-backed Topology (pycusaxs.topology) is required to read "
-                          f"topology/trajectory files: {exc}") from exc
+                          f"{Path(topology_path).suffix or 'these'} topology / "
+                          f"{Path(trajectory_path).suffix or 'these'} trajectory files "
+                          f"(read natively: topology {', '.join(NATIVE_TOPOLOGY)}; trajectory "
+                          f"{', '.join(NATIVE_TRAJECTORY)}): {exc}") from exc
     return Topology(topology_path, trajectory_path)
 
 
@@ -97,7 +112,8 @@ def run_saxs_calculation(required_params: Dict[str, Any], advanced_params: Dict[
     """core.py:134-211: validate paths and frames, load the topology, run the backend.
 
     ``topology_factory(topology_path, trajectory_path)`` builds the topology
-    object (default: the reference's MDAnalysis ``Topology``).
+    object (default: the native readers for GRO/PDB topologies with TRR, DCD or
+    GRO trajectories, else the reference's MDAnalysis ``Topology``).
     """
     try:
         topology_path = Path(required_params["topology"]).expanduser().resolve()

@@ -227,6 +227,35 @@ class SaxsEngine:
         return self._staging
 
     # -- results ----------------------------------------------------------
+    def run_trajectory(self, traj, begin: int = 0, end: int | None = None, stride: int = 1,
+                       batch: int | None = None) -> int:
+        """Frames begin, begin+stride, ... < end of `traj` (a reader from
+        pycusaxs_b200.trajectory: n_frames, n_atoms, read(k, out)) through the plan.
+
+        A reader thread fills two pinned host batches of up to `batch` frames
+        (default max_frames) while the previous batch is copied to the device and
+        processed; returns the number of frames processed.
+        """
+        from .trajectory import BatchStream
+
+        torch = self._torch
+        end = traj.n_frames if end is None else min(int(end), traj.n_frames)
+        frames = range(max(0, int(begin)), end, max(1, int(stride)))
+        B = self.max_frames if batch is None else max(1, min(int(batch), self.max_frames))
+        bufs = [torch.empty((B, traj.n_atoms, 3), dtype=torch.float32).pin_memory() for _ in range(2)]
+        stream = BatchStream(traj, frames, B, bufs)
+        done = 0
+        try:
+            for slot, buf, boxes, n in stream:
+                self.forward_host(buf[:n], boxes)
+                ev = torch.cuda.Event()
+                ev.record(self._copy_stream)  # the batch's copies are queued before this
+                stream.release(slot, ev)
+                done += n
+        finally:
+            stream.close()
+        return done
+
     def histogram(self):
         """FP64 (hist, nhist) accumulated so far (waits for the device)."""
         nb = self.info.num_bins
