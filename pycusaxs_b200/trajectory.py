@@ -95,10 +95,11 @@ def _gro_frames(path):
             if not n_line.strip():
                 return
             n = int(n_line)
-            names, resnames = [], []
+            names, resnames, resids = [], [], []
             pos = np.empty((n, 3), dtype=np.float32)
             for i in range(n):
                 ln = fh.readline()
+                resids.append(int(ln[0:5]))
                 resnames.append(ln[5:10].strip())
                 names.append(ln[10:15].strip())
                 pos[i] = (float(ln[20:28]) * NM, float(ln[28:36]) * NM, float(ln[36:44]) * NM)
@@ -109,13 +110,14 @@ def _gro_frames(path):
                     t = float(title.split("t=")[1].split()[0])
                 except (ValueError, IndexError):
                     t = 0.0
-            yield names, resnames, pos, box, t
+            yield names, resnames, pos, box, t, resids
 
 
 def read_gro(path) -> dict:
-    """First frame of a GRO file: names, resnames, elements, positions (A), box rows (A)."""
-    names, resnames, pos, box, _ = next(_gro_frames(path))
-    return {"names": names, "resnames": resnames,
+    """First frame of a GRO file: names, resnames, residue numbers, elements,
+    positions (A), box rows (A)."""
+    names, resnames, pos, box, _, resids = next(_gro_frames(path))
+    return {"names": names, "resnames": resnames, "resids": resids,
             "elements": [guess_element(a, r) for a, r in zip(names, resnames)],
             "positions": pos, "box": box}
 
@@ -147,7 +149,7 @@ class GroTrajectory:
 def read_pdb(path) -> dict:
     """ATOM/HETATM records of the first model: names, resnames, elements (columns 77-78,
     else guessed from the name), positions (A), box from CRYST1 (A, degrees)."""
-    names, resnames, elements, pos = [], [], [], []
+    names, resnames, elements, pos, resids = [], [], [], [], []
     box = np.zeros((3, 3), dtype=np.float32)
     with open(path) as fh:
         for ln in fh:
@@ -161,11 +163,12 @@ def read_pdb(path) -> dict:
                 el = ln[76:78].strip() if len(ln) >= 78 else ""
                 names.append(name)
                 resnames.append(res)
+                resids.append(int(ln[22:26]))
                 elements.append(el[0].upper() + el[1:].lower() if el else guess_element(name, res))
                 pos.append((float(ln[30:38]), float(ln[38:46]), float(ln[46:54])))
             elif rec == "ENDMDL":
                 break
-    return {"names": names, "resnames": resnames, "elements": elements,
+    return {"names": names, "resnames": resnames, "resids": resids, "elements": elements,
             "positions": np.asarray(pos, dtype=np.float32).reshape(-1, 3), "box": box}
 
 
@@ -260,6 +263,14 @@ def read_topology(path) -> dict:
 
 # -- the reference's topology contract --------------------------------------------
 
+# standard atomic masses (g/mol) for the densities of stored profiles
+_MASS = {"H": 1.008, "C": 12.011, "N": 14.007, "O": 15.999, "P": 30.974, "S": 32.06, "Na": 22.990,
+         "Cl": 35.45, "K": 39.098, "Ca": 40.078, "Mg": 24.305, "Zn": 65.38, "Fe": 55.845,
+         "F": 18.998, "Br": 79.904, "I": 126.904, "Li": 6.94, "Cu": 63.546, "Mn": 54.938, "Se": 78.971}
+_WATER_RES = {"SOL", "HOH", "WAT", "TIP3", "TIP4", "TIP5", "SPC", "H2O", "T3P", "T4P"}
+_ION_RES = {"NA": "Na", "NA+": "Na", "SOD": "Na", "CL": "Cl", "CL-": "Cl", "CLA": "Cl", "K": "K",
+            "K+": "K", "POT": "K", "CA": "Ca", "CAL": "Ca", "MG": "Mg", "MG2": "Mg"}
+
 
 class FileTopology:
     """Topology + trajectory from files, with the callback contract the drop-in
@@ -269,6 +280,8 @@ class FileTopology:
     def __init__(self, topology, trajectory=None, box=None, prefetch: int = 4):
         top = read_topology(topology)
         self.elements = top["elements"]
+        self.resnames = top["resnames"]
+        self.resids = top["resids"]
         self.traj = open_trajectory(trajectory if trajectory is not None else topology,
                                     box=box if box is not None else top["box"])
         if self.traj.n_atoms != len(self.elements):
@@ -283,6 +296,39 @@ class FileTopology:
     @property
     def n_atoms(self) -> int:
         return self.traj.n_atoms
+
+    def get_system_info(self) -> dict:
+        """System description for the profile store (the keys the reference's
+        Topology.get_system_info provides, topology.py:288-450): atom count, box
+        edge lengths and volume of the first frame (A, A^3), waters (by residue
+        name, counted by their oxygens), ions by residue, other residues, density
+        (g/cm^3) and the time between frames (ps)."""
+        pos, box, t0 = self.traj.read(0)
+        lengths = np.linalg.norm(np.asarray(box, np.float64), axis=1)
+        volume = abs(float(np.linalg.det(np.asarray(box, np.float64))))
+        n_water, ions, other, water_atoms = 0, {}, {}, []
+        seen = set()
+        for i, (res, el, rid) in enumerate(zip(self.resnames, self.elements, self.resids)):
+            r = res.upper()
+            if r in _WATER_RES:
+                if el == "O":
+                    n_water += 1
+                water_atoms.append(i)
+            elif r in _ION_RES:
+                ions[_ION_RES[r]] = ions.get(_ION_RES[r], 0) + 1
+            elif (rid, res) not in seen:  # one count per residue
+                seen.add((rid, res))
+                other[res] = other.get(res, 0) + 1
+        per_water = len(water_atoms) / n_water if n_water else 0
+        model = {3: "TIP3P/SPC", 4: "TIP4P", 5: "TIP5P"}.get(int(round(per_water)), "") if n_water else ""
+        mass = sum(_MASS.get(e, 0.0) for e in self.elements)
+        dt = 0.0
+        if self.n_frames > 1:
+            dt = float(self.traj.read(1)[2] - t0)
+        return {"n_atoms": self.n_atoms, "box_x": float(lengths[0]), "box_y": float(lengths[1]),
+                "box_z": float(lengths[2]), "box_volume": volume, "n_water_molecules": n_water,
+                "ion_counts": ions, "other_molecules": other, "detected_water_model": model,
+                "density_g_cm3": mass / (volume * 0.602214076) if volume > 0 else None, "dt": dt}
 
     def get_atom_index(self) -> dict:
         out: dict[str, list[int]] = {}
