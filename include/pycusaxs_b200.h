@@ -59,7 +59,20 @@ typedef struct SaxsParams {
   float box0[9];        /* first-frame box: fixes Delta-q, q-cut and the k-box     */
   int max_frames;       /* frames per saxs_forward call (batch capacity)           */
   float box_margin;     /* relative box shrink the k-box tolerates (e.g. 0.05)     */
+  /* Opt-in physics extensions (no counterpart in the reference's output; 0 keeps
+   * the reference's behaviour):                                                  */
+  int box_mode;         /* SAXS_BOX_PARITY: oc from the box's upper triangle       */
+                        /* (Cell.cpp:111-126); SAXS_BOX_TRICLINIC: full H^-T, and   */
+                        /* q from its transpose                                    */
+  int padding_mode;     /* SAXS_PAD_AVERAGE: z-border mean per type per frame      */
+                        /* (saxsKernel.cu:150-162); SAXS_PAD_GIVEN: padding_values  */
+  const float *padding_values; /* [ntypes] atoms per grid point (given mode)      */
 } SaxsParams;
+
+#define SAXS_BOX_PARITY 0
+#define SAXS_BOX_TRICLINIC 1
+#define SAXS_PAD_AVERAGE 0
+#define SAXS_PAD_GIVEN 1
 
 /* Sizes derived at plan creation. */
 typedef struct SaxsPlanInfo {

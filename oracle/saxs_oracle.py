@@ -142,9 +142,13 @@ def find_closest_product(n: int, sigma: float) -> int:
     return closest
 
 
-def cell_matrices(box) -> tuple[np.ndarray, np.ndarray]:
-    """co (the box rows) and oc from the upper triangle only (Cell.cpp:111-126)."""
+def cell_matrices(box, box_mode: int = 0) -> tuple[np.ndarray, np.ndarray]:
+    """co (the box rows) and oc from the upper triangle only (Cell.cpp:111-126);
+    with box_mode 1 (the opt-in triclinic extension, no reference counterpart)
+    oc is the full inverse-transpose H^-T computed in double."""
     co = np.asarray(box, dtype=np.float32).reshape(3, 3)
+    if box_mode == 1:
+        return co, np.linalg.inv(co.astype(np.float64)).T.astype(np.float32)
     f = np.float32
     oc = np.zeros((3, 3), dtype=np.float32)
     oc[0, 0] = f(1.0 / float(co[0, 0]))
@@ -378,6 +382,8 @@ class OraclePlan:
     qcut: float = 0.0
     ensemble: str = "npt"
     contraction: int = DEFAULT_CONTRACTION
+    box_mode: int = 0                # 1: triclinic extension (oc = H^-T, q from its transpose)
+    padding: np.ndarray | None = None  # given padding per type (atoms per grid point)
     nn: tuple[int, int, int] = field(init=False)
     dq: np.float32 = field(init=False)
     kcut: np.float32 = field(init=False)
@@ -389,7 +395,7 @@ class OraclePlan:
             self.nn = tuple(int(v) for v in self.scaled_grid)
         else:
             self.nn = tuple(find_closest_product(int(n), self.sigma) for n in self.grid)
-        _, oc0 = cell_matrices(self.box0)
+        _, oc0 = cell_matrices(self.box0, self.box_mode)
         self.dq, self.kcut, self.num_bins = histogram_parameters(self.nn, oc0, self.sigma,
                                                                  self.bin_size, self.qcut)
         ndim = max(self.nn)
@@ -397,9 +403,11 @@ class OraclePlan:
         self.oc0 = oc0
 
     def scaled_oc(self, oc) -> np.ndarray:
-        """sigma' * oc with sigma' = nx/nnx in float (saxsKernel.cu:71-79)."""
+        """sigma' * oc with sigma' = nx/nnx in float (saxsKernel.cu:71-79), as the
+        map from k indices to q / 2 pi (rows); transposed in the triclinic mode."""
         s = np.float32(self.grid[0]) / np.float32(self.nn[0])
-        return (s * np.asarray(oc, dtype=np.float32)).astype(np.float32)
+        m = (s * np.asarray(oc, dtype=np.float32)).astype(np.float32)
+        return np.ascontiguousarray(m.T) if self.box_mode == 1 else m
 
 
 def frame_intensity(plan: OraclePlan, xyz, type_of_atom, box, *, return_parts=False):
@@ -407,7 +415,7 @@ def frame_intensity(plan: OraclePlan, xyz, type_of_atom, box, *, return_parts=Fa
 
     ``type_of_atom[a]`` is the index into ``plan.types`` of atom a (or -1 to skip).
     """
-    _, oc = cell_matrices(box)
+    _, oc = cell_matrices(box, plan.box_mode)
     ocs = plan.scaled_oc(oc)
     nn = plan.nn
     mw, bins = kpoint_bins(nn, ocs, plan.dq, plan.kcut, plan.num_bins, plan.contraction)
@@ -418,7 +426,7 @@ def frame_intensity(plan: OraclePlan, xyz, type_of_atom, box, *, return_parts=Fa
     for t, _name in enumerate(plan.types):
         sel = np.nonzero(np.asarray(type_of_atom) == t)[0]
         g = spread(r[sel], plan.grid, plan.order)
-        mean = border_mean(g)
+        mean = border_mean(g) if plan.padding is None else float(plan.padding[t])
         means.append(mean)
         sup = supercell(g, mean, nn)
         ft = np.fft.rfftn(sup)

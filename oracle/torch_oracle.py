@@ -27,7 +27,7 @@ def cubic_weights(u):
 
 def profile(plan: O.OraclePlan, xyz: torch.Tensor, type_of_atom, box):
     """(num_bins,) FP64 profile hist/nhist (0 where nhist == 0 and in bin 0) for one frame."""
-    co, oc = O.cell_matrices(box)
+    co, oc = O.cell_matrices(box, plan.box_mode)
     ocs = plan.scaled_oc(oc)
     nn = plan.nn
     n = plan.grid
@@ -63,7 +63,8 @@ def profile(plan: O.OraclePlan, xyz: torch.Tensor, type_of_atom, box):
                         val.append(w[0][o, sel] * w[1][p, sel] * w[2][q, sel])
             g = g.index_add(0, torch.cat(idx), torch.cat(val))
         g = g.reshape(n[0], n[1], n[2])
-        mean = g[:, :, border].sum() / (n[0] * n[1] * int(border.sum()))
+        mean = (g[:, :, border].sum() / (n[0] * n[1] * int(border.sum())) if plan.padding is None
+                else torch.tensor(float(plan.padding[t]), dtype=torch.float64))
         ex = [min(n[d], nn[d]) for d in range(3)]
         sup = mean * torch.ones(nn, dtype=torch.float64)
         sup = sup.clone()

@@ -56,6 +56,9 @@ class SaxsParams(ctypes.Structure):
         ("box0", ctypes.c_float * 9),
         ("max_frames", ctypes.c_int),
         ("box_margin", ctypes.c_float),
+        ("box_mode", ctypes.c_int),
+        ("padding_mode", ctypes.c_int),
+        ("padding_values", c_float_p),
     ]
 
 

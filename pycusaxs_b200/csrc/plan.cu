@@ -115,6 +115,7 @@ struct DevArgs {
   int *offsets;
   float4 *rec;
   double *border;
+  const float *pad_val;  // [T] given padding densities (atoms per grid point); null: z-border mean
   float2 *Z;
   float2 *Y;
   float *ibox;
@@ -174,6 +175,13 @@ __device__ __forceinline__ double warp_sum(double v) {
 }
 
 __device__ __forceinline__ int signed_k(int k, int nn, int nf) { return k < nf ? k : k - nn; }
+
+// Padding density of type t in frame f: the plan's given value, or the mean of
+// the type's z-border planes (saxsKernel.cu:150-162).
+__device__ __forceinline__ float padding_mean(const DevArgs &a, int f, int t) {
+  return a.pad_val ? a.pad_val[t]
+                   : static_cast<float>(a.border[static_cast<int64_t>(f) * a.T + t] / a.border_count);
+}
 
 // ---------------------------------------------------------------------------
 // kernels
@@ -426,8 +434,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_spread_zdft(DevArgs a, int item
     // mean padding: the supercell is g on the corner block and the border mean
     // elsewhere = (g - mean) on the corner + a constant whose transform is k = 0
     // only.  The column DFT of -mean over z < ez is -mean * sum_z tw[z][n].
-    const float mean =
-        static_cast<float>(a.border[static_cast<int64_t>(f) * a.T + t] / a.border_count);
+    const float mean = padding_mean(a, f, t);
     float2 *Zft = a.Z + (static_cast<int64_t>(f) * a.T + t) * a.nkz * zplane;
     for (int rd = 0; rd < rounds; ++rd) {
       const int task = rounds > 1 ? rd * blockDim.x + tid : tid % tps;
@@ -997,7 +1004,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_spread_zdft_tc(DevArgs a, int
       bool valid;
       // the range and mean loads are issued before the wait for the slot
       home_ranges_load(a, home_x, home_y, it.f, it.t, x0, y0, s0, cnt, valid);
-      const double bsum = a.border[static_cast<int64_t>(it.f) * a.T + it.t];
+      const float pmean = a.pad_val ? a.pad_val[it.t] : 0.0f;
+      const double bsum = a.pad_val ? 0.0 : a.border[static_cast<int64_t>(it.f) * a.T + it.t];
       if (j >= 2) wait(&rec_empty[b], (j - 2) >> 1);
       if (__any_sync(0xffffffffu, abort_flag != 0)) break;
       TcSlot &sl = slot[b];
@@ -1009,7 +1017,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_spread_zdft_tc(DevArgs a, int
         sl.y0 = y0;
         sl.cw = min(kTile, a.ext[0] - x0);
         sl.ch = min(kTile, a.ext[1] - y0);
-        sl.mean = static_cast<float>(bsum / a.border_count);
+        sl.mean = a.pad_val ? pmean : static_cast<float>(bsum / a.border_count);
       }
       __syncwarp();
       if (lane == 0) {
@@ -1454,9 +1462,7 @@ __global__ void __launch_bounds__(dtc_threads<kX>(), 1)
         for (int q = 0; q < 9; ++q) ocs[q] = a.geom[f * kGeom + 9 + q];
         const int ka = signed_k(kz, a.nn[2], a.nf[2]);
         const int ja = a.ky_lo + min(ky, a.nky - 1);
-        const float mean = row_ok ? static_cast<float>(a.border[static_cast<int64_t>(f) * a.T + t] /
-                                                       a.border_count)
-                                  : 0.0f;
+        const float mean = row_ok ? padding_mean(a, f, t) : 0.0f;
         float ff[9];
 #pragma unroll
         for (int q = 0; q < 9; ++q) ff[q] = a.ff[9 * (t < a.T ? t : 0) + q];
@@ -1529,7 +1535,7 @@ __global__ void __launch_bounds__(kThreads) k_xdft_post(DevArgs a, int xc) {
   const int tid = threadIdx.x;
   if (tid < 9) ocs[tid] = a.geom[f * kGeom + 9 + tid];
   for (int t = tid; t < a.T && t < 64; t += blockDim.x)
-    means[t] = static_cast<float>(a.border[static_cast<int64_t>(f) * a.T + t] / a.border_count);
+    means[t] = padding_mean(a, f, t);
   const bool one_chunk = xc >= ex;
   if (one_chunk) {
     const float4 *src = reinterpret_cast<const float4 *>(a.twx);
@@ -1705,7 +1711,7 @@ __global__ void __launch_bounds__(kThreads) k_xdft_grad(DevArgs a, AdjArgs j, in
   const int tid = threadIdx.x;
   if (tid < 9) ocs[tid] = a.geom[9 + tid];
   for (int t = tid; t < a.T && t < 64; t += blockDim.x)
-    means[t] = static_cast<float>(a.border[t] / a.border_count);
+    means[t] = padding_mean(a, 0, t);
   const int ka = signed_k(kz, a.nn[2], a.nf[2]);
   const int npairs = a.T * a.nkx;
   const int kx_hi = a.kx_lo + a.nkx - 1, ky_hi = a.ky_lo + a.nky - 1;
@@ -1983,7 +1989,9 @@ __global__ void __launch_bounds__(kThreads) k_gather(DevArgs a, AdjArgs j) {
     }
   }
   // the border mean: every border voxel carries (nn^3 Re G(0) - S_t) / count
-  const float cm = static_cast<float>((static_cast<double>(j.dcg[t]) - j.S[t]) / a.border_count);
+  // (a given padding does not depend on the positions)
+  const float cm = a.pad_val ? 0.0f
+                             : static_cast<float>((static_cast<double>(j.dcg[t]) - j.S[t]) / a.border_count);
   float sx = 0.f, sy = 0.f, szb = 0.f, dsx = 0.f, dsy = 0.f, dszb = 0.f;
 #pragma unroll
   for (int o = 0; o < 4; ++o) {
@@ -2178,7 +2186,8 @@ __global__ void __launch_bounds__(kThreads) k_mean_grad(DevArgs a, AdjArgs j) {
   const float4 q = a.rec[i];
   const int e = __float_as_int(q.w);
   const int t = a.entry_type[e];
-  const float cm = static_cast<float>((static_cast<double>(j.dcg[t]) - j.S[t]) / a.border_count);
+  const float cm = a.pad_val ? 0.0f
+                             : static_cast<float>((static_cast<double>(j.dcg[t]) - j.S[t]) / a.border_count);
   if (cm == 0.0f) return;
   const int m[3] = {static_cast<int>(q.x), static_cast<int>(q.y), static_cast<int>(q.z)};
   float w[3][4], dw[3][4];
@@ -2241,6 +2250,7 @@ struct SaxsPlan {
   int device = 0;
   SaxsParams p{};
   std::vector<float> ff;
+  std::vector<float> pad;  // given padding densities per type (empty: z-border mean)
   DevArgs a{};
   int ensemble = SAXS_NPT;
   long long half[3] = {0, 0, 0};
@@ -2346,13 +2356,23 @@ bool home_tile_table(int ext, int n, int order, int bin_w, std::vector<int4> *ou
   return true;
 }
 
+// Per-frame geometry: g[0..9) = oc, the map from Cartesian to fractional
+// coordinates (rows); g[9..18) = the map from k indices to q / 2pi used by the
+// k-point code (rows).  Reference parity: oc from the box's upper triangle and
+// q rows = sigma' oc.  Triclinic mode: oc = H^-T and q = 2 pi (sigma' oc)^T m,
+// so the q rows are the transpose.
 void frame_geometry(const SaxsPlan *pl, const float box[9], float g[kGeom]) {
   float oc[9];
-  saxs::cell_oc(box, oc);
-  for (int i = 0; i < 9; ++i) {
-    g[i] = oc[i];
-    g[9 + i] = pl->sigma_scale * oc[i];
-  }
+  if (pl->p.box_mode == SAXS_BOX_TRICLINIC)
+    saxs::cell_oc_triclinic(box, oc);
+  else
+    saxs::cell_oc(box, oc);
+  const bool tr = pl->p.box_mode == SAXS_BOX_TRICLINIC;
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) {
+      g[3 * r + c] = oc[3 * r + c];
+      g[9 + 3 * r + c] = pl->sigma_scale * (tr ? oc[3 * c + r] : oc[3 * r + c]);
+    }
   for (int i = 18; i < kGeom; ++i) g[i] = 0.0f;
 }
 
@@ -2450,6 +2470,16 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
   if (p.ensemble != SAXS_NPT && p.ensemble != SAXS_NVT)
     return fail(SAXS_E_INVALID, "ensemble must be npt or nvt");
   if (int rc = check_box(p.box0)) return rc;
+  if (p.box_mode != SAXS_BOX_PARITY && p.box_mode != SAXS_BOX_TRICLINIC)
+    return fail(SAXS_E_INVALID, "box_mode must be parity (0) or triclinic (1)");
+  if (p.padding_mode != SAXS_PAD_AVERAGE && p.padding_mode != SAXS_PAD_GIVEN)
+    return fail(SAXS_E_INVALID, "padding_mode must be average (0) or given (1)");
+  if (p.padding_mode == SAXS_PAD_GIVEN) {
+    if (!p.padding_values) return fail(SAXS_E_INVALID, "given padding needs padding_values");
+    for (int t = 0; t < p.ntypes; ++t)
+      if (!std::isfinite(p.padding_values[t]) || p.padding_values[t] < 0.0f)
+        return fail(SAXS_E_INVALID, "padding values must be finite and non-negative");
+  }
   for (int i = 0; i < p.nentries; ++i) {
     if (p.entry_atom[i] < 0 || p.entry_atom[i] >= p.natoms)
       return fail(SAXS_E_INVALID, "atom index " + std::to_string(p.entry_atom[i]) +
@@ -2481,6 +2511,8 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
   SaxsPlan *pl = new SaxsPlan();
   cudaGetDevice(&pl->device);
   pl->p = p;
+  if (p.padding_mode == SAXS_PAD_GIVEN) pl->pad.assign(p.padding_values, p.padding_values + p.ntypes);
+  pl->p.padding_values = nullptr;  // the caller's array is not kept
   pl->ensemble = p.ensemble;
   pl->ff.assign(p.form_factors, p.form_factors + 9 * p.ntypes);
   DevArgs &a = pl->a;
@@ -2521,17 +2553,20 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
   }
   a.nn3 = static_cast<double>(nn[0]) * nn[1] * nn[2];
 
-  float oc0[9];
-  saxs::cell_oc(p.box0, oc0);
+  pl->sigma_scale = static_cast<float>(a.n[0]) / static_cast<float>(nn[0]);
+  float geo0[kGeom];
+  frame_geometry(pl, p.box0, geo0);
+  float oc0[9], ocs0[9];
+  for (int i = 0; i < 9; ++i) {
+    oc0[i] = geo0[i];
+    ocs0[i] = geo0[9 + i];
+  }
   saxs::histogram_parameters(nn, oc0, p.scale_factor, p.bin_size, p.qcut, &a.dq, &a.qcut,
                              &a.num_bins);
   if (a.num_bins < 1) a.num_bins = 1;
-  pl->sigma_scale = static_cast<float>(a.n[0]) / static_cast<float>(nn[0]);
 
   // k-box: every integer k with |2 pi ocs k| <= qcut for the first frame and
   // for boxes up to `box_margin` smaller.
-  float ocs0[9];
-  for (int i = 0; i < 9; ++i) ocs0[i] = pl->sigma_scale * oc0[i];
   const double margin = std::max(0.0f, p.box_margin) + 1e-5;
   saxs::kbox_halfwidths(ocs0, a.qcut, margin, pl->half);
   for (int d = 0; d < 2; ++d) {
@@ -2674,6 +2709,8 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
   ALLOC(d_mody, nn[1]);
   ALLOC(d_modz, nn[2]);
   ALLOC(d_ff, 9 * a.T);
+  float *d_pad = nullptr;
+  if (!pl->pad.empty()) ALLOC(d_pad, a.T);
   int4 *d_hx = nullptr, *d_hy = nullptr;
   float *d_twzs = nullptr, *d_twztc = nullptr, *d_twytc = nullptr, *d_twxtc = nullptr;
   ALLOC(d_twzs, 2 * a.nkzp);
@@ -2707,6 +2744,7 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
   a.mody = d_mody;
   a.modz = d_modz;
   a.ff = d_ff;
+  a.pad_val = d_pad;
   a.twz_sum = d_twzs;
   a.twz_tc = d_twztc;
   pl->yshape.B = d_twytc;
@@ -2786,6 +2824,7 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
       (rc = up(d_mody, my.data(), sizeof(float) * nn[1])) ||
       (rc = up(d_modz, mz.data(), sizeof(float) * nn[2])) ||
       (rc = up(d_ff, pl->ff.data(), sizeof(float) * pl->ff.size())) ||
+      (rc = up(d_pad, pl->pad.data(), sizeof(float) * pl->pad.size())) ||
       (rc = up(d_hx, hxt.data(), sizeof(int4) * hxt.size())) ||
       (rc = up(d_twzs, twzs.data(), sizeof(float) * twzs.size())) ||
       (rc = up(d_twztc, twtc.data(), sizeof(float) * twtc.size())) ||

@@ -59,6 +59,17 @@ void cell_oc(const float co[9], float oc[9]) {
   oc[8] = static_cast<float>(1.0 / co[8]);
 }
 
+void cell_oc_triclinic(const float co[9], float oc[9]) {
+  const double h[9] = {co[0], co[1], co[2], co[3], co[4], co[5], co[6], co[7], co[8]};
+  // cofactors of H; H^-1 = adj(H) / det, and oc = (H^-1)^T = cof(H) / det
+  const double c00 = h[4] * h[8] - h[5] * h[7], c01 = h[5] * h[6] - h[3] * h[8], c02 = h[3] * h[7] - h[4] * h[6];
+  const double c10 = h[2] * h[7] - h[1] * h[8], c11 = h[0] * h[8] - h[2] * h[6], c12 = h[1] * h[6] - h[0] * h[7];
+  const double c20 = h[1] * h[5] - h[2] * h[4], c21 = h[2] * h[3] - h[0] * h[5], c22 = h[0] * h[4] - h[1] * h[3];
+  const double det = h[0] * c00 + h[1] * c01 + h[2] * c02;
+  const double cof[9] = {c00, c01, c02, c10, c11, c12, c20, c21, c22};
+  for (int i = 0; i < 9; ++i) oc[i] = static_cast<float>(cof[i] / det);
+}
+
 int nf_of(int n) { return (n % 2 == 0) ? n / 2 : n / 2 + 1; }
 
 // saxsKernel::resetHistogramParameters (saxsKernel.cu:489-526) and num_bins

@@ -67,7 +67,13 @@ class SaxsEngine:
     def __init__(self, grid, atom_index: dict, natoms: int, box0, *, scaled_grid=(0, 0, 0),
                  order: int = 4, scale_factor: float = 1.0, bin_size: float = 0.0,
                  qcut: float = 0.0, ensemble: str = "npt", max_frames: int = 1,
-                 box_margin: float = 0.05, device=None, form_factors: dict | None = None):
+                 box_margin: float = 0.05, device=None, form_factors: dict | None = None,
+                 box_mode: str = "parity", padding: str = "average", padding_values=None):
+        """``box_mode``: "parity" (the reference's upper-triangle inverse) or
+        "triclinic" (full inverse of the box rows); ``padding``: "average" (the
+        z-border mean, as the reference) or "given" with ``padding_values``: a
+        mapping element -> atoms per grid point or an array in type order (see
+        pycusaxs_b200.solvent.given_padding)."""
         torch = _torch()
         self._torch = torch
         self.lib = _native.load()
@@ -105,6 +111,24 @@ class SaxsEngine:
         p.box0[:] = [float(v) for v in np.asarray(box0, dtype=np.float32).reshape(9)]
         p.max_frames = self.max_frames
         p.box_margin = float(box_margin)
+        if box_mode not in ("parity", "triclinic"):
+            raise ValueError(f"box_mode must be 'parity' or 'triclinic', not {box_mode!r}")
+        p.box_mode = 1 if box_mode == "triclinic" else 0
+        if padding not in ("average", "given"):
+            raise ValueError(f"padding must be 'average' or 'given', not {padding!r}")
+        self._pad = None
+        if padding == "given":
+            if padding_values is None:
+                raise ValueError("padding='given' needs padding_values")
+            if isinstance(padding_values, dict):
+                vals = [float(padding_values.get(t, 0.0)) for t in self.type_names]
+            else:
+                vals = list(np.asarray(padding_values, dtype=np.float32).reshape(-1))
+            if len(vals) != len(self.type_names):
+                raise ValueError("one padding value per element type is required")
+            self._pad = np.ascontiguousarray(vals, dtype=np.float32)
+            p.padding_mode = 1
+            p.padding_values = self._pad.ctypes.data_as(_native.c_float_p)
         self._params = p
         plan = ctypes.c_void_p()
         with torch.cuda.device(self.device):

@@ -138,11 +138,17 @@ def build_summary(topology, trajectory, grid, scaled, begin, end, stride, order,
 def run(obj_topology: Any, topology: str, trajectory: str, grid, scaled_grid=(), begin: int = 0,
         end: int = 0, stride: int = 1, output: str = "", order: int = 4, scale_factor: float = 1.0,
         bin_size: float = 0.0, qcut: float = 0.0, water_model: str = "", sodium: int = 0,
-        chlorine: int = 0, simulation: str = "") -> dict:
+        chlorine: int = 0, simulation: str = "", *, box_mode: str = "parity",
+        padding: str = "average") -> dict:
     """Compute the SAXS profile of frames begin..end (inclusive, every ``stride``) and write it.
 
     Same arguments and defaults as ``pycusaxs_cuda.run`` of the reference
     (cuda_bindings.cpp:172-196).  Returns {'summary', 'grid', 'scaled_grid'}.
+    Two keyword-only extensions, off by default (reference behaviour):
+    ``box_mode="triclinic"`` inverts the full box matrix instead of its upper
+    triangle, and ``padding="given"`` pads the supercell with bulk solvent of
+    ``water_model`` (SPC/E if empty) plus ``sodium`` / ``chlorine`` ions
+    (pycusaxs_b200.solvent.given_padding) instead of the z-border average.
     """
     grid_l = _int_list(grid, "grid")
     scaled_l = _int_list(scaled_grid or (), "scaled_grid")
@@ -169,7 +175,8 @@ def run(obj_topology: Any, topology: str, trajectory: str, grid, scaled_grid=(),
     result = {"summary": summary, "grid": list(norm_grid),
               "scaled_grid": list(norm_scaled) if norm_scaled else [0, 0, 0]}
     _run_frames(obj_topology, norm_grid, norm_scaled, begin, end, stride, order, scale_factor,
-                bin_size, qcut, ensemble, out_path)
+                bin_size, qcut, ensemble, out_path, box_mode=box_mode, padding=padding,
+                water_model=water_model, sodium=sodium, chlorine=chlorine)
     return result
 
 
@@ -184,7 +191,8 @@ def _call(fn, *args):
         raise _PythonCallbackError(f"{type(exc).__name__}: {exc}") from exc
 
 
-def _run_frames(topo, grid, scaled, begin, end, stride, order, sigma, dq, qcut, ensemble, out_path):
+def _run_frames(topo, grid, scaled, begin, end, stride, order, sigma, dq, qcut, ensemble, out_path,
+                box_mode="parity", padding="average", water_model="", sodium=0, chlorine=0):
     from .engine import SaxsEngine, format_profile
 
     t0 = time.perf_counter()
@@ -195,9 +203,22 @@ def _run_frames(topo, grid, scaled, begin, end, stride, order, sigma, dq, qcut, 
         box0 = np.asarray(_call(topo.get_box), dtype=np.float32).reshape(3, 3)
         natoms = 1 + max((max(v) for v in index.values() if len(v)), default=-1)
         try:
+            ext = {}
+            if box_mode != "parity":
+                ext["box_mode"] = box_mode
+            if padding == "given":
+                from .engine import entries_from_index
+                from .solvent import given_padding
+
+                names = entries_from_index(index, natoms)[0]
+                ext["padding"] = "given"
+                ext["padding_values"] = given_padding(names, box0, grid, water_model or "SPCE",
+                                                      {"Na": sodium, "Cl": chlorine})
+            elif padding != "average":
+                raise ValueError(f"padding must be 'average' or 'given', not {padding!r}")
             engine = SaxsEngine(grid, index, natoms, box0, scaled_grid=scaled or (0, 0, 0),
                                 order=order, scale_factor=sigma, bin_size=dq, qcut=qcut,
-                                ensemble=ensemble or "npt", max_frames=1)
+                                ensemble=ensemble or "npt", max_frames=1, **ext)
         except KeyError as exc:
             raise RuntimeError(f"CuSAXS error: {exc.args[0]}") from None
         except ValueError as exc:

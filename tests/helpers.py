@@ -10,20 +10,22 @@ RTOL_PROFILE = 1e-4
 
 
 def oracle_hist(system, grid, frames, *, scaled_grid=(0, 0, 0), order=4, sigma=2.0, bin_size=0.0,
-                qcut=0.5, ensemble="npt", boxes=None):
+                qcut=0.5, ensemble="npt", boxes=None, box_mode=0, padding=None):
     names = sorted({str(e) for e in system.elements}, key=lambda s: s.encode())
     ff = O.load_form_factors()
     box0 = system.box if boxes is None else boxes[0]
     plan = O.OraclePlan(grid=tuple(grid), types=names, coeffs=np.stack([ff[n] for n in names]),
                         box0=box0, scaled_grid=tuple(scaled_grid), order=order, sigma=sigma,
-                        bin_size=bin_size, qcut=qcut, ensemble=ensemble)
+                        bin_size=bin_size, qcut=qcut, ensemble=ensemble, box_mode=box_mode,
+                        padding=None if padding is None else np.asarray(padding, np.float64))
     fr = [(frames[k], system.box if boxes is None else boxes[k]) for k in range(len(frames))]
     h, n = O.run_frames(plan, fr, system.type_of_atom(names))
     return h, n, plan
 
 
 def engine_hist(system, grid, frames, *, scaled_grid=(0, 0, 0), order=4, sigma=2.0, bin_size=0.0,
-                qcut=0.5, ensemble="npt", boxes=None, max_frames=1, device_input=True):
+                qcut=0.5, ensemble="npt", boxes=None, max_frames=1, device_input=True, box_mode=0,
+                padding=None):
     import torch
 
     from pycusaxs_b200 import SaxsEngine
@@ -32,7 +34,9 @@ def engine_hist(system, grid, frames, *, scaled_grid=(0, 0, 0), order=4, sigma=2
     bx = np.stack([system.box] * len(frames)) if boxes is None else np.asarray(boxes)
     eng = SaxsEngine(grid, system.atom_index(), system.natoms, box0, scaled_grid=scaled_grid,
                      order=order, scale_factor=sigma, bin_size=bin_size, qcut=qcut,
-                     ensemble=ensemble, max_frames=max_frames)
+                     ensemble=ensemble, max_frames=max_frames,
+                     box_mode="triclinic" if box_mode else "parity",
+                     padding="average" if padding is None else "given", padding_values=padding)
     x = np.ascontiguousarray(np.stack(frames), dtype=np.float32)
     if device_input:
         eng.forward(torch.from_numpy(x).to(eng.device), bx)
