@@ -55,6 +55,7 @@ def parse():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-multi", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="keep the plan's default kernels")
     return ap.parse_args()
 
 
@@ -211,8 +212,16 @@ def bench_ours(args):
                      scale_factor=SCALE, bin_size=BIN, qcut=QCUT, max_frames=B)
     st = eng.stream
     x_dev = torch.from_numpy(frames).to(dev)
+    default_cfg = eng.config()
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
     hist_buf = torch.zeros(2 * eng.info.num_bins, dtype=torch.float64, device=dev)
+
+    # the plan's kernel configuration, tuned on this step's frames before any timing
+    tuned = None
+    if not args.no_tune:
+        t = eng.autotune(x_dev, boxes, repeats=3)
+        tuned = {"config": t["config"], "default": default_cfg,
+                 "candidates_ms": {k: round(v, 3) for k, v in t["ms"].items()}}
 
     def step_device():
         eng.forward(x_dev, boxes)
@@ -360,6 +369,7 @@ def bench_ours(args):
                    "kbox": [nkx, nky, nkz], "plain_path_frames_per_s": round(plain, 1) if plain else None,
                    "stage_share": stage_share,
                    "stage_kernels": {k: kernel_of.get(k, k) for k in stage_share},
+                   "kernel_config": eng.config(), "autotune": tuned,
                    "parallelism": f"frames sharded over {world} GPU(s)",
                    "adjoint": adj, "multi_system": multi},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": ck,

@@ -101,6 +101,25 @@ void saxs_plan_destroy(SaxsPlan *plan);
 
 int saxs_plan_info(const SaxsPlan *plan, SaxsPlanInfo *info);
 
+/* Kernel configuration of a plan, for tuning (no counterpart in the reference,
+ * which has one fixed kernel sequence).  The plan picks the tensor-core passes
+ * whose operands fit; an autotuner may time the alternatives on real frames and
+ * set the fastest.  Graphs built by saxs_graph_create keep the configuration
+ * they were captured with. */
+typedef struct SaxsPlanConfig {
+  int z_tensor_cores;     /* 1: spreading + z-axis DFT on tcgen05, 0: FP32 SIMT     */
+  int y_tensor_cores;     /* 1: y-axis DFT on tcgen05, 0: FP32 SIMT                  */
+  int x_tensor_cores;     /* 1: x-axis DFT + post on tcgen05, 0: FP32 SIMT           */
+  int z_producer_groups;  /* producer warp groups of the tensor-core spreading: 1|2 */
+  /* read by saxs_plan_config only: what the plan can run */
+  int z_tensor_cores_available, y_tensor_cores_available, x_tensor_cores_available;
+  int z_producer_groups_max;
+} SaxsPlanConfig;
+
+int saxs_plan_config(const SaxsPlan *plan, SaxsPlanConfig *cfg);
+/* Select a configuration among those saxs_plan_config reports as available. */
+int saxs_plan_set_config(SaxsPlan *plan, const SaxsPlanConfig *cfg);
+
 /* Process `nframes` frames (<= max_frames).  Frame f's positions are
  * xyz_dev[f*frame_stride .. +3*natoms) (float32, device memory); its box is
  * boxes_host[9*f .. +9] (host memory).  npt: the frames' histograms are added

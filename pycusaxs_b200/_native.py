@@ -23,7 +23,8 @@ SAXS_NVT = 1
 
 #: every symbol the header declares, in declaration order
 EXPORTED = (
-    "saxs_plan_create", "saxs_plan_destroy", "saxs_plan_info", "saxs_forward", "saxs_histogram",
+    "saxs_plan_create", "saxs_plan_destroy", "saxs_plan_info", "saxs_plan_config",
+    "saxs_plan_set_config", "saxs_forward", "saxs_histogram",
     "saxs_reset", "saxs_debug_kbox_intensity", "saxs_debug_border_sums", "saxs_backward",
     "saxs_graph_create", "saxs_graph_launch", "saxs_graph_destroy",
     "saxs_forward_noalloc", "saxs_profile_stages", "saxs_profile_stage_name", "saxs_profile_enable", "saxs_profile_read",
@@ -60,6 +61,13 @@ class SaxsParams(ctypes.Structure):
         ("padding_mode", ctypes.c_int),
         ("padding_values", c_float_p),
     ]
+
+
+class SaxsPlanConfig(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int) for n in (
+        "z_tensor_cores", "y_tensor_cores", "x_tensor_cores", "z_producer_groups",
+        "z_tensor_cores_available", "y_tensor_cores_available", "x_tensor_cores_available",
+        "z_producer_groups_max")]
 
 
 class SaxsPlanInfo(ctypes.Structure):
@@ -106,6 +114,10 @@ def load(path: os.PathLike | str | None = None) -> ctypes.CDLL:
     lib.saxs_plan_destroy.restype = None
     lib.saxs_plan_info.argtypes = [vp, ctypes.POINTER(SaxsPlanInfo)]
     lib.saxs_plan_info.restype = ctypes.c_int
+    lib.saxs_plan_config.argtypes = [vp, ctypes.POINTER(SaxsPlanConfig)]
+    lib.saxs_plan_config.restype = ctypes.c_int
+    lib.saxs_plan_set_config.argtypes = [vp, ctypes.POINTER(SaxsPlanConfig)]
+    lib.saxs_plan_set_config.restype = ctypes.c_int
     lib.saxs_forward.argtypes = [vp, vp, ctypes.c_int64, ctypes.c_int, c_float_p, vp]
     lib.saxs_forward.restype = ctypes.c_int
     lib.saxs_histogram.argtypes = [vp, c_double_p, c_double_p, vp]

@@ -89,6 +89,7 @@ struct DevArgs {
   int zc;  // z rows of twiddles k_spread_zdft holds in shared memory at once
   // tensor-core z-DFT (k_spread_zdft_tc): GEMM N, K, spread rows, stages, TMEM columns
   int tcN, tcK, tcR, tcS, tcCols, tcRB, tcCap;
+  int tcG;  // producer groups of k_spread_zdft_tc (1, or 2 with two operand stages)
   int xtcTP;  // tensor-core x-axis DFT: rows per ky (types padded to 8 or 16)
   int nf[3];
   int dz;
@@ -850,7 +851,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_spread_zdft_tc(DevArgs a, int
   int4 *home_x = reinterpret_cast<int4 *>(recs + 2 * RB);
   int4 *home_y = home_x + a.stiles[0];
   // producer groups: two when there are two operand stages
-  const int G = S == 2 ? 2 : 1;
+  const int G = (S == 2 && a.tcG == 2) ? 2 : 1;
   const int group = warp < kTcProducerWarps ? warp / (kTcProducerWarps / G) : 0;
   const int gthreads = kTcProducers / G, gtid = tid - group * gthreads;
   const int cap = a.tcCap;
@@ -2275,6 +2276,7 @@ struct SaxsPlan {
   bool use_tc = false;  // z-axis DFT on the tensor cores (k_spread_zdft_tc)
   size_t smem_spread_tc = 0;
   int tc_ctas = 1;
+  bool tc_ok = false, ytc_ok = false, xtc_ok = false;  // tensor-core kernels the plan can run
   bool use_ytc = false;  // y-axis DFT on the tensor cores (k_dft_tc<false>)
   bool use_xtc = false;  // x-axis DFT + post on the tensor cores (k_dft_tc<true>)
   DtcShape yshape{}, xshape{};
@@ -2647,6 +2649,7 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
       a.tcS = S;
       a.tcRB = RB;
       a.tcCap = CAP;
+      a.tcG = S == 2 ? 2 : 1;
       int cols = 32;
       while (cols < S * N) cols *= 2;
       a.tcCols = cols;
@@ -2669,6 +2672,9 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
       pl->use_xtc = dtc_shape(a.nkx, a.ext[0], optin - static_smem(k_dft_tc<true>), &pl->xshape,
                               &pl->smem_xdft_tc);
   }
+  pl->tc_ok = pl->use_tc;
+  pl->ytc_ok = pl->use_ytc;
+  pl->xtc_ok = pl->use_xtc;
   pl->smem_hist = a.num_bins <= kHistSmemBins ? 2 * sizeof(double) * a.num_bins : 0;
   pl->smem_bin = static_cast<size_t>(kThreads / 32) * a.T * sizeof(double);
   if (pl->smem_spread + static_smem(k_spread_zdft) > optin ||
@@ -3556,6 +3562,34 @@ int saxs_plan_info(const SaxsPlan *pl, SaxsPlanInfo *info) {
   info->path = (pl->use_tc ? 1 : 0) | (pl->use_ytc ? 2 : 0) | (pl->use_xtc ? 4 : 0);
   info->device_bytes = pl->bytes;
   info->frames_accumulated = pl->frames;
+  return SAXS_OK;
+}
+
+int saxs_plan_config(const SaxsPlan *pl, SaxsPlanConfig *cfg) {
+  if (!pl || !cfg) return fail(SAXS_E_INVALID, "null argument");
+  cfg->z_tensor_cores = pl->use_tc ? 1 : 0;
+  cfg->y_tensor_cores = pl->use_ytc ? 1 : 0;
+  cfg->x_tensor_cores = pl->use_xtc ? 1 : 0;
+  cfg->z_producer_groups = pl->use_tc ? pl->a.tcG : 1;
+  cfg->z_tensor_cores_available = pl->tc_ok ? 1 : 0;
+  cfg->y_tensor_cores_available = pl->ytc_ok ? 1 : 0;
+  cfg->x_tensor_cores_available = pl->xtc_ok ? 1 : 0;
+  cfg->z_producer_groups_max = (pl->tc_ok && pl->a.tcS == 2) ? 2 : 1;
+  return SAXS_OK;
+}
+
+int saxs_plan_set_config(SaxsPlan *pl, const SaxsPlanConfig *cfg) {
+  if (!pl || !cfg) return fail(SAXS_E_INVALID, "null argument");
+  if ((cfg->z_tensor_cores && !pl->tc_ok) || (cfg->y_tensor_cores && !pl->ytc_ok) ||
+      (cfg->x_tensor_cores && !pl->xtc_ok))
+    return fail(SAXS_E_INVALID, "a tensor-core pass the plan cannot run was requested");
+  const int gmax = (pl->tc_ok && pl->a.tcS == 2) ? 2 : 1;
+  if (cfg->z_producer_groups < 1 || cfg->z_producer_groups > gmax)
+    return fail(SAXS_E_INVALID, "z_producer_groups must be 1.." + std::to_string(gmax));
+  pl->use_tc = cfg->z_tensor_cores != 0;
+  pl->use_ytc = cfg->y_tensor_cores != 0;
+  pl->use_xtc = cfg->x_tensor_cores != 0;
+  pl->a.tcG = cfg->z_producer_groups;
   return SAXS_OK;
 }
 

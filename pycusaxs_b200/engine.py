@@ -11,6 +11,9 @@ PyTorch is used only as plumbing: device/pinned allocations and streams.
 from __future__ import annotations
 
 import ctypes
+import itertools
+import json
+import os
 from dataclasses import dataclass
 
 import numpy as np
@@ -39,7 +42,10 @@ class PlanInfo:
     kbox: tuple
     device_bytes: int
     frames: int
-    path: int = 0  # 1: z-axis DFT on the tensor cores (tcgen05), 0: FP32 SIMT
+    path: int = 0  # bits 1, 2, 4: the z-, y-, x-axis DFT on the tensor cores (tcgen05)
+
+
+CONFIG_KEYS = ("z_tensor_cores", "y_tensor_cores", "x_tensor_cores", "z_producer_groups")
 
 
 def entries_from_index(atom_index: dict, natoms: int | None = None):
@@ -150,6 +156,106 @@ class SaxsEngine:
     @property
     def frames(self) -> int:
         return self._info().frames
+
+    # -- kernel configuration ----------------------------------------------
+    def _config_struct(self):
+        c = _native.SaxsPlanConfig()
+        _native.check(self.lib.saxs_plan_config(self._plan, ctypes.byref(c)))
+        return c
+
+    def config(self) -> dict:
+        """The kernel configuration in use: tensor cores (1) or FP32 SIMT (0) for
+        the z, y and x passes, and the producer groups of the tensor-core
+        spreading."""
+        c = self._config_struct()
+        return {k: int(getattr(c, k)) for k in CONFIG_KEYS}
+
+    def config_candidates(self) -> list:
+        """Every configuration the plan can run (its resources cover them all)."""
+        c = self._config_struct()
+        zs = [0, 1] if c.z_tensor_cores_available else [0]
+        ys = [0, 1] if c.y_tensor_cores_available else [0]
+        xs = [0, 1] if c.x_tensor_cores_available else [0]
+        out = []
+        for z, y, x in itertools.product(zs, ys, xs):
+            for g in (range(1, c.z_producer_groups_max + 1) if z else (1,)):
+                out.append({"z_tensor_cores": z, "y_tensor_cores": y, "x_tensor_cores": x,
+                            "z_producer_groups": g})
+        return out
+
+    def set_config(self, cfg: dict) -> None:
+        """Select one of ``config_candidates()``; work already queued keeps the
+        configuration it was launched with."""
+        c = self._config_struct()
+        for k in CONFIG_KEYS:
+            if k in cfg:
+                setattr(c, k, int(cfg[k]))
+        _native.check(self.lib.saxs_plan_set_config(self._plan, ctypes.byref(c)))
+        self.info = self._info()
+
+    def tuning_key(self) -> str:
+        """What a tuned configuration depends on: the grids, k-box, atoms, element
+        types, frames per launch and the device."""
+        torch = self._torch
+        i = self.info
+        prop = torch.cuda.get_device_properties(self.device)
+        return "|".join(str(v) for v in (
+            "x".join(map(str, i.grid)), "x".join(map(str, i.scaled_grid)), "x".join(map(str, i.kbox)),
+            self.natoms, int(self._ea.size), len(self.type_names), self.max_frames,
+            prop.name, prop.multi_processor_count))
+
+    def autotune(self, xyz, boxes, repeats: int = 3, cache: str | None = None) -> dict:
+        """Time every candidate configuration on the frames ``xyz`` (device
+        tensor, as ``forward``) and keep the fastest.
+
+        Each candidate runs once untimed, then ``repeats`` times between CUDA
+        events on the engine stream; the median decides.  Tuning runs the frames
+        through the plan, so it must come before any frames are accumulated and
+        it resets the accumulators afterwards.  ``cache`` (default: the
+        PYCUSAXS_TUNE_CACHE environment variable) names a JSON file of earlier
+        choices keyed by ``tuning_key()``: a hit is applied without timing.
+        Returns {"config": ..., "ms": {candidate: median ms} , "cached": bool}.
+        """
+        torch = self._torch
+        if self.frames:
+            raise RuntimeError("autotune must run before frames are accumulated")
+        cache = cache if cache is not None else os.environ.get("PYCUSAXS_TUNE_CACHE")
+        key = self.tuning_key()
+        cands = self.config_candidates()
+        if cache and os.path.exists(cache):
+            with open(cache) as fh:
+                hit = json.load(fh).get(key)
+            if hit is not None and hit in cands:
+                self.set_config(hit)
+                return {"config": dict(hit), "ms": {}, "cached": True}
+        times = {}
+        for cfg in cands:
+            self.set_config(cfg)
+            self.forward(xyz, boxes)
+            ms = []
+            for _ in range(max(1, int(repeats))):
+                t0 = torch.cuda.Event(enable_timing=True)
+                t1 = torch.cuda.Event(enable_timing=True)
+                t0.record(self.stream)
+                self.forward(xyz, boxes)
+                t1.record(self.stream)
+                t1.synchronize()
+                ms.append(t0.elapsed_time(t1))
+            times[json.dumps(cfg, sort_keys=True)] = float(np.median(ms))
+        best = json.loads(min(times, key=times.get))
+        self.set_config(best)
+        self.reset()
+        if cache:
+            data = {}
+            if os.path.exists(cache):
+                with open(cache) as fh:
+                    data = json.load(fh)
+            data[key] = best
+            tmp = f"{cache}.{os.getpid()}.tmp"
+            with open(tmp, "w") as fh:
+                json.dump(data, fh, indent=1, sort_keys=True)
+            os.replace(tmp, cache)
+        return {"config": best, "ms": times, "cached": False}
 
     # -- frames -----------------------------------------------------------
     def forward(self, xyz, boxes) -> None:
