@@ -292,9 +292,11 @@ def bench_ours(args):
     per_launch_s = dom_ms / 1e3 / max(dom_launches, 1)
     frames_per_launch = frames_timed / max(dom_launches, 1)
     achieved = algo_bytes.get(dom, 0) * frames_per_launch / per_launch_s / 1e9
-    # the kernel that ran for each stage: plan path bits 0/1/2 = z/y/x DFT on tcgen05
+    # the kernel that ran for each stage: plan path bits 0/1/2 = z/y/x DFT on tcgen05,
+    # bit 3 = wide z tiles
     path = info.path
-    kernel_of = {"k_spread_zdft": "k_spread_zdft_tc" if path & 1 else "k_spread_zdft",
+    kernel_of = {"k_spread_zdft": ("k_spread_zdft_tcw" if path & 8 else "k_spread_zdft_tc") if path & 1
+                 else "k_spread_zdft",
                  "k_ydft": "k_dft_tc<y>" if path & 2 else "k_ydft",
                  "k_xdft_post": "k_dft_tc<x>" if path & 4 else "k_xdft_post"}
     tensor = bool({"k_spread_zdft": 1, "k_ydft": 2, "k_xdft_post": 4}.get(dom, 0) & path)

@@ -107,13 +107,17 @@ int saxs_plan_info(const SaxsPlan *plan, SaxsPlanInfo *info);
  * set the fastest.  Graphs built by saxs_graph_create keep the configuration
  * they were captured with. */
 typedef struct SaxsPlanConfig {
-  int z_tensor_cores;     /* 1: spreading + z-axis DFT on tcgen05, 0: FP32 SIMT     */
-  int y_tensor_cores;     /* 1: y-axis DFT on tcgen05, 0: FP32 SIMT                  */
-  int x_tensor_cores;     /* 1: x-axis DFT + post on tcgen05, 0: FP32 SIMT           */
-  int z_producer_groups;  /* producer warp groups of the tensor-core spreading: 1|2 */
+  int z_tensor_cores;     /* 1: spreading + z-axis DFT on tcgen05, 0: FP32 SIMT      */
+  int y_tensor_cores;     /* 1: y-axis DFT on tcgen05, 0: FP32 SIMT                   */
+  int x_tensor_cores;     /* 1: x-axis DFT + post on tcgen05, 0: FP32 SIMT            */
+  int z_wide_tiles;       /* with z_tensor_cores: 1 = 128-column tiles (A in tensor
+                             memory), 0 = 64-column tiles                            */
+  int z_producer_groups;  /* producer warp groups of the tensor-core spreading: 1|2  */
   /* read by saxs_plan_config only: what the plan can run */
   int z_tensor_cores_available, y_tensor_cores_available, x_tensor_cores_available;
-  int z_producer_groups_max;
+  int z_narrow_tiles_available, z_wide_tiles_available;
+  int z_producer_groups_max;       /* 64-column tiles  */
+  int z_wide_producer_groups_max;  /* 128-column tiles */
 } SaxsPlanConfig;
 
 int saxs_plan_config(const SaxsPlan *plan, SaxsPlanConfig *cfg);

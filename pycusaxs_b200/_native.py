@@ -65,9 +65,10 @@ class SaxsParams(ctypes.Structure):
 
 class SaxsPlanConfig(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int) for n in (
-        "z_tensor_cores", "y_tensor_cores", "x_tensor_cores", "z_producer_groups",
+        "z_tensor_cores", "y_tensor_cores", "x_tensor_cores", "z_wide_tiles", "z_producer_groups",
         "z_tensor_cores_available", "y_tensor_cores_available", "x_tensor_cores_available",
-        "z_producer_groups_max")]
+        "z_narrow_tiles_available", "z_wide_tiles_available", "z_producer_groups_max",
+        "z_wide_producer_groups_max")]
 
 
 class SaxsPlanInfo(ctypes.Structure):

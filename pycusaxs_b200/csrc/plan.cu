@@ -90,6 +90,9 @@ struct DevArgs {
   // tensor-core z-DFT (k_spread_zdft_tc): GEMM N, K, spread rows, stages, TMEM columns
   int tcN, tcK, tcR, tcS, tcCols, tcRB, tcCap;
   int tcG;  // producer groups of k_spread_zdft_tc (1, or 2 with two operand stages)
+  // wide-tile variant (k_spread_zdft_tcw): tile row stride (floats), record buffer,
+  // atom table entries, producer groups; y tiles of 16 rows
+  int twN, twRS, twRB, twCap, twG, stw;
   int xtcTP;  // tensor-core x-axis DFT: rows per ky (types padded to 8 or 16)
   int nf[3];
   int dz;
@@ -109,8 +112,10 @@ struct DevArgs {
   const float *ff;    // [T][9]
   const float *twz_sum; // [2*nkzp]: sum over z < ez of the z twiddles (re, im)
   const float *twz_tc;  // [2][tcK x tcN]: z twiddles as TF32 head / remainder, K-major
+  const float *twz_tcw; // the same with twN columns (wide tiles)
   const int4 *home_x; // per spread tile along x: home tiles whose atoms reach it (-1 padded)
   const int4 *home_y;
+  const int4 *home_yw; // per 16-row y tile: up to eight home tiles (two int4, -1 padded)
   int2 *key;
   int *counts;
   int *offsets;
@@ -636,9 +641,12 @@ struct ItemIter {
   int dtx, dty, dt, df;
   int sx, sy, T;
   __device__ __forceinline__ void init(const DevArgs &a, int w0, int g) {
-    sx = a.stiles[0];
-    sy = a.stiles[1];
-    T = a.T;
+    init_dims(w0, g, a.stiles[0], a.stiles[1], a.T);
+  }
+  __device__ __forceinline__ void init_dims(int w0, int g, int sx_, int sy_, int T_) {
+    sx = sx_;
+    sy = sy_;
+    T = T_;
     const int st = sx * sy;
     tx = (w0 % st) % sx;
     ty = (w0 % st) / sx;
@@ -1093,6 +1101,465 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_spread_zdft_tc(DevArgs a, int
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(a.tcCols));
 }
 
+
+// ---------------------------------------------------------------------------
+// Wide-tile tensor-core spreading + z-axis DFT (k_spread_zdft_tcw)
+// ---------------------------------------------------------------------------
+// The same GEMM as k_spread_zdft_tc with M = 128 columns per work item (a tile
+// of 8 x-columns by 16 y-rows, column m = 16*lx + ly in TMEM lane m): twice the
+// columns per item halve the per-item fixed work and the halo share of the
+// atoms, and M = 128 runs the tensor core at its full rate.  The FP32 tile is
+// accumulated in shared memory as [m][z] rows of twRS floats (twRS = tcR + 4, so
+// that 8 consecutive rows of 16-byte loads and the 16 taps of one atom fall in
+// distinct banks), then split into the TF32 head and remainder straight into
+// tensor memory, where the MMAs read A.  Tensor memory (512 columns):
+//   [0, 256)    A: kTwSlots chunks of kTwChunk z (K <= 128), head in the first
+//               32 columns of a chunk, remainder in the next 32
+//   [256, 512)  two accumulator stages of up to 128 columns (N <= 128)
+constexpr int kTwX = 8, kTwY = 16;  // wide tile: x-columns, y-rows (M = 128)
+constexpr int kTwProducerWarps = 24;
+constexpr int kTwMmaWarp = kTwProducerWarps;
+constexpr int kTwLoaderWarp = kTwProducerWarps + 1;
+constexpr int kTwThreads = 32 * (kTwProducerWarps + 6);  // producers, MMA, loader, 4 epilogue warps
+constexpr int kTwSlots = 4;  // A chunks in tensor memory
+constexpr int kTwChunk = 32; // z per chunk
+
+// Record ranges of an item's home bins (up to 4 along x times 8 along y).
+struct TileAtomsW {
+  int start[32];
+  int cum[33];
+  int nb;
+};
+
+struct TwSlot {
+  TileAtomsW ta;
+  int f, t, x0, y0, cw, ch;
+  float mean;
+};
+
+// Loader, first half, for wide tiles: lane 4*iy + ix loads the record range of
+// home bin (hx[ix], hy[iy]); home_y holds eight bins per wide y tile.
+__device__ __forceinline__ void home_ranges_load_w(const DevArgs &a, const int4 *home_x, const int4 *home_y,
+                                                   int f, int t, int tx, int ty, int &s0, int &cnt,
+                                                   bool &valid) {
+  const int lane = threadIdx.x & 31;
+  const int ix = lane & 3, iy = lane >> 2;
+  const int4 hxv = home_x[tx], hyv = home_y[2 * ty + (iy >> 2)];
+  const int hx = ix == 0 ? hxv.x : ix == 1 ? hxv.y : ix == 2 ? hxv.z : hxv.w;
+  const int jy = iy & 3;
+  const int hy = jy == 0 ? hyv.x : jy == 1 ? hyv.y : jy == 2 ? hyv.z : hyv.w;
+  valid = hx >= 0 && hy >= 0;
+  s0 = 0;
+  cnt = 0;
+  if (valid) {
+    const int *off = a.offsets + static_cast<int64_t>(f) * (a.nbins + 1);
+    const int bin = (t * a.tiles[1] + hy) * a.tiles[0] + hx;
+    s0 = off[bin];
+    cnt = off[bin + 1] - s0;
+  }
+}
+
+__device__ __forceinline__ void home_ranges_publish_w(TileAtomsW &ta, int s0, int cnt, bool valid) {
+  const int lane = threadIdx.x & 31;
+  const unsigned bal = __ballot_sync(0xffffffffu, valid);
+  const int pos = __popc(bal & ((1u << lane) - 1u));
+  int inc = cnt;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const int v = __shfl_up_sync(0xffffffffu, inc, d);
+    if (lane >= d) inc += v;
+  }
+  if (valid) {
+    ta.start[pos] = s0;
+    ta.cum[pos + 1] = inc;
+  }
+  if (lane == 0) {
+    ta.cum[0] = 0;
+    ta.nb = __popc(bal);
+  }
+}
+
+// Pre-pass for wide tiles: as spread_prepass, with z offsets that are plain z
+// rows of the [m][z] tile.
+__device__ __forceinline__ void spread_prepass_w(const DevArgs &a, const TileAtomsW &ta, const float4 *srec,
+                                                 int nrec_smem, int f, int v0, int nv, const AtomTab &tab,
+                                                 int x0, int y0, int cw, int ch, int tid, int nthreads) {
+  const int P = a.order, nt = a.ntaps, nz = a.n[2];
+  for (int i = tid; i < nv; i += nthreads) {
+    const int v = v0 + i;
+    float4 q;
+    if (v < nrec_smem) {
+      q = srec[v];
+    } else {
+      int j = 0;
+      while (v >= ta.cum[j + 1]) ++j;
+      q = a.rec[static_cast<int64_t>(f) * a.M + ta.start[j] + (v - ta.cum[j])];
+    }
+    const int m0 = static_cast<int>(q.x), m1 = static_cast<int>(q.y), m2 = static_cast<int>(q.z);
+    float wx[4], wy[4], wz[4];
+    cubic_weights(q.x - static_cast<float>(m0), wx);
+    cubic_weights(q.y - static_cast<float>(m1), wy);
+    cubic_weights(q.z - static_cast<float>(m2), wz);
+    int lxp = 0, lyp = 0, zo[4];
+#pragma unroll
+    for (int o = 0; o < 4; ++o) {
+      int bx = 0xFF, by = 0xFF, zz = 0;
+      if (o < nt) {
+        int x = m0 - P + o;
+        if (x < 0) x += a.n[0];
+        if (static_cast<unsigned>(x - x0) < static_cast<unsigned>(cw)) bx = x - x0;
+        int y = m1 - P + o;
+        if (y < 0) y += a.n[1];
+        if (static_cast<unsigned>(y - y0) < static_cast<unsigned>(ch)) by = y - y0;
+        int z = m2 - P + o;
+        if (z < 0) z += nz;
+        zz = z;
+      }
+      lxp |= bx << (8 * o);
+      lyp |= by << (8 * o);
+      zo[o] = zz;
+    }
+    tab.wx[i] = make_float4(wx[0], wx[1], wx[2], wx[3]);
+    tab.wy[i] = make_float4(wy[0], wy[1], wy[2], wy[3]);
+    tab.wz[i] = make_float4(wz[0], wz[1], wz[2], wz[3]);
+    tab.zo[i] = make_int4(zo[0], zo[1], zo[2], zo[3]);
+    tab.lx[i] = lxp;
+    tab.ly[i] = lyp;
+  }
+}
+
+// Taps for wide tiles: one lane per (atom, y tap, z tap), four x taps each, into
+// the [m][z] tile (row stride rs, m = 16*lx + ly).  With rs = 4 (mod 32) the 16
+// lanes of an atom write banks 4*ly + z (mod 32), all distinct.
+__device__ __forceinline__ void spread_taps_w(const AtomTab &tab, int nv, int nt, float *A, int rs, int tid,
+                                              int nthreads) {
+  for (int u = tid; u < nv * 16; u += nthreads) {
+    const int i = u >> 4, p = (u >> 2) & 3, r = u & 3;
+    if (p >= nt || r >= nt) continue;
+    const int ly = (tab.ly[i] >> (8 * p)) & 0xFF;
+    const int lxp = tab.lx[i];
+    if (ly == 0xFF || lxp == -1) continue;
+    const float wy = reinterpret_cast<const float *>(&tab.wy[i])[p];
+    const float wz = reinterpret_cast<const float *>(&tab.wz[i])[r];
+    const int zo = reinterpret_cast<const int *>(&tab.zo[i])[r];
+    const float4 wx4 = tab.wx[i];
+    const float wx[4] = {wx4.x, wx4.y, wx4.z, wx4.w};
+    float *col = A + zo + ly * rs;
+#pragma unroll
+    for (int o = 0; o < 4; ++o) {
+      const int lx = (lxp >> (8 * o)) & 0xFF;
+      if (lx != 0xFF) atomicAdd(col + lx * kTwY * rs, (wx[o] * wy) * wz);
+    }
+  }
+}
+
+// Persistent, warp-specialized like k_spread_zdft_tc; grid = min(work items,
+// SMs), block kTwThreads.  Work items w = ((f*T + t)*stw + ty)*stiles[0] + tx.
+//   producer warps: twG groups on alternate items, each with its own FP32 tile
+//               and atom table: pre-pass and shared-memory taps into the tile,
+//               then the split: warp q (mod 4) of a group converts rows
+//               32q..32q+31 of 16-z units (tile - mean -> TF32 head and
+//               remainder) into tensor-memory A chunk c with tcgen05.st and
+//               zeroes what it read; the split of item j starts once the MMAs
+//               of item j-1 are complete
+//   MMA warp    one lane issues per A chunk 3 x (kTwChunk/8) MMAs with A from
+//               tensor memory (M = 128, N = twN, K = 8) into the item's
+//               accumulator stage, chunk by chunk as the split delivers them
+//   loader warp home-bin record ranges (up to 32 bins), item data, bulk copies
+//   4 epilogue  accumulator -> Z (lane m = column 16*lx + ly)
+// Hand-offs (mbarriers, every wait bounded):
+//   rec_full[b] / rec_empty[b]   loader <-> producers, record slot b
+//   a_full[c]                    8 split units (4 lane quarters x 2) -> MMA
+//   acc_full[d]                  MMA commit -> epilogue, and -> producers
+//                                (A chunks free for the next item)
+//   acc_empty[d]                 epilogue -> MMA, stage d
+// Every waiter observes each phase of a barrier it waits on in order, never two
+// phases ahead (parity waits cannot tell those apart): a producer group waits
+// for the completion of every item before its own (G = 1) or of the other
+// group's items (G = 2), which alternate on acc_full[d] with d = item & 1.
+// Dynamic shared memory: Bh, Bl (tcK x tcN floats each), twG tiles of 128 x twRS
+// floats, two record buffers of twRB float4, the home-bin tables (stiles[0] +
+// 2*stw int4) and twG atom tables of twCap entries.
+__global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, int items) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ TwSlot slot[2];
+  __shared__ __align__(8) uint64_t bars[4 + kTwSlots + 4];
+  __shared__ uint32_t tmem_slot;
+  __shared__ volatile int abort_flag;
+  const int N = a.twN, KT = a.tcK, R = a.tcR, RB = a.twRB, RS = a.twRS, G = a.twG;
+  const int CH = (KT + kTwChunk - 1) / kTwChunk;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  float *bh = reinterpret_cast<float *>(smem);
+  float *bl = bh + KT * N;
+  float *tiles = bl + KT * N;
+  float4 *recs = reinterpret_cast<float4 *>(tiles + static_cast<size_t>(G) * 128 * RS);
+  int4 *home_x = reinterpret_cast<int4 *>(recs + 2 * RB);
+  int4 *home_y = home_x + a.stiles[0];
+  const int gwarps = kTwProducerWarps / G;
+  const int group = warp < kTwProducerWarps ? warp / gwarps : 0;
+  const int gthreads = 32 * gwarps, gtid = tid - group * gthreads;
+  const int cap = a.twCap;
+  AtomTab tab;
+  tab.wx = reinterpret_cast<float4 *>(reinterpret_cast<unsigned char *>(home_y + 2 * a.stw) +
+                                      static_cast<size_t>(group) * cap * kTcAtomBytes);
+  tab.wy = tab.wx + cap;
+  tab.wz = tab.wy + cap;
+  tab.zo = reinterpret_cast<int4 *>(tab.wz + cap);
+  tab.lx = reinterpret_cast<int *>(tab.zo + cap);
+  tab.ly = tab.lx + cap;
+  uint64_t *rec_full = bars, *rec_empty = bars + 2, *a_full = bars + 4, *acc_full = bars + 4 + kTwSlots,
+           *acc_empty = acc_full + 2;
+  {
+    const float4 *src = reinterpret_cast<const float4 *>(a.twz_tcw);
+    float4 *dst = reinterpret_cast<float4 *>(bh);
+    for (int i = tid; i < KT * N / 2; i += blockDim.x) dst[i] = src[i];
+    float4 *t4 = reinterpret_cast<float4 *>(tiles);
+    for (int i = tid; i < G * 32 * RS; i += blockDim.x) t4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int i = tid; i < a.stiles[0]; i += blockDim.x) home_x[i] = a.home_x[i];
+    for (int i = tid; i < 2 * a.stw; i += blockDim.x) home_y[i] = a.home_yw[i];
+  }
+  if (warp == kTwMmaWarp) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_addr(&tmem_slot)),
+                 "r"(512));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+  }
+  if (tid == 0) {
+    for (int i = 0; i < 4 + kTwSlots + 4; ++i) {
+      int cnt = 1;
+      if (i >= 4 && i < 4 + kTwSlots) cnt = 8;  // a_full: 4 lane quarters x 2 units
+      if (i >= 4 + kTwSlots + 2) cnt = 4;       // acc_empty: 4 epilogue warps
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&bars[i])), "r"(cnt));
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    abort_flag = 0;
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_slot;
+
+  auto wait = [&](uint64_t *bar, int parity) {
+    if (abort_flag) return;
+    if (!mbar_wait(smem_addr(bar), static_cast<uint32_t>(parity & 1))) {
+      abort_flag = 1;
+      atomicExch(a.status, 1);
+    }
+  };
+
+  if (warp < kTwProducerWarps) {
+    const int bar_id = 1 + group;
+    float *A = tiles + static_cast<size_t>(group) * 128 * RS;
+    const int gw = warp - group * gwarps;          // warp within the group (groups start at multiples of 4)
+    const int quarter = warp & 3, wpq = gwarps / 4, rq = gw >> 2;
+    const int m = 32 * quarter + lane;             // the tile row this lane splits
+    float *row = A + static_cast<size_t>(m) * RS;
+    for (int j = group, w = blockIdx.x + group * gridDim.x; w < items; j += G, w += G * gridDim.x) {
+      const int b = j & 1;
+      wait(&rec_full[b], j >> 1);
+      const bool skip = producers_sync_or(abort_flag != 0, bar_id, gthreads);
+      const TwSlot &sl = slot[b];
+      const float mean = sl.mean;
+      if (!skip) {
+        const int nvis = sl.ta.cum[sl.ta.nb];
+        const int nrec = min(nvis, RB);
+        for (int v0 = 0; v0 < nvis; v0 += cap) {
+          const int nv = min(cap, nvis - v0);
+          if (v0 > 0) producers_sync(bar_id, gthreads);
+          spread_prepass_w(a, sl.ta, recs + static_cast<size_t>(b) * RB, nrec, sl.f, v0, nv, tab, sl.x0, sl.y0,
+                           sl.cw, sl.ch, gtid, gthreads);
+          producers_sync(bar_id, gthreads);
+          spread_taps_w(tab, nv, a.ntaps, A, RS, gtid, gthreads);
+        }
+      }
+      producers_sync(bar_id, gthreads);
+      if (gtid == 0) mbar_arrive(smem_addr(&rec_empty[b]));
+      // rows z in [tcK, tcR) meet no twiddle: cleared for the next item
+      for (int i = gtid; i < 128 * ((R - KT) / 4); i += gthreads) {
+        const int mm = i / ((R - KT) / 4), zq = i % ((R - KT) / 4);
+        reinterpret_cast<float4 *>(A + static_cast<size_t>(mm) * RS + KT)[zq] = make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+      // the A chunks are free once the MMAs of the previous item are complete
+      if (j >= 1) wait(&acc_full[(j - 1) & 1], (j - 1) >> 1);
+      __syncwarp();  // converged for the .sync.aligned tensor-memory stores
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      // split units: unit u = 2*c + h covers z in [32c + 16h, +16) of chunk c
+      for (int u = rq; u < 2 * CH; u += wpq) {
+        const int c = u >> 1, h = u & 1;
+        // two halves of 8 z: head to the slot's first 32 columns, remainder to the next 32
+#pragma unroll
+        for (int sub = 0; sub < 2; ++sub) {
+          const int z0 = kTwChunk * c + 16 * h + 8 * sub;
+          uint32_t hi[8], lo[8];
+#pragma unroll
+          for (int k4 = 0; k4 < 2; ++k4) {
+            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (z0 + 4 * k4 < KT) {
+              float4 *p = reinterpret_cast<float4 *>(row + z0 + 4 * k4);
+              v = *p;
+              *p = make_float4(0.f, 0.f, 0.f, 0.f);
+              v.x -= mean;
+              v.y -= mean;
+              v.z -= mean;
+              v.w -= mean;
+            }
+            const float vv[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+              const float hh = tf32_head(vv[e]);
+              hi[4 * k4 + e] = __float_as_uint(hh);
+              lo[4 * k4 + e] = __float_as_uint(vv[e] - hh);
+            }
+          }
+          const uint32_t dst = tmem + (static_cast<uint32_t>(32 * quarter) << 16) +
+                               static_cast<uint32_t>(64 * c + 16 * h + 8 * sub);
+          asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"r"(dst),
+                       "r"(hi[0]), "r"(hi[1]), "r"(hi[2]), "r"(hi[3]), "r"(hi[4]), "r"(hi[5]), "r"(hi[6]),
+                       "r"(hi[7])
+                       : "memory");
+          asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"r"(dst + 32),
+                       "r"(lo[0]), "r"(lo[1]), "r"(lo[2]), "r"(lo[3]), "r"(lo[4]), "r"(lo[5]), "r"(lo[6]),
+                       "r"(lo[7])
+                       : "memory");
+        }
+        asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncwarp();
+        if (lane == 0) mbar_arrive(smem_addr(&a_full[c]));
+      }
+    }
+  } else if (warp == kTwMmaWarp) {
+    if (lane == 0) {
+      // kind::tf32, D f32, A from tensor memory, B K-major, N >> 3 at bit 17, M = 128
+      const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) |
+                             (static_cast<uint32_t>(N >> 3) << 17) | (static_cast<uint32_t>(128 >> 4) << 24);
+      const uint64_t dbh0 = umma_desc(smem_addr(bh), N * 16, 128);
+      const uint64_t dbl0 = umma_desc(smem_addr(bl), N * 16, 128);
+      const uint64_t bstep = static_cast<uint64_t>(N) * 2;  // 8 z of B in 16-byte units
+      int j = 0;
+      uint32_t last_bar = 0;
+      int last_parity = 0;
+      for (int w = blockIdx.x; w < items && !abort_flag; w += gridDim.x, ++j) {
+        const int d = j & 1;
+        const uint32_t dcol = tmem + 256u + static_cast<uint32_t>(128 * d);
+        for (int c = 0; c < CH; ++c) {
+          wait(&a_full[c], j);
+          if (c == 0 && j >= 2) wait(&acc_empty[d], (j - 2) >> 1);
+          if (abort_flag) break;
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const int ks = min(kTwChunk, KT - kTwChunk * c) / 8;
+          for (int kk = 0; kk < ks; ++kk) {
+            const uint32_t ahi = tmem + static_cast<uint32_t>(64 * c + 8 * kk);
+            const uint64_t zb = static_cast<uint64_t>(kTwChunk / 8 * c + kk);
+            umma_tf32_ts(dcol, ahi + 32, dbh0 + zb * bstep, idesc, (c | kk) ? 1u : 0u);
+            umma_tf32_ts(dcol, ahi, dbl0 + zb * bstep, idesc, 1u);
+            umma_tf32_ts(dcol, ahi, dbh0 + zb * bstep, idesc, 1u);
+          }
+        }
+        if (abort_flag) break;
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                         smem_addr(&acc_full[d]))
+                     : "memory");
+        last_bar = smem_addr(&acc_full[d]);
+        last_parity = j >> 1;
+      }
+      if (abort_flag && last_bar) mbar_wait(last_bar, static_cast<uint32_t>(last_parity & 1));
+    }
+  } else if (warp == kTwLoaderWarp) {
+    ItemIter it;
+    it.init_dims(blockIdx.x, gridDim.x, a.stiles[0], a.stw, a.T);
+    int j = 0;
+    for (int w = blockIdx.x; w < items; w += gridDim.x, ++j, it.next()) {
+      const int b = j & 1;
+      const int x0 = it.tx * kTwX, y0 = it.ty * kTwY;
+      int s0, cnt;
+      bool valid;
+      home_ranges_load_w(a, home_x, home_y, it.f, it.t, it.tx, it.ty, s0, cnt, valid);
+      const float pmean = a.pad_val ? a.pad_val[it.t] : 0.0f;
+      const double bsum = a.pad_val ? 0.0 : a.border[static_cast<int64_t>(it.f) * a.T + it.t];
+      if (j >= 2) wait(&rec_empty[b], (j - 2) >> 1);
+      if (__any_sync(0xffffffffu, abort_flag != 0)) break;
+      TwSlot &sl = slot[b];
+      home_ranges_publish_w(sl.ta, s0, cnt, valid);
+      if (lane == 0) {
+        sl.f = it.f;
+        sl.t = it.t;
+        sl.x0 = x0;
+        sl.y0 = y0;
+        sl.cw = min(kTwX, a.ext[0] - x0);
+        sl.ch = min(kTwY, a.ext[1] - y0);
+        sl.mean = a.pad_val ? pmean : static_cast<float>(bsum / a.border_count);
+      }
+      __syncwarp();
+      if (lane == 0) {
+        const TileAtomsW &tb = sl.ta;
+        const int nrec = min(tb.cum[tb.nb], RB);
+        const uint32_t bar = smem_addr(&rec_full[b]);
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(nrec * 16)
+                     : "memory");
+        const float4 *src = a.rec + static_cast<int64_t>(it.f) * a.M;
+        const uint32_t dst = smem_addr(recs + static_cast<size_t>(b) * RB);
+        int r = 0;
+        while (r < tb.nb && tb.cum[r] < nrec) {
+          int e = r;
+          while (e + 1 < tb.nb && tb.start[e + 1] == tb.start[e] + (tb.cum[e + 1] - tb.cum[e])) ++e;
+          const int lo = tb.cum[r], hi = min(tb.cum[e + 1], nrec);
+          if (hi > lo)
+            asm volatile(
+                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                    dst + static_cast<uint32_t>(lo) * 16),
+                "l"(src + tb.start[r]), "r"((hi - lo) * 16), "r"(bar)
+                : "memory");
+          r = e + 1;
+        }
+      }
+    }
+  } else {
+    const int quarter = warp & 3;
+    ItemIter it;
+    it.init_dims(blockIdx.x, gridDim.x, a.stiles[0], a.stw, a.T);
+    const int64_t zplane = static_cast<int64_t>(a.ext[0]) * a.ext[1];
+    int j = 0;
+    for (int w = blockIdx.x; w < items; w += gridDim.x, ++j, it.next()) {
+      const int d = j & 1;
+      wait(&acc_full[d], j >> 1);
+      if (__any_sync(0xffffffffu, abort_flag != 0)) break;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const int x0 = it.tx * kTwX, y0 = it.ty * kTwY;
+      float2 *Zft = a.Z + (static_cast<int64_t>(it.f) * a.T + it.t) * a.nkz * zplane;
+      const int m = 32 * quarter + lane, lx = m >> 4, ly = m & 15;
+      const bool valid = lx < min(kTwX, a.ext[0] - x0) && ly < min(kTwY, a.ext[1] - y0);
+      const int64_t cell = static_cast<int64_t>(x0 + lx) * a.ext[1] + (y0 + ly);
+      const uint32_t lane_base = tmem + (static_cast<uint32_t>(32 * quarter) << 16) + 256u +
+                                 static_cast<uint32_t>(128 * d);
+      for (int c0 = 0; c0 < N; c0 += 8) {
+        uint32_t r[8];
+        asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                     : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                       "=r"(r[7])
+                     : "r"(lane_base + c0));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (valid) {
+#pragma unroll
+          for (int jj = 0; jj < 4; ++jj) {
+            const int kz = c0 / 2 + jj;
+            if (kz < a.nkz)
+              Zft[kz * zplane + cell] = make_float2(__uint_as_float(r[2 * jj]), __uint_as_float(r[2 * jj + 1]));
+          }
+        }
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(smem_addr(&acc_empty[d]));
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (warp == kTwMmaWarp)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
+}
 
 // grid (ceil(ex/64), nkz, frames*T), block 256: y-axis DFT.
 // Y[f,t,kz][ky][x] = sum_y Z[f,t,kz][x][y] * exp(-2 pi i ja y / nny).
@@ -2273,9 +2740,12 @@ struct SaxsPlan {
   bool adj_tiled_y = false, adj_tiled_z = false;
   size_t smem_yadj = 0, smem_zadj = 0;
   int spread_ctas = 1;  // resident CTAs of the persistent spreading kernel
-  bool use_tc = false;  // z-axis DFT on the tensor cores (k_spread_zdft_tc)
-  size_t smem_spread_tc = 0;
-  int tc_ctas = 1;
+  bool use_tc = false;   // z-axis DFT on the tensor cores
+  bool use_tcw = false;  // ... with the wide-tile kernel (k_spread_zdft_tcw), else k_spread_zdft_tc
+  size_t smem_spread_tc = 0, smem_spread_tcw = 0;
+  int tc_ctas = 1, tcw_ctas = 1;
+  bool tcn_ok = false, tcw_ok = false;  // z kernels the plan can run: 64- and 128-column tiles
+  int twG_max = 1;                      // producer groups the wide kernel's shared memory allows
   bool tc_ok = false, ytc_ok = false, xtc_ok = false;  // tensor-core kernels the plan can run
   bool use_ytc = false;  // y-axis DFT on the tensor cores (k_dft_tc<false>)
   bool use_xtc = false;  // x-axis DFT + post on the tensor cores (k_dft_tc<true>)
@@ -2354,6 +2824,30 @@ bool home_tile_table(int ext, int n, int order, int bin_w, std::vector<int4> *ou
       }
     }
     out->push_back(make_int4(h[0], h[1], h[2], h[3]));
+  }
+  return true;
+}
+
+// The same for the 16-row y tiles of k_spread_zdft_tcw: up to eight bins per
+// tile, two int4 each.  Returns false when a tile would need more.
+bool home_tile_table_w(int ext, int n, int order, int bin_w, std::vector<int4> *out) {
+  out->clear();
+  for (int c0 = 0; c0 < ext; c0 += kTwY) {
+    const int cw = std::min(kTwY, ext - c0);
+    int h[8] = {-1, -1, -1, -1, -1, -1, -1, -1}, cnt = 0;
+    for (int d = 0; d < cw + order - 1; ++d) {
+      int x = (c0 - order + 1 + d) % n;
+      if (x < 0) x += n;
+      const int t = x / bin_w;
+      bool seen = false;
+      for (int k = 0; k < cnt; ++k) seen |= (h[k] == t);
+      if (!seen) {
+        if (cnt == 8) return false;
+        h[cnt++] = t;
+      }
+    }
+    out->push_back(make_int4(h[0], h[1], h[2], h[3]));
+    out->push_back(make_int4(h[4], h[5], h[6], h[7]));
   }
   return true;
 }
@@ -2545,6 +3039,8 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
   a.tiles[1] = (a.n[1] + a.bin_w - 1) / a.bin_w;
   a.stiles[0] = (a.ext[0] + kTile - 1) / kTile;
   a.stiles[1] = (a.ext[1] + kTile - 1) / kTile;
+  std::vector<int4> hywt;
+  a.stw = home_tile_table_w(a.ext[1], a.n[1], a.order, a.bin_w, &hywt) ? (a.ext[1] + kTwY - 1) / kTwY : 0;
   a.nbins = a.T * a.tiles[0] * a.tiles[1];
   a.dz = static_cast<int>(0.07f * a.n[2] / 2);  // borderBins (saxsKernel.h:107-110)
   {
@@ -2615,12 +3111,15 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
     pl->smem_xdft = fixed + static_cast<size_t>(pl->xc) * per_x;
   }
   {
-    // tensor-core z-DFT: N = 2*nkz padded to 8 (<= 256), K = ez padded to 8, two
-    // operand stages when they fit, else one.  PYCUSAXS_ZDFT=simt keeps the FP32
-    // SIMT kernel.
+    // tensor-core z-DFT: N = 2*nkz padded to 8 (<= 256; to 16 and <= 128 for wide tiles),
+    // K = ez padded to 8, two operand stages when they fit, else one.
+    // PYCUSAXS_ZDFT=simt keeps the FP32 SIMT kernel, PYCUSAXS_ZDFT=narrow the
+    // 64-column tensor-core kernel.
     const char *mode = std::getenv("PYCUSAXS_ZDFT");
     const bool simt_only = mode && std::strcmp(mode, "simt") == 0;
+    const bool narrow_only = mode && std::strcmp(mode, "narrow") == 0;
     const int N = round_up(2 * a.nkz, 8);
+    const int NW = round_up(2 * a.nkz, 16);  // M = 128 needs N a multiple of 16
     const int KT = round_up(a.ext[2], 8);
     const int R = std::max(KT, round_up(a.n[2], 8));
     const size_t avail = optin - static_smem(k_spread_zdft_tc);
@@ -2641,11 +3140,48 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
             RB = rb;
             CAP = cap;
           }
-    if (!simt_only && N <= 256 && S > 0) {
+    // wide tiles: twG FP32 tiles of 128 x (R + 4) floats; two producer groups
+    // before larger record buffers and atom tables
+    int GW = 0, RBW = 0, CAPW = 0;
+    const int RSW = R + 4;
+    const size_t home_w = static_cast<size_t>(a.stiles[0] + 2 * a.stw) * sizeof(int4);
+    const size_t bw_bytes = 2 * static_cast<size_t>(KT) * NW * sizeof(float);
+    if (a.stw > 0 && NW <= 128 && KT <= kTwSlots * kTwChunk) {
+      const size_t avail_w = optin - static_smem(k_spread_zdft_tcw);
+      static const int cand[][2] = {{1024, 256}, {512, 256}, {512, 128}, {1024, 64},
+                                    {256, 128},  {256, 64},  {128, 64}};
+      for (int g = 2; g >= 1 && GW == 0; --g)
+        for (const auto &c : cand)
+          if (GW == 0 && bw_bytes + static_cast<size_t>(g) * 128 * RSW * sizeof(float) +
+                                 2 * static_cast<size_t>(c[0]) * 16 + home_w +
+                                 static_cast<size_t>(g) * c[1] * kTcAtomBytes <=
+                             avail_w) {
+            GW = g;
+            RBW = c[0];
+            CAPW = c[1];
+          }
+    }
+    pl->tcn_ok = !simt_only && N <= 256 && S > 0;
+    pl->tcw_ok = !simt_only && !narrow_only && GW > 0;
+    if (pl->tcn_ok || pl->tcw_ok) {
       pl->use_tc = true;
+      pl->use_tcw = pl->tcw_ok;
       a.tcN = N;
       a.tcK = KT;
       a.tcR = R;
+    }
+    if (pl->tcw_ok) {
+      a.twN = NW;
+      a.twRS = RSW;
+      a.twRB = RBW;
+      a.twCap = CAPW;
+      a.twG = GW;
+      pl->twG_max = GW;
+      pl->smem_spread_tcw = bw_bytes + static_cast<size_t>(GW) * 128 * RSW * sizeof(float) +
+                            2 * static_cast<size_t>(RBW) * 16 + home_w +
+                            static_cast<size_t>(GW) * CAPW * kTcAtomBytes;
+    }
+    if (pl->tcn_ok) {
       a.tcS = S;
       a.tcRB = RB;
       a.tcCap = CAP;
@@ -2720,7 +3256,11 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
   int4 *d_hx = nullptr, *d_hy = nullptr;
   float *d_twzs = nullptr, *d_twztc = nullptr, *d_twytc = nullptr, *d_twxtc = nullptr;
   ALLOC(d_twzs, 2 * a.nkzp);
-  if (pl->use_tc) ALLOC(d_twztc, 2 * static_cast<size_t>(a.tcK) * a.tcN);
+  int4 *d_hyw = nullptr;
+  float *d_twztcw = nullptr;
+  if (pl->tcn_ok) ALLOC(d_twztc, 2 * static_cast<size_t>(a.tcK) * a.tcN);
+  if (pl->tcw_ok) ALLOC(d_twztcw, 2 * static_cast<size_t>(a.tcK) * a.twN);
+  if (pl->tcw_ok) ALLOC(d_hyw, 2 * static_cast<size_t>(a.stw));
   if (pl->use_ytc) ALLOC(d_twytc, static_cast<size_t>(pl->yshape.chunks) * 4 * pl->yshape.N * kDtcChunk);
   if (pl->use_xtc) ALLOC(d_twxtc, static_cast<size_t>(pl->xshape.chunks) * 4 * pl->xshape.N * kDtcChunk);
   ALLOC(d_hx, a.stiles[0]);
@@ -2753,10 +3293,12 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
   a.pad_val = d_pad;
   a.twz_sum = d_twzs;
   a.twz_tc = d_twztc;
+  a.twz_tcw = d_twztcw;
   pl->yshape.B = d_twytc;
   pl->xshape.B = d_twxtc;
   a.home_x = d_hx;
   a.home_y = d_hy;
+  a.home_yw = d_hyw;
   a.geom = d_geom;
   a.status = d_status;
 
@@ -2778,9 +3320,11 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
   }
   // the same z twiddles in the tensor-core B layout, split into a TF32 head and
   // the exact remainder
-  std::vector<float> twtc(pl->use_tc ? 2 * static_cast<size_t>(a.tcK) * a.tcN : 0, 0.0f);
-  if (pl->use_tc) {
-    const size_t half = static_cast<size_t>(a.tcK) * a.tcN;
+  // B operand of the tensor-core z passes, N columns: the z twiddles split into a
+  // TF32 head and remainder, K-major canonical layout
+  auto z_operand = [&](int N) {
+    std::vector<float> out(2 * static_cast<size_t>(a.tcK) * N, 0.0f);
+    const size_t half = static_cast<size_t>(a.tcK) * N;
     for (int z = 0; z < ez; ++z)
       for (int n = 0; n < 2 * a.nkz; ++n) {
         const float2 w = twz[z * a.nkzp + n / 2];
@@ -2790,11 +3334,14 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
         bits &= 0xFFFFE000u;
         float head;
         std::memcpy(&head, &bits, sizeof(head));
-        const size_t o = static_cast<size_t>(z / 4) * (a.tcN / 8) * 32 + (n / 8) * 32 + (n % 8) * 4 + z % 4;
-        twtc[o] = head;
-        twtc[half + o] = v - head;
+        const size_t o = static_cast<size_t>(z / 4) * (N / 8) * 32 + (n / 8) * 32 + (n % 8) * 4 + z % 4;
+        out[o] = head;
+        out[half + o] = v - head;
       }
-  }
+    return out;
+  };
+  const std::vector<float> twtc = pl->tcn_ok ? z_operand(a.tcN) : std::vector<float>();
+  const std::vector<float> twtcw = pl->tcw_ok ? z_operand(a.twN) : std::vector<float>();
   std::vector<float2> twy(static_cast<size_t>(ey) * a.nkyp, make_float2(0.f, 0.f));
   for (int y = 0; y < ey; ++y)
     for (int k = 0; k < a.nky; ++k)
@@ -2834,9 +3381,11 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
       (rc = up(d_hx, hxt.data(), sizeof(int4) * hxt.size())) ||
       (rc = up(d_twzs, twzs.data(), sizeof(float) * twzs.size())) ||
       (rc = up(d_twztc, twtc.data(), sizeof(float) * twtc.size())) ||
+      (rc = up(d_twztcw, twtcw.data(), sizeof(float) * twtcw.size())) ||
       (rc = up(d_twytc, twytc.data(), sizeof(float) * twytc.size())) ||
       (rc = up(d_twxtc, twxtc.data(), sizeof(float) * twxtc.size())) ||
       (rc = up(d_hy, hyt.data(), sizeof(int4) * hyt.size())) ||
+      (rc = up(d_hyw, hywt.data(), pl->tcw_ok ? sizeof(int4) * hywt.size() : 0)) ||
       (rc = up(pl->d_geom0, g0, sizeof(g0)))) {
     destroy(pl);
     return rc;
@@ -2859,6 +3408,7 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
   if (e == cudaSuccess) e = raise_smem_limit(k_hist<float>);
   if (e == cudaSuccess) e = raise_smem_limit(k_hist<double>);
   if (e == cudaSuccess) e = raise_smem_limit(k_spread_zdft_tc);
+  if (e == cudaSuccess) e = raise_smem_limit(k_spread_zdft_tcw);
   if (e == cudaSuccess) e = raise_smem_limit(k_dft_tc<false>);
   if (e == cudaSuccess) e = raise_smem_limit(k_dft_tc<true>);
   if (e == cudaSuccess) {
@@ -2867,7 +3417,8 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
                                                       pl->smem_spread);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, pl->device);
     pl->spread_ctas = std::max(1, per_sm) * std::max(1, sms);
-    if (e == cudaSuccess && pl->use_tc) {
+    if (e == cudaSuccess && pl->tcw_ok) pl->tcw_ctas = std::max(1, sms);  // 512 TMEM columns: one per SM
+    if (e == cudaSuccess && pl->tcn_ok) {
       // resident CTAs whose tensor-memory allocations fit the SM's 512 columns together
       int tc_per_sm = 0;
       e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tc_per_sm, k_spread_zdft_tc, kTcThreads,
@@ -2932,9 +3483,16 @@ struct StageTimer {
   }
 };
 
-// Spreading + z-axis DFT of `items` work items: the tensor-core kernel when the
-// plan has it, else the FP32 SIMT kernel.
-int launch_spread(const SaxsPlan *pl, const DevArgs &a, int items, cudaStream_t st) {
+// Spreading + z-axis DFT of `nframes` frames: the wide-tile or 64-column
+// tensor-core kernel the plan is configured for, else the FP32 SIMT kernel.
+int launch_spread(const SaxsPlan *pl, const DevArgs &a, int nframes, cudaStream_t st) {
+  if (pl->use_tc && pl->use_tcw) {
+    const int items = a.stiles[0] * a.stw * a.T * nframes;
+    k_spread_zdft_tcw<<<std::max(1, std::min(items, pl->tcw_ctas)), kTwThreads, pl->smem_spread_tcw, st>>>(
+        a, items);
+    return launch_check("k_spread_zdft_tcw");
+  }
+  const int items = a.stiles[0] * a.stiles[1] * a.T * nframes;
   if (pl->use_tc) {
     k_spread_zdft_tc<<<std::max(1, std::min(items, pl->tc_ctas)), kTcThreads, pl->smem_spread_tc,
                        st>>>(a, items);
@@ -3053,9 +3611,8 @@ int enqueue_batch(SaxsPlan *pl, const DevArgs &a, int nframes, cudaStream_t st, 
     CUDA_TRY(cudaMemsetAsync(a.offsets, 0, sizeof(int) * nframes * (a.nbins + 1), st));
   }
   {
-    const int items = a.stiles[0] * a.stiles[1] * a.T * nframes;
     tm.begin(kStSpread);
-    const int rc = launch_spread(pl, a, items, st);
+    const int rc = launch_spread(pl, a, nframes, st);
     tm.end(kStSpread);
     if (rc) return rc;
   }
@@ -3393,9 +3950,9 @@ int backward(SaxsPlan *pl, const float *xyz, const float *box, const double *dl,
   } else {
     CUDA_TRY(cudaMemsetAsync(a.offsets, 0, sizeof(int) * (a.nbins + 1), st));
   }
-  const int items = a.stiles[0] * a.stiles[1] * a.T;
-  if (int rc = launch_spread(pl, a, items, st)) return rc;
+  if (int rc = launch_spread(pl, a, 1, st)) return rc;
   if (int rc = launch_ydft(pl, a, a.T * a.nkz, st)) return rc;
+  const int items = a.stiles[0] * a.stiles[1] * a.T;  // 8 x 8 column tiles of the z adjoint
   // adjoint passes
   dim3 gx((a.nky + kXRows - 1) / kXRows, a.nkz, 1);
   k_xdft_grad<<<gx, kThreads, pl->smem_xdft, st>>>(a, j, pl->xc);
@@ -3522,8 +4079,7 @@ int forward_into_scratch(SaxsPlan *pl, const float *xyz, const float *box, unsig
   } else {
     CUDA_TRY(cudaMemsetAsync(a.offsets, 0, sizeof(int) * (a.nbins + 1), st));
   }
-  const int items = a.stiles[0] * a.stiles[1] * a.T;
-  if (int rc = launch_spread(pl, a, items, st)) return rc;
+  if (int rc = launch_spread(pl, a, 1, st)) return rc;
   if (int rc = launch_ydft(pl, a, a.T * a.nkz, st)) return rc;
   if (int rc = launch_xdft(pl, a, 1, st)) return rc;
   dim3 gh(a.nkz, 1);
@@ -3559,7 +4115,8 @@ int saxs_plan_info(const SaxsPlan *pl, SaxsPlanInfo *info) {
   info->kbox[1] = a.nky;
   info->kbox[2] = a.nkz;
   info->kz_count = a.nkz;
-  info->path = (pl->use_tc ? 1 : 0) | (pl->use_ytc ? 2 : 0) | (pl->use_xtc ? 4 : 0);
+  info->path = (pl->use_tc ? 1 : 0) | (pl->use_ytc ? 2 : 0) | (pl->use_xtc ? 4 : 0) |
+               (pl->use_tc && pl->use_tcw ? 8 : 0);
   info->device_bytes = pl->bytes;
   info->frames_accumulated = pl->frames;
   return SAXS_OK;
@@ -3570,26 +4127,35 @@ int saxs_plan_config(const SaxsPlan *pl, SaxsPlanConfig *cfg) {
   cfg->z_tensor_cores = pl->use_tc ? 1 : 0;
   cfg->y_tensor_cores = pl->use_ytc ? 1 : 0;
   cfg->x_tensor_cores = pl->use_xtc ? 1 : 0;
-  cfg->z_producer_groups = pl->use_tc ? pl->a.tcG : 1;
+  cfg->z_wide_tiles = pl->use_tc && pl->use_tcw ? 1 : 0;
+  cfg->z_producer_groups = !pl->use_tc ? 1 : pl->use_tcw ? pl->a.twG : pl->a.tcG;
   cfg->z_tensor_cores_available = pl->tc_ok ? 1 : 0;
   cfg->y_tensor_cores_available = pl->ytc_ok ? 1 : 0;
   cfg->x_tensor_cores_available = pl->xtc_ok ? 1 : 0;
-  cfg->z_producer_groups_max = (pl->tc_ok && pl->a.tcS == 2) ? 2 : 1;
+  cfg->z_narrow_tiles_available = pl->tcn_ok ? 1 : 0;
+  cfg->z_wide_tiles_available = pl->tcw_ok ? 1 : 0;
+  cfg->z_producer_groups_max = (pl->tcn_ok && pl->a.tcS == 2) ? 2 : 1;
+  cfg->z_wide_producer_groups_max = pl->tcw_ok ? pl->twG_max : 1;
   return SAXS_OK;
 }
 
 int saxs_plan_set_config(SaxsPlan *pl, const SaxsPlanConfig *cfg) {
   if (!pl || !cfg) return fail(SAXS_E_INVALID, "null argument");
-  if ((cfg->z_tensor_cores && !pl->tc_ok) || (cfg->y_tensor_cores && !pl->ytc_ok) ||
+  const bool z = cfg->z_tensor_cores != 0, wide = z && cfg->z_wide_tiles != 0;
+  if ((z && !(wide ? pl->tcw_ok : pl->tcn_ok)) || (cfg->y_tensor_cores && !pl->ytc_ok) ||
       (cfg->x_tensor_cores && !pl->xtc_ok))
     return fail(SAXS_E_INVALID, "a tensor-core pass the plan cannot run was requested");
-  const int gmax = (pl->tc_ok && pl->a.tcS == 2) ? 2 : 1;
+  const int gmax = !z ? 1 : wide ? pl->twG_max : (pl->a.tcS == 2 ? 2 : 1);
   if (cfg->z_producer_groups < 1 || cfg->z_producer_groups > gmax)
     return fail(SAXS_E_INVALID, "z_producer_groups must be 1.." + std::to_string(gmax));
-  pl->use_tc = cfg->z_tensor_cores != 0;
+  pl->use_tc = z;
+  pl->use_tcw = wide;
   pl->use_ytc = cfg->y_tensor_cores != 0;
   pl->use_xtc = cfg->x_tensor_cores != 0;
-  pl->a.tcG = cfg->z_producer_groups;
+  if (wide)
+    pl->a.twG = cfg->z_producer_groups;
+  else if (z)
+    pl->a.tcG = cfg->z_producer_groups;
   return SAXS_OK;
 }
 

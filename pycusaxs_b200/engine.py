@@ -42,10 +42,10 @@ class PlanInfo:
     kbox: tuple
     device_bytes: int
     frames: int
-    path: int = 0  # bits 1, 2, 4: the z-, y-, x-axis DFT on the tensor cores (tcgen05)
+    path: int = 0  # bits 1, 2, 4: the z-, y-, x-axis DFT on the tensor cores (tcgen05); 8: wide z tiles
 
 
-CONFIG_KEYS = ("z_tensor_cores", "y_tensor_cores", "x_tensor_cores", "z_producer_groups")
+CONFIG_KEYS = ("z_tensor_cores", "y_tensor_cores", "x_tensor_cores", "z_wide_tiles", "z_producer_groups")
 
 
 def entries_from_index(atom_index: dict, natoms: int | None = None):
@@ -165,23 +165,23 @@ class SaxsEngine:
 
     def config(self) -> dict:
         """The kernel configuration in use: tensor cores (1) or FP32 SIMT (0) for
-        the z, y and x passes, and the producer groups of the tensor-core
-        spreading."""
+        the z, y and x passes, 128- (1) or 64-column (0) tiles and the producer
+        groups of the tensor-core spreading."""
         c = self._config_struct()
         return {k: int(getattr(c, k)) for k in CONFIG_KEYS}
 
     def config_candidates(self) -> list:
         """Every configuration the plan can run (its resources cover them all)."""
         c = self._config_struct()
-        zs = [0, 1] if c.z_tensor_cores_available else [0]
+        zk = [(0, 0, 1)]  # (tensor cores, wide tiles, producer groups)
+        if c.z_narrow_tiles_available:
+            zk += [(1, 0, g) for g in range(1, c.z_producer_groups_max + 1)]
+        if c.z_wide_tiles_available:
+            zk += [(1, 1, g) for g in range(1, c.z_wide_producer_groups_max + 1)]
         ys = [0, 1] if c.y_tensor_cores_available else [0]
         xs = [0, 1] if c.x_tensor_cores_available else [0]
-        out = []
-        for z, y, x in itertools.product(zs, ys, xs):
-            for g in (range(1, c.z_producer_groups_max + 1) if z else (1,)):
-                out.append({"z_tensor_cores": z, "y_tensor_cores": y, "x_tensor_cores": x,
-                            "z_producer_groups": g})
-        return out
+        return [{"z_tensor_cores": z, "y_tensor_cores": y, "x_tensor_cores": x, "z_wide_tiles": w,
+                 "z_producer_groups": g} for (z, w, g), y, x in itertools.product(zk, ys, xs)]
 
     def set_config(self, cfg: dict) -> None:
         """Select one of ``config_candidates()``; work already queued keeps the

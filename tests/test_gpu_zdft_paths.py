@@ -1,9 +1,11 @@
 """Tensor-core (tcgen05, 3xTF32) z-, y- and x-axis DFTs vs the FP32 SIMT kernels and the FP64 oracle (GPU).
 
 Plans take a tensor-core kernel whenever its operands fit shared memory
-(``info.path`` bits 0, 1, 2 for the z-, y- and x-axis DFTs);
+(``info.path`` bits 0, 1, 2 for the z-, y- and x-axis DFTs; bit 3 when the z
+pass runs the 128-column wide-tile kernel);
 ``PYCUSAXS_ZDFT=simt`` / ``PYCUSAXS_YDFT=simt`` / ``PYCUSAXS_XDFT=simt`` at plan
-creation keep the SIMT kernel.  Both must give identical bin counts and profiles within the 1e-4
+creation keep the SIMT kernel, ``PYCUSAXS_ZDFT=narrow`` the 64-column
+tensor-core z kernel.  Every z case runs with both z kernels.  Both must give identical bin counts and profiles within the 1e-4
 tolerance of the FP64 oracle; the 3xTF32 products are accurate to ~2^-19, and
 TC_VS_SIMT_RTOL (2e-5 per bin) bounds the difference between the two kernels.
 """
@@ -40,9 +42,14 @@ def dft_mode(var, mode):
 _AXES = {"z": ("PYCUSAXS_ZDFT", 1), "y": ("PYCUSAXS_YDFT", 2), "x": ("PYCUSAXS_XDFT", 4)}
 
 
-def _both(system, grid, frames, expect_tc=True, axis="z", **kw):
+@pytest.fixture(params=["wide", "narrow"])
+def zmode(request):
+    return request.param
+
+
+def _both(system, grid, frames, expect_tc=True, axis="z", zmode="wide", expect_wide=None, **kw):
     var, bit = _AXES[axis]
-    with dft_mode(var, None):
+    with dft_mode(var, "narrow" if (axis == "z" and zmode == "narrow") else None):
         h_tc, n_tc, e_tc = engine_hist(system, grid, frames, **kw)
         path_tc = e_tc.info.path
         e_tc.close()
@@ -52,6 +59,10 @@ def _both(system, grid, frames, expect_tc=True, axis="z", **kw):
         e_s.close()
     assert path_s & bit == 0
     assert (path_tc & bit) == (bit if expect_tc else 0)
+    if axis == "z" and zmode == "narrow":
+        assert path_tc & 8 == 0
+    elif axis == "z" and expect_wide is not None:
+        assert (path_tc & 8) == (8 if expect_wide else 0), path_tc
     np.testing.assert_array_equal(n_tc, n_s)
     sel = n_s > 0
     sel[0] = False
@@ -59,7 +70,8 @@ def _both(system, grid, frames, expect_tc=True, axis="z", **kw):
     ho, no, _ = oracle_hist(system, grid, frames, **{k: v for k, v in kw.items() if k != "max_frames"})
     err_tc = assert_profiles_close(h_tc, n_tc, ho, no)
     err_s = assert_profiles_close(h_s, n_s, ho, no)
-    print(f"vs FP64 oracle: tensor cores {err_tc:.2e}, SIMT {err_s:.2e}; between them {diff.max():.2e}")
+    print(f"path {path_tc}: vs FP64 oracle: tensor cores {err_tc:.2e}, SIMT {err_s:.2e}; "
+          f"between them {diff.max():.2e}")
     assert diff.max() <= TC_VS_SIMT_RTOL, diff.max()
     return err_tc, float(diff.max())
 
@@ -72,46 +84,55 @@ def _line_system(n, lengths, seed, elements=("C", "O")):
     return System(el, pos, np.diag(L).astype(np.float32))
 
 
-def test_tc_small_cubic(cuda):
+def test_tc_small_cubic(cuda, zmode):
     s = cubic_system(4000, 40.0, seed=11)
-    _both(s, (32, 32, 32), [s.positions], sigma=2.0, qcut=0.6)
+    _both(s, (32, 32, 32), [s.positions], sigma=2.0, qcut=0.6, zmode=zmode, expect_wide=True)
 
 
-def test_tc_bench_sized_grid128(cuda):
+def test_tc_bench_sized_grid128(cuda, zmode):
     # the trajectory workload's plan: grid 128, 256^3 supercell, q-cut 0.5
     s = cubic_system(30_000, 120.0, seed=12)
-    _both(s, (128, 128, 128), [s.positions], sigma=2.0, qcut=0.5, bin_size=0.002)
+    _both(s, (128, 128, 128), [s.positions], sigma=2.0, qcut=0.5, bin_size=0.002, zmode=zmode,
+          expect_wide=True)
 
 
-def test_tc_uneven_grid_z_not_multiple_of_8(cuda):
-    # z extent 44 -> K padded to 48 with zero twiddle rows
+def test_tc_uneven_grid_z_not_multiple_of_8(cuda, zmode):
+    # z extent 44 -> K padded to 48 with zero twiddle rows (a partial last ring
+    # slot of the wide kernel); x extent 24 and y extent 32
     s = _line_system(3000, (30.0, 40.0, 44.0), 13, ("H", "C", "O", "N"))
-    _both(s, (24, 32, 44), [s.positions], sigma=2.5, qcut=0.9)
+    _both(s, (24, 32, 44), [s.positions], sigma=2.5, qcut=0.9, zmode=zmode, expect_wide=True)
 
 
-def test_tc_order2_two_taps(cuda):
+def test_tc_ragged_tiles(cuda, zmode):
+    # x extent 20 and y extent 28: the last tiles of both axes are partial
+    s = _line_system(3000, (25.0, 35.0, 40.0), 113, ("H", "C", "O"))
+    _both(s, (20, 28, 32), [s.positions], sigma=2.0, qcut=0.8, zmode=zmode, expect_wide=True)
+
+
+def test_tc_order2_two_taps(cuda, zmode):
     s = cubic_system(3000, 36.0, seed=14)
-    _both(s, (32, 32, 32), [s.positions], order=2, sigma=2.0, qcut=0.7)
+    _both(s, (32, 32, 32), [s.positions], order=2, sigma=2.0, qcut=0.7, zmode=zmode)
 
 
-def test_tc_supercell_smaller_than_grid(cuda):
+def test_tc_supercell_smaller_than_grid(cuda, zmode):
     # scaled grid below the grid: the transform crops, spread rows exceed K
     s = cubic_system(3000, 36.0, seed=15)
-    _both(s, (40, 40, 40), [s.positions], scaled_grid=(32, 32, 30), qcut=0.6)
+    _both(s, (40, 40, 40), [s.positions], scaled_grid=(32, 32, 30), qcut=0.6, zmode=zmode)
 
 
-def test_tc_single_operand_stage_long_z(cuda):
-    # z extent 256, 17 kz values (N = 40): twiddles 80 KB + one 128 KB operand stage
-    # fit shared memory, two stages do not
+def test_tc_single_operand_stage_long_z(cuda, zmode):
+    # z extent 256, 17 kz values (N = 48): twiddles 96 KB + one 128 KB operand stage
+    # fit shared memory, two stages do not; a wide tile (133 KB) does not fit
     s = _line_system(4000, (80.0, 80.0, 320.0), 16)
-    _both(s, (32, 32, 256), [s.positions], sigma=2.0, qcut=0.15)
+    _both(s, (32, 32, 256), [s.positions], sigma=2.0, qcut=0.15, zmode=zmode, expect_wide=False)
 
 
-def test_tc_many_kz_wide_n(cuda):
+def test_tc_many_kz_wide_n(cuda, zmode):
     # long z at the largest q-cut the grid allows (reset to ~1.55 /A): the full kz
     # axis, 97 values, N = 200 with one operand stage
+    # (N > 128: no wide tiles)
     s = _line_system(1500, (16.0, 16.0, 192.0), 17)
-    _both(s, (16, 16, 96), [s.positions], sigma=2.0, qcut=3.5)
+    _both(s, (16, 16, 96), [s.positions], sigma=2.0, qcut=3.5, zmode=zmode, expect_wide=False)
 
 
 def test_too_many_kz_keeps_simt(cuda):
@@ -121,10 +142,10 @@ def test_too_many_kz_keeps_simt(cuda):
     _both(s, (16, 16, 256), [s.positions], expect_tc=False, sigma=2.0, qcut=50.0)
 
 
-def test_tc_batched_frames(cuda):
+def test_tc_batched_frames(cuda, zmode):
     s = cubic_system(5000, 40.0, seed=19, jitter=0.5, nframes=3)
     frames = [s.frame(k) for k in range(3)]
-    _both(s, (32, 32, 32), frames, sigma=2.0, qcut=0.6, max_frames=3)
+    _both(s, (32, 32, 32), frames, sigma=2.0, qcut=0.6, max_frames=3, zmode=zmode, expect_wide=True)
 
 
 # -- y-axis DFT -------------------------------------------------------------
