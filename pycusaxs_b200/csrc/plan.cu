@@ -112,7 +112,7 @@ struct DevArgs {
   const float *ff;    // [T][9]
   const float *twz_sum; // [2*nkzp]: sum over z < ez of the z twiddles (re, im)
   const float *twz_tc;  // [2][tcK x tcN]: z twiddles as TF32 head / remainder, K-major
-  const float *twz_tcw; // the same with twN columns (wide tiles)
+  const float *twz_tcw; // [tcK x 2*twN]: head and remainder side by side (wide tiles)
   const int4 *home_x; // per spread tile along x: home tiles whose atoms reach it (-1 padded)
   const int4 *home_y;
   const int4 *home_yw; // per 16-row y tile: up to eight home tiles (two int4, -1 padded)
@@ -1112,17 +1112,25 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_spread_zdft_tc(DevArgs a, int
 // accumulated in shared memory as [m][z] rows of twRS floats (twRS = tcR + 4, so
 // that 8 consecutive rows of 16-byte loads and the 16 taps of one atom fall in
 // distinct banks), then split into the TF32 head and remainder straight into
-// tensor memory, where the MMAs read A.  Tensor memory (512 columns):
-//   [0, 256)    A: kTwSlots chunks of kTwChunk z (K <= 128), head in the first
-//               32 columns of a chunk, remainder in the next 32
-//   [256, 512)  two accumulator stages of up to 128 columns (N <= 128)
+// tensor memory, where the MMAs read A.
+// A tf32 MMA costs about the same up to N = 192 (it is bound by its issue and
+// accumulator latency, not by its N), so B holds the twiddle head and
+// remainder side by side, B' = [Bh | Bl] (N' = 2*twN), and one k step is two
+// MMAs, D += Ah * B' and D += Al * B', where three were needed with separate
+// operands; the epilogue adds the two halves of D:
+// D[:, n] + D[:, twN + n] = (Ah + Al)(Bh + Bl), all four products.
+// Tensor memory (512 columns):
+//   [0, 256)    A ring: kTwRing slots of kTwChunk z, head in the first 32
+//               columns of a slot, remainder in the next 32
+//   [256, 512)  two accumulator stages of 2*twN <= 128 columns
 constexpr int kTwX = 8, kTwY = 16;  // wide tile: x-columns, y-rows (M = 128)
 constexpr int kTwProducerWarps = 24;
 constexpr int kTwMmaWarp = kTwProducerWarps;
 constexpr int kTwLoaderWarp = kTwProducerWarps + 1;
-constexpr int kTwThreads = 32 * (kTwProducerWarps + 6);  // producers, MMA, loader, 4 epilogue warps
-constexpr int kTwSlots = 4;  // A chunks in tensor memory
-constexpr int kTwChunk = 32; // z per chunk
+constexpr int kTwReleaseWarp = kTwProducerWarps + 6;
+constexpr int kTwThreads = 32 * (kTwProducerWarps + 7);  // producers, MMA, loader, 4 epilogue, release
+constexpr int kTwChunk = 32; // z per A ring slot
+constexpr int kTwRing = 4;   // A ring slots
 
 // Record ranges of an item's home bins (up to 4 along x times 8 along y).
 struct TileAtomsW {
@@ -1256,42 +1264,46 @@ __device__ __forceinline__ void spread_taps_w(const AtomTab &tab, int nv, int nt
 // Persistent, warp-specialized like k_spread_zdft_tc; grid = min(work items,
 // SMs), block kTwThreads.  Work items w = ((f*T + t)*stw + ty)*stiles[0] + tx.
 //   producer warps: twG groups on alternate items, each with its own FP32 tile
-//               and atom table: pre-pass and shared-memory taps into the tile,
-//               then the split: warp q (mod 4) of a group converts rows
-//               32q..32q+31 of 16-z units (tile - mean -> TF32 head and
-//               remainder) into tensor-memory A chunk c with tcgen05.st and
-//               zeroes what it read; the split of item j starts once the MMAs
-//               of item j-1 are complete
-//   MMA warp    one lane issues per A chunk 3 x (kTwChunk/8) MMAs with A from
-//               tensor memory (M = 128, N = twN, K = 8) into the item's
+//               and atom table: pre-pass and shared-memory taps into the
+//               tile, then the split, chunk by chunk of kTwChunk z: chunk q
+//               (q = j*CH + c over the CTA's items j) goes to ring slot
+//               q % kTwRing once the MMAs of chunk q - kTwRing are complete;
+//               warp q (mod 4) with rank h < 2 among the group's warps of that
+//               lane quarter converts rows 32q..32q+31, z in [32c + 16h, +16)
+//               (tile - mean -> TF32 head and remainder) with tcgen05.st and
+//               zeroes what it read
+//   MMA warp    one lane issues per chunk 2 x (kTwChunk/8) MMAs with A from
+//               tensor memory (M = 128, N = 2*twN, K = 8) into the item's
 //               accumulator stage, chunk by chunk as the split delivers them
 //   loader warp home-bin record ranges (up to 32 bins), item data, bulk copies
-//   4 epilogue  accumulator -> Z (lane m = column 16*lx + ly)
+//   4 epilogue  accumulator halves summed -> Z (lane m = column 16*lx + ly)
+//   release     one lane waits for the MMA completion of every chunk in order
+//               and publishes the count of completed chunks (`released`)
 // Hand-offs (mbarriers, every wait bounded):
 //   rec_full[b] / rec_empty[b]   loader <-> producers, record slot b
-//   a_full[c]                    8 split units (4 lane quarters x 2) -> MMA
-//   acc_full[d]                  MMA commit -> epilogue, and -> producers
-//                                (A chunks free for the next item)
-//   acc_empty[d]                 epilogue -> MMA, stage d
-// Every waiter observes each phase of a barrier it waits on in order, never two
-// phases ahead (parity waits cannot tell those apart): a producer group waits
-// for the completion of every item before its own (G = 1) or of the other
-// group's items (G = 2), which alternate on acc_full[d] with d = item & 1.
-// Dynamic shared memory: Bh, Bl (tcK x tcN floats each), twG tiles of 128 x twRS
+//   a_full[s]                    8 split units (4 lane quarters x 2) -> MMA
+//   a_empty[s]                   MMA commit -> release lane
+//   released                     release lane -> split warps (a counter)
+//   acc_full[d] / acc_empty[d]   MMA commit -> epilogue -> MMA, stage d
+// Each mbarrier has waiters that observe every one of its phases in order and
+// can neither fall two phases behind nor run two ahead (parity waits cannot
+// tell those apart); the ring slots, filled by both groups, are handed back
+// through the monotonic counter instead.
+// Dynamic shared memory: B' (tcK x 2*twN floats), twG tiles of 128 x twRS
 // floats, two record buffers of twRB float4, the home-bin tables (stiles[0] +
 // 2*stw int4) and twG atom tables of twCap entries.
 __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, int items) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ TwSlot slot[2];
-  __shared__ __align__(8) uint64_t bars[4 + kTwSlots + 4];
+  __shared__ __align__(8) uint64_t bars[4 + 2 * kTwRing + 4];
   __shared__ uint32_t tmem_slot;
   __shared__ volatile int abort_flag;
-  const int N = a.twN, KT = a.tcK, R = a.tcR, RB = a.twRB, RS = a.twRS, G = a.twG;
+  __shared__ volatile int released;
+  const int NB = a.twN, N = 2 * a.twN, KT = a.tcK, R = a.tcR, RB = a.twRB, RS = a.twRS, G = a.twG;
   const int CH = (KT + kTwChunk - 1) / kTwChunk;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  float *bh = reinterpret_cast<float *>(smem);
-  float *bl = bh + KT * N;
-  float *tiles = bl + KT * N;
+  float *bh = reinterpret_cast<float *>(smem);  // B' = [Bh | Bl], K-major, N columns
+  float *tiles = bh + KT * N;
   float4 *recs = reinterpret_cast<float4 *>(tiles + static_cast<size_t>(G) * 128 * RS);
   int4 *home_x = reinterpret_cast<int4 *>(recs + 2 * RB);
   int4 *home_y = home_x + a.stiles[0];
@@ -1307,12 +1319,12 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
   tab.zo = reinterpret_cast<int4 *>(tab.wz + cap);
   tab.lx = reinterpret_cast<int *>(tab.zo + cap);
   tab.ly = tab.lx + cap;
-  uint64_t *rec_full = bars, *rec_empty = bars + 2, *a_full = bars + 4, *acc_full = bars + 4 + kTwSlots,
-           *acc_empty = acc_full + 2;
+  uint64_t *rec_full = bars, *rec_empty = bars + 2, *a_full = bars + 4, *a_empty = bars + 4 + kTwRing,
+           *acc_full = bars + 4 + 2 * kTwRing, *acc_empty = acc_full + 2;
   {
     const float4 *src = reinterpret_cast<const float4 *>(a.twz_tcw);
     float4 *dst = reinterpret_cast<float4 *>(bh);
-    for (int i = tid; i < KT * N / 2; i += blockDim.x) dst[i] = src[i];
+    for (int i = tid; i < KT * N / 4; i += blockDim.x) dst[i] = src[i];
     float4 *t4 = reinterpret_cast<float4 *>(tiles);
     for (int i = tid; i < G * 32 * RS; i += blockDim.x) t4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     for (int i = tid; i < a.stiles[0]; i += blockDim.x) home_x[i] = a.home_x[i];
@@ -1325,14 +1337,15 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
   }
   if (tid == 0) {
-    for (int i = 0; i < 4 + kTwSlots + 4; ++i) {
+    for (int i = 0; i < 4 + 2 * kTwRing + 4; ++i) {
       int cnt = 1;
-      if (i >= 4 && i < 4 + kTwSlots) cnt = 8;  // a_full: 4 lane quarters x 2 units
-      if (i >= 4 + kTwSlots + 2) cnt = 4;       // acc_empty: 4 epilogue warps
+      if (i >= 4 && i < 4 + kTwRing) cnt = 8;  // a_full: 4 lane quarters x 2 units
+      if (i >= 4 + 2 * kTwRing + 2) cnt = 4;   // acc_empty: 4 epilogue warps
       asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&bars[i])), "r"(cnt));
     }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     abort_flag = 0;
+    released = 0;
   }
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -1347,12 +1360,24 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
       atomicExch(a.status, 1);
     }
   };
+  // bounded wait until the MMAs of the first `n` chunks are complete
+  auto wait_released = [&](int n) {
+    const uint64_t t0 = global_ns();
+    while (released < n && !abort_flag) {
+      if (global_ns() - t0 > 2000000000ull) {
+        abort_flag = 1;
+        atomicExch(a.status, 1);
+      }
+      __nanosleep(64);
+    }
+    __threadfence_block();
+  };
 
   if (warp < kTwProducerWarps) {
     const int bar_id = 1 + group;
     float *A = tiles + static_cast<size_t>(group) * 128 * RS;
     const int gw = warp - group * gwarps;          // warp within the group (groups start at multiples of 4)
-    const int quarter = warp & 3, wpq = gwarps / 4, rq = gw >> 2;
+    const int quarter = warp & 3, rq = gw >> 2;
     const int m = 32 * quarter + lane;             // the tile row this lane splits
     float *row = A + static_cast<size_t>(m) * RS;
     for (int j = group, w = blockIdx.x + group * gridDim.x; w < items; j += G, w += G * gridDim.x) {
@@ -1380,13 +1405,14 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
         const int mm = i / ((R - KT) / 4), zq = i % ((R - KT) / 4);
         reinterpret_cast<float4 *>(A + static_cast<size_t>(mm) * RS + KT)[zq] = make_float4(0.f, 0.f, 0.f, 0.f);
       }
-      // the A chunks are free once the MMAs of the previous item are complete
-      if (j >= 1) wait(&acc_full[(j - 1) & 1], (j - 1) >> 1);
-      __syncwarp();  // converged for the .sync.aligned tensor-memory stores
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      // split units: unit u = 2*c + h covers z in [32c + 16h, +16) of chunk c
-      for (int u = rq; u < 2 * CH; u += wpq) {
-        const int c = u >> 1, h = u & 1;
+      // split, chunk by chunk through the A ring
+      for (int c = 0; c < CH; ++c) {
+        const int q = j * CH + c, s = q % kTwRing;
+        if (rq >= 2) break;  // not a split warp
+        if (q >= kTwRing) wait_released(q - kTwRing + 1);
+        __syncwarp();  // converged for the .sync.aligned tensor-memory stores
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const int h = rq;
         // two halves of 8 z: head to the slot's first 32 columns, remainder to the next 32
 #pragma unroll
         for (int sub = 0; sub < 2; ++sub) {
@@ -1413,7 +1439,7 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
             }
           }
           const uint32_t dst = tmem + (static_cast<uint32_t>(32 * quarter) << 16) +
-                               static_cast<uint32_t>(64 * c + 16 * h + 8 * sub);
+                               static_cast<uint32_t>(64 * s + 16 * h + 8 * sub);
           asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"r"(dst),
                        "r"(hi[0]), "r"(hi[1]), "r"(hi[2]), "r"(hi[3]), "r"(hi[4]), "r"(hi[5]), "r"(hi[6]),
                        "r"(hi[7])
@@ -1426,17 +1452,16 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
         asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         __syncwarp();
-        if (lane == 0) mbar_arrive(smem_addr(&a_full[c]));
+        if (lane == 0) mbar_arrive(smem_addr(&a_full[s]));
       }
     }
   } else if (warp == kTwMmaWarp) {
     if (lane == 0) {
-      // kind::tf32, D f32, A from tensor memory, B K-major, N >> 3 at bit 17, M = 128
+      // kind::tf32, D f32, A from tensor memory, B' K-major, N >> 3 at bit 17, M = 128
       const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) |
                              (static_cast<uint32_t>(N >> 3) << 17) | (static_cast<uint32_t>(128 >> 4) << 24);
-      const uint64_t dbh0 = umma_desc(smem_addr(bh), N * 16, 128);
-      const uint64_t dbl0 = umma_desc(smem_addr(bl), N * 16, 128);
-      const uint64_t bstep = static_cast<uint64_t>(N) * 2;  // 8 z of B in 16-byte units
+      const uint64_t db0 = umma_desc(smem_addr(bh), N * 16, 128);
+      const uint64_t bstep = static_cast<uint64_t>(N) * 2;  // 8 z of B' in 16-byte units
       int j = 0;
       uint32_t last_bar = 0;
       int last_parity = 0;
@@ -1444,18 +1469,21 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
         const int d = j & 1;
         const uint32_t dcol = tmem + 256u + static_cast<uint32_t>(128 * d);
         for (int c = 0; c < CH; ++c) {
-          wait(&a_full[c], j);
+          const int q = j * CH + c, s = q % kTwRing;
+          wait(&a_full[s], q / kTwRing);
           if (c == 0 && j >= 2) wait(&acc_empty[d], (j - 2) >> 1);
           if (abort_flag) break;
           asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
           const int ks = min(kTwChunk, KT - kTwChunk * c) / 8;
           for (int kk = 0; kk < ks; ++kk) {
-            const uint32_t ahi = tmem + static_cast<uint32_t>(64 * c + 8 * kk);
-            const uint64_t zb = static_cast<uint64_t>(kTwChunk / 8 * c + kk);
-            umma_tf32_ts(dcol, ahi + 32, dbh0 + zb * bstep, idesc, (c | kk) ? 1u : 0u);
-            umma_tf32_ts(dcol, ahi, dbl0 + zb * bstep, idesc, 1u);
-            umma_tf32_ts(dcol, ahi, dbh0 + zb * bstep, idesc, 1u);
+            const uint32_t ahi = tmem + static_cast<uint32_t>(64 * s + 8 * kk);
+            const uint64_t db = db0 + static_cast<uint64_t>(kTwChunk / 8 * c + kk) * bstep;
+            umma_tf32_ts(dcol, ahi + 32, db, idesc, (c | kk) ? 1u : 0u);
+            umma_tf32_ts(dcol, ahi, db, idesc, 1u);
           }
+          asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                           smem_addr(&a_empty[s]))
+                       : "memory");
         }
         if (abort_flag) break;
         asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
@@ -1515,6 +1543,18 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
         }
       }
     }
+  } else if (warp == kTwReleaseWarp) {
+    if (lane == 0) {
+      const int mine = items > static_cast<int>(blockIdx.x)
+                           ? (items - 1 - static_cast<int>(blockIdx.x)) / static_cast<int>(gridDim.x) + 1
+                           : 0;
+      for (int q = 0; q < mine * CH && !abort_flag; ++q) {
+        wait(&a_empty[q % kTwRing], q / kTwRing);
+        if (abort_flag) break;
+        __threadfence_block();
+        released = q + 1;
+      }
+    }
   } else {
     const int quarter = warp & 3;
     ItemIter it;
@@ -1533,19 +1573,25 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
       const int64_t cell = static_cast<int64_t>(x0 + lx) * a.ext[1] + (y0 + ly);
       const uint32_t lane_base = tmem + (static_cast<uint32_t>(32 * quarter) << 16) + 256u +
                                  static_cast<uint32_t>(128 * d);
-      for (int c0 = 0; c0 < N; c0 += 8) {
-        uint32_t r[8];
+      for (int c0 = 0; c0 < NB; c0 += 8) {
+        uint32_t r[8], t[8];
         asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
                      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
                        "=r"(r[7])
                      : "r"(lane_base + c0));
+        asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                     : "=r"(t[0]), "=r"(t[1]), "=r"(t[2]), "=r"(t[3]), "=r"(t[4]), "=r"(t[5]), "=r"(t[6]),
+                       "=r"(t[7])
+                     : "r"(lane_base + NB + c0));
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
         if (valid) {
 #pragma unroll
           for (int jj = 0; jj < 4; ++jj) {
             const int kz = c0 / 2 + jj;
             if (kz < a.nkz)
-              Zft[kz * zplane + cell] = make_float2(__uint_as_float(r[2 * jj]), __uint_as_float(r[2 * jj + 1]));
+              Zft[kz * zplane + cell] =
+                  make_float2(__uint_as_float(r[2 * jj]) + __uint_as_float(t[2 * jj]),
+                              __uint_as_float(r[2 * jj + 1]) + __uint_as_float(t[2 * jj + 1]));
           }
         }
       }
@@ -2746,6 +2792,8 @@ struct SaxsPlan {
   int tc_ctas = 1, tcw_ctas = 1;
   bool tcn_ok = false, tcw_ok = false;  // z kernels the plan can run: 64- and 128-column tiles
   int twG_max = 1;                      // producer groups the wide kernel's shared memory allows
+  int tw_cap[2] = {0, 0}, tw_rb[2] = {0, 0};  // wide kernel atom table / record buffer, 1 or 2 groups
+  size_t tw_smem[2] = {0, 0};
   bool tc_ok = false, ytc_ok = false, xtc_ok = false;  // tensor-core kernels the plan can run
   bool use_ytc = false;  // y-axis DFT on the tensor cores (k_dft_tc<false>)
   bool use_xtc = false;  // x-axis DFT + post on the tensor cores (k_dft_tc<true>)
@@ -2759,6 +2807,14 @@ struct SaxsPlan {
 };
 
 namespace {
+
+// The wide kernel's producer groups with the table sizes planned for them.
+void set_wide_groups(SaxsPlan *pl, int g) {
+  pl->a.twG = g;
+  pl->a.twCap = pl->tw_cap[g - 1];
+  pl->a.twRB = pl->tw_rb[g - 1];
+  pl->smem_spread_tcw = pl->tw_smem[g - 1];
+}
 
 int optin_smem() {
   int dev = 0, v = 0;
@@ -3142,23 +3198,28 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
           }
     // wide tiles: twG FP32 tiles of 128 x (R + 4) floats; two producer groups
     // before larger record buffers and atom tables
-    int GW = 0, RBW = 0, CAPW = 0;
+    // wide tiles, for one and for two producer groups: the largest atom table
+    // (each table chunk costs a latency-bound pre-pass and two barriers), then
+    // the largest record buffer that fit beside the groups' FP32 tiles
     const int RSW = R + 4;
     const size_t home_w = static_cast<size_t>(a.stiles[0] + 2 * a.stw) * sizeof(int4);
     const size_t bw_bytes = 2 * static_cast<size_t>(KT) * NW * sizeof(float);
-    if (a.stw > 0 && NW <= 128 && KT <= kTwSlots * kTwChunk) {
+    auto wide_bytes = [&](int g, int rb, int cap) {
+      return bw_bytes + static_cast<size_t>(g) * 128 * RSW * sizeof(float) + 2 * static_cast<size_t>(rb) * 16 +
+             home_w + static_cast<size_t>(g) * cap * kTcAtomBytes;
+    };
+    int GW = 0;
+    if (a.stw > 0 && NW <= 64) {  // two accumulator stages of 2*NW columns
       const size_t avail_w = optin - static_smem(k_spread_zdft_tcw);
-      static const int cand[][2] = {{1024, 256}, {512, 256}, {512, 128}, {1024, 64},
-                                    {256, 128},  {256, 64},  {128, 64}};
-      for (int g = 2; g >= 1 && GW == 0; --g)
+      static const int cand[][2] = {{1024, 1024}, {1024, 512}, {512, 1024}, {512, 512}, {1024, 256},
+                                    {512, 256},   {256, 1024}, {256, 512},  {256, 256}, {128, 512},
+                                    {128, 256},   {128, 128},  {64, 128}};  // {cap, records}
+      for (int g = 1; g <= 2; ++g)
         for (const auto &c : cand)
-          if (GW == 0 && bw_bytes + static_cast<size_t>(g) * 128 * RSW * sizeof(float) +
-                                 2 * static_cast<size_t>(c[0]) * 16 + home_w +
-                                 static_cast<size_t>(g) * c[1] * kTcAtomBytes <=
-                             avail_w) {
+          if (pl->tw_cap[g - 1] == 0 && wide_bytes(g, c[1], c[0]) <= avail_w) {
+            pl->tw_cap[g - 1] = c[0];
+            pl->tw_rb[g - 1] = c[1];
             GW = g;
-            RBW = c[0];
-            CAPW = c[1];
           }
     }
     pl->tcn_ok = !simt_only && N <= 256 && S > 0;
@@ -3173,13 +3234,11 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
     if (pl->tcw_ok) {
       a.twN = NW;
       a.twRS = RSW;
-      a.twRB = RBW;
-      a.twCap = CAPW;
-      a.twG = GW;
       pl->twG_max = GW;
-      pl->smem_spread_tcw = bw_bytes + static_cast<size_t>(GW) * 128 * RSW * sizeof(float) +
-                            2 * static_cast<size_t>(RBW) * 16 + home_w +
-                            static_cast<size_t>(GW) * CAPW * kTcAtomBytes;
+      for (int g = 1; g <= GW; ++g) pl->tw_smem[g - 1] = wide_bytes(g, pl->tw_rb[g - 1], pl->tw_cap[g - 1]);
+      // one group by default: its larger atom table measured faster than two
+      // groups on the 100k-atom trajectory workload (2.95 vs 3.42 ms per 100 frames)
+      set_wide_groups(pl, 1);
     }
     if (pl->tcn_ok) {
       a.tcS = S;
@@ -3341,7 +3400,23 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
     return out;
   };
   const std::vector<float> twtc = pl->tcn_ok ? z_operand(a.tcN) : std::vector<float>();
-  const std::vector<float> twtcw = pl->tcw_ok ? z_operand(a.twN) : std::vector<float>();
+  // wide tiles: B' = [Bh | Bl] as one K-major operand of 2*twN columns
+  std::vector<float> twtcw;
+  if (pl->tcw_ok) {
+    const std::vector<float> hl = z_operand(a.twN);
+    const int NB = a.twN, N2 = 2 * a.twN;
+    const size_t half = static_cast<size_t>(a.tcK) * NB;
+    twtcw.assign(2 * half, 0.0f);
+    for (int z = 0; z < a.tcK; ++z)
+      for (int n = 0; n < NB; ++n) {
+        const size_t o = static_cast<size_t>(z / 4) * (NB / 8) * 32 + (n / 8) * 32 + (n % 8) * 4 + z % 4;
+        for (int part = 0; part < 2; ++part) {
+          const int n2 = n + part * NB;
+          const size_t o2 = static_cast<size_t>(z / 4) * (N2 / 8) * 32 + (n2 / 8) * 32 + (n2 % 8) * 4 + z % 4;
+          twtcw[o2] = hl[part * half + o];
+        }
+      }
+  }
   std::vector<float2> twy(static_cast<size_t>(ey) * a.nkyp, make_float2(0.f, 0.f));
   for (int y = 0; y < ey; ++y)
     for (int k = 0; k < a.nky; ++k)
@@ -4153,7 +4228,7 @@ int saxs_plan_set_config(SaxsPlan *pl, const SaxsPlanConfig *cfg) {
   pl->use_ytc = cfg->y_tensor_cores != 0;
   pl->use_xtc = cfg->x_tensor_cores != 0;
   if (wide)
-    pl->a.twG = cfg->z_producer_groups;
+    set_wide_groups(pl, cfg->z_producer_groups);
   else if (z)
     pl->a.tcG = cfg->z_producer_groups;
   return SAXS_OK;
