@@ -1188,13 +1188,18 @@ __device__ __forceinline__ void home_ranges_publish_w(TileAtomsW &ta, int s0, in
 }
 
 // Pre-pass for wide tiles: as spread_prepass, with z offsets that are plain z
-// rows of the [m][z] tile.
+// rows of the [m][z] tile, and only the atoms whose stencil reaches the tile
+// kept: each warp appends its reaching atoms to the table at *count (a
+// shared-memory counter that starts at 0).
 __device__ __forceinline__ void spread_prepass_w(const DevArgs &a, const TileAtomsW &ta, const float4 *srec,
                                                  int nrec_smem, int f, int v0, int nv, const AtomTab &tab,
-                                                 int x0, int y0, int cw, int ch, int tid, int nthreads) {
+                                                 int x0, int y0, int cw, int ch, int tid, int nthreads,
+                                                 int *count) {
   const int P = a.order, nt = a.ntaps, nz = a.n[2];
-  for (int i = tid; i < nv; i += nthreads) {
-    const int v = v0 + i;
+  const int lane = tid & 31;
+  for (int i0 = tid - lane; i0 < nv; i0 += nthreads) {
+    const int i = i0 + lane;
+    const int v = v0 + min(i, nv - 1);
     float4 q;
     if (v < nrec_smem) {
       q = srec[v];
@@ -1227,12 +1232,20 @@ __device__ __forceinline__ void spread_prepass_w(const DevArgs &a, const TileAto
       lyp |= by << (8 * o);
       zo[o] = zz;
     }
-    tab.wx[i] = make_float4(wx[0], wx[1], wx[2], wx[3]);
-    tab.wy[i] = make_float4(wy[0], wy[1], wy[2], wy[3]);
-    tab.wz[i] = make_float4(wz[0], wz[1], wz[2], wz[3]);
-    tab.zo[i] = make_int4(zo[0], zo[1], zo[2], zo[3]);
-    tab.lx[i] = lxp;
-    tab.ly[i] = lyp;
+    const bool reach = i < nv && lxp != -1 && lyp != -1;
+    const unsigned m = __ballot_sync(0xffffffffu, reach);
+    int base = 0;
+    if (lane == 0 && m) base = atomicAdd(count, __popc(m));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (reach) {
+      const int e = base + __popc(m & ((1u << lane) - 1u));
+      tab.wx[e] = make_float4(wx[0], wx[1], wx[2], wx[3]);
+      tab.wy[e] = make_float4(wy[0], wy[1], wy[2], wy[3]);
+      tab.wz[e] = make_float4(wz[0], wz[1], wz[2], wz[3]);
+      tab.zo[e] = make_int4(zo[0], zo[1], zo[2], zo[3]);
+      tab.lx[e] = lxp;
+      tab.ly[e] = lyp;
+    }
   }
 }
 
@@ -1299,6 +1312,7 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
   __shared__ uint32_t tmem_slot;
   __shared__ volatile int abort_flag;
   __shared__ volatile int released;
+  __shared__ int tab_count[2][2];  // reaching atoms in the table: [group][chunk parity]
   const int NB = a.twN, N = 2 * a.twN, KT = a.tcK, R = a.tcR, RB = a.twRB, RS = a.twRS, G = a.twG;
   const int CH = (KT + kTwChunk - 1) / kTwChunk;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -1346,6 +1360,7 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     abort_flag = 0;
     released = 0;
+    tab_count[0][0] = tab_count[0][1] = tab_count[1][0] = tab_count[1][1] = 0;
   }
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -1389,16 +1404,21 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
       if (!skip) {
         const int nvis = sl.ta.cum[sl.ta.nb];
         const int nrec = min(nvis, RB);
-        for (int v0 = 0; v0 < nvis; v0 += cap) {
+        // chunk k of the visible atoms counts its reaching atoms in
+        // tab_count[group][k & 1]; the other counter is cleared meanwhile (its
+        // readers passed the barrier at the top of this chunk)
+        for (int v0 = 0, k = 0; v0 < nvis; v0 += cap, ++k) {
           const int nv = min(cap, nvis - v0);
           if (v0 > 0) producers_sync(bar_id, gthreads);
+          if (gtid == 0 && k > 0) tab_count[group][(k + 1) & 1] = 0;
           spread_prepass_w(a, sl.ta, recs + static_cast<size_t>(b) * RB, nrec, sl.f, v0, nv, tab, sl.x0, sl.y0,
-                           sl.cw, sl.ch, gtid, gthreads);
+                           sl.cw, sl.ch, gtid, gthreads, &tab_count[group][k & 1]);
           producers_sync(bar_id, gthreads);
-          spread_taps_w(tab, nv, a.ntaps, A, RS, gtid, gthreads);
+          spread_taps_w(tab, tab_count[group][k & 1], a.ntaps, A, RS, gtid, gthreads);
         }
       }
       producers_sync(bar_id, gthreads);
+      if (gtid == 0) tab_count[group][0] = tab_count[group][1] = 0;  // for the next item
       if (gtid == 0) mbar_arrive(smem_addr(&rec_empty[b]));
       // rows z in [tcK, tcR) meet no twiddle: cleared for the next item
       for (int i = gtid; i < 128 * ((R - KT) / 4); i += gthreads) {
