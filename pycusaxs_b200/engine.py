@@ -289,8 +289,12 @@ class SaxsEngine:
         copied straight to the device; anything else goes through a pinned
         staging buffer first.  Host-to-device copies run on a copy stream,
         double-buffered against the compute stream, in sub-batches of ``chunk``
-        frames (default: a quarter of the call's frames, at most max_frames) so
-        that the copy of one sub-batch overlaps the kernels of the previous one.
+        frames (default: a tenth of the call's frames, at least 4, at most
+        max_frames) so that the copy of one sub-batch overlaps the kernels of
+        the previous one.  On a B200 (43 GB/s pinned host-to-device) with 100
+        frames of 100k atoms per call, tenths measured 5.7 ms per call against
+        6.5 ms for quarters and 6.7 ms for one copy: the first sub-batch's copy
+        is not overlapped, and every sub-batch pays its launches' ramp-up.
         """
         torch = self._torch
         pinned = isinstance(xyz, torch.Tensor) and xyz.device.type == "cpu" and xyz.is_pinned()
@@ -313,7 +317,7 @@ class SaxsEngine:
             raise ValueError("positions must have shape (B, natoms, 3)")
         st = self._staging_buffers(x.shape[1])
         B = self.max_frames
-        step = min(B, max(1, -(-nf // 4))) if chunk is None else max(1, min(B, int(chunk)))
+        step = min(B, max(4, -(-nf // 10))) if chunk is None else max(1, min(B, int(chunk)))
         for s in range(0, nf, step):
             e = min(nf, s + step)
             slot = st["next"]
