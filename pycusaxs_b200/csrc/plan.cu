@@ -1796,6 +1796,7 @@ __global__ void __launch_bounds__(dtc_threads<kX>(), 1)
   __shared__ uint32_t tmem_slot;
   __shared__ volatile int abort_flag;
   const int N = sh.N, NS = sh.S, NC = sh.chunks;
+  const int ND = sh.merged ? sh.ND : 2;              // accumulator stages
   const int NM = sh.merged ? 2 * N : N;              // MMA N and accumulator stage width
   const int a_col0 = sh.merged ? sh.ND * NM : 2 * N; // first A column of tensor memory
   const int KP = 2 * kDtcChunk;                      // K' per chunk
@@ -1918,8 +1919,8 @@ __global__ void __launch_bounds__(dtc_threads<kX>(), 1)
       uint32_t last_bar = 0;
       int last_parity = 0;
       for (int w = blockIdx.x; w < items && !abort_flag; w += gridDim.x, ++i) {
-        const int d = i & 1;
-        if (i >= 2) wait(&dempty[d], (i - 2) >> 1);
+        const int d = i % ND;  // accumulator stage
+        if (i >= ND) wait(&dempty[d], (i - ND) / ND);
         const uint32_t dcol = tmem + static_cast<uint32_t>(d * NM);
         for (int c = 0; c < NC; ++c, ++g) {
           const int st = g % NS;
@@ -1973,8 +1974,8 @@ __global__ void __launch_bounds__(dtc_threads<kX>(), 1)
     const int r = 32 * quarter + lane;
     int i = 0;
     for (int w = blockIdx.x; w < items; w += gridDim.x, ++i) {
-      const int d = i & 1;
-      wait(&dfull[d], i >> 1);
+      const int d = i % ND;
+      wait(&dfull[d], i / ND);
       if (__any_sync(0xffffffffu, abort_flag != 0)) break;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const uint32_t lane_base = tmem + (static_cast<uint32_t>(32 * quarter) << 16) + static_cast<uint32_t>(d * NM);

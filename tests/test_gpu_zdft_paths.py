@@ -186,6 +186,29 @@ def test_ytc_batched_frames(cuda):
     _both(s, (32, 32, 32), frames, axis="y", sigma=2.0, qcut=0.6, max_frames=3)
 
 
+@pytest.mark.parametrize("axis", ["y", "x"])
+def test_yx_tc_many_items_per_cta(cuda, axis):
+    # 4 frames at grid 128: several hundred items, so every CTA of the persistent
+    # y/x kernels processes more than one item and reuses its accumulator and
+    # operand stages (one-frame cases give each CTA at most one item)
+    s = cubic_system(20_000, 100.0, seed=28, jitter=0.4, nframes=4)
+    frames = [s.frame(k) for k in range(4)]
+    var, bit = _AXES[axis]
+    kw = dict(sigma=2.0, qcut=0.5, bin_size=0.002, max_frames=4)
+    with dft_mode(var, None):
+        h_tc, n_tc, e = engine_hist(s, (128, 128, 128), frames, **kw)
+        assert e.info.path & bit
+        e.close()
+    with dft_mode(var, "simt"):
+        h_s, n_s, e = engine_hist(s, (128, 128, 128), frames, **kw)
+        e.close()
+    np.testing.assert_array_equal(n_tc, n_s)
+    sel = n_s > 0
+    sel[0] = False
+    diff = np.abs(h_tc[sel] - h_s[sel]) / np.abs(h_s[sel])
+    assert diff.max() <= TC_VS_SIMT_RTOL, diff.max()
+
+
 # -- x-axis DFT (with form factors, type sum and moduli) --------------------
 
 
