@@ -1734,16 +1734,10 @@ template <bool kX>
 __host__ __device__ constexpr int dtc_threads() { return 32 * (kDtcProducerWarps + 2 + dtc_epi_warps<kX>()); }
 constexpr int kDtcMaxStages = 4;
 
-// One pass's GEMM shape: N', K chunks, stages, TMEM columns, B' table.  With
-// `merged` the head and remainder of B' sit side by side as one operand of
-// 2N' columns (a tf32 MMA costs about the same up to N = 192, so a k step is
-// two MMAs, D += Ah [Bh|Bl] and D += Al [Bh|Bl], instead of three), with ND
-// accumulator stages of 2N' columns; the epilogue adds the two halves of D.
+// One pass's GEMM shape: N', K chunks, stages, TMEM columns, B' table.
 struct DtcShape {
   int N, chunks, S, cols;
-  int merged, ND;
-  const float *B;  // [chunk]: head block then remainder block (N' x 2*kDtcChunk
-                   // each), or one block of 2N' x 2*kDtcChunk when merged
+  const float *B;  // [chunk][2][N' x 2*kDtcChunk]: head block then remainder block
 };
 
 // Tensor copy of chunk c of item w's 128 rows into `dst`, 1024-byte aligned
@@ -1787,7 +1781,7 @@ __device__ __forceinline__ void dtc_tensor_copy(const DevArgs &a, const CUtensor
 // Dynamic shared memory: S stages of { raw A rows (128 x K'), B' head, B'
 // remainder (N' x K') } floats, 1024-byte aligned.  Tensor memory (512
 // columns): accumulators d at columns d*N', A stage st at 2N' + 64*st (head) and
-// + 32 (remainder); merged: accumulators d at d*2N', A stages from ND*2N'.
+// + 32 (remainder).
 template <bool kX>
 __global__ void __launch_bounds__(dtc_threads<kX>(), 1)
     k_dft_tc(DevArgs a, DtcShape sh, const __grid_constant__ CUtensorMap amap, int items) {
@@ -1796,9 +1790,6 @@ __global__ void __launch_bounds__(dtc_threads<kX>(), 1)
   __shared__ uint32_t tmem_slot;
   __shared__ volatile int abort_flag;
   const int N = sh.N, NS = sh.S, NC = sh.chunks;
-  const int ND = sh.merged ? sh.ND : 2;              // accumulator stages
-  const int NM = sh.merged ? 2 * N : N;              // MMA N and accumulator stage width
-  const int a_col0 = sh.merged ? sh.ND * NM : 2 * N; // first A column of tensor memory
   const int KP = 2 * kDtcChunk;                      // K' per chunk
   const int a_floats = 128 * KP, b_floats = N * KP;  // raw A tile; B' head or remainder
   const int stage_floats = a_floats + 2 * b_floats;
@@ -1870,7 +1861,7 @@ __global__ void __launch_bounds__(dtc_threads<kX>(), 1)
             lo[4 * jj + e] = __float_as_uint(vv[e] - h);
           }
         }
-        const uint32_t col = tmem + lane_off + static_cast<uint32_t>(a_col0 + 64 * st + 16 * half);
+        const uint32_t col = tmem + lane_off + static_cast<uint32_t>(2 * N + 64 * st + 16 * half);
         asm volatile(
             "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], "
             "{%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(col),
@@ -1914,14 +1905,14 @@ __global__ void __launch_bounds__(dtc_threads<kX>(), 1)
     if (lane == 0) {
       // kind::tf32: D f32, A and B tf32, both K-major, N >> 3 at bit 17, M = 128
       const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) |
-                             (static_cast<uint32_t>(NM >> 3) << 17) | (static_cast<uint32_t>(128 >> 4) << 24);
+                             (static_cast<uint32_t>(N >> 3) << 17) | (static_cast<uint32_t>(128 >> 4) << 24);
       int g = 0, i = 0;
       uint32_t last_bar = 0;
       int last_parity = 0;
       for (int w = blockIdx.x; w < items && !abort_flag; w += gridDim.x, ++i) {
-        const int d = i % ND;  // accumulator stage
-        if (i >= ND) wait(&dempty[d], (i - ND) / ND);
-        const uint32_t dcol = tmem + static_cast<uint32_t>(d * NM);
+        const int d = i & 1;
+        if (i >= 2) wait(&dempty[d], (i - 2) >> 1);
+        const uint32_t dcol = tmem + static_cast<uint32_t>(d * N);
         for (int c = 0; c < NC; ++c, ++g) {
           const int st = g % NS;
           wait(&bfull[st], g / NS);
@@ -1929,28 +1920,17 @@ __global__ void __launch_bounds__(dtc_threads<kX>(), 1)
           if (abort_flag) break;
           asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
           const float *sb = stages + static_cast<size_t>(st) * stage_floats;
-          const uint32_t ah0 = tmem + static_cast<uint32_t>(a_col0 + 64 * st);
-          if (sh.merged) {
-            // one k step (8 of K'): A advances 8 TMEM columns, B' 2N*32 B
-            const uint64_t db0 = umma_desc(smem_addr(sb + a_floats), NM * 16, 128);
-            for (int kk = 0; kk < KP / 8; ++kk) {
-              const uint32_t ah = ah0 + 8 * kk, al = ah + 32;
-              const uint64_t db = db0 + static_cast<uint64_t>(kk * 2 * NM);
-              umma_tf32_ts(dcol, al, db, idesc, (c > 0 || kk > 0) ? 1u : 0u);
-              umma_tf32_ts(dcol, ah, db, idesc, 1u);
-            }
-          } else {
-            const uint64_t dbh0 = umma_desc(smem_addr(sb + a_floats), N * 16, 128);
-            const uint64_t dbl0 = umma_desc(smem_addr(sb + a_floats + b_floats), N * 16, 128);
-            // one k step (8 of K'): A advances 8 TMEM columns, B' N*32 B (+N*2)
-            for (int kk = 0; kk < KP / 8; ++kk) {
-              const uint32_t ah = ah0 + 8 * kk, al = ah + 32;
-              const uint64_t dbh = dbh0 + static_cast<uint64_t>(kk * 2 * N);
-              const uint64_t dbl = dbl0 + static_cast<uint64_t>(kk * 2 * N);
-              umma_tf32_ts(dcol, al, dbh, idesc, (c > 0 || kk > 0) ? 1u : 0u);
-              umma_tf32_ts(dcol, ah, dbl, idesc, 1u);
-              umma_tf32_ts(dcol, ah, dbh, idesc, 1u);
-            }
+          const uint64_t dbh0 = umma_desc(smem_addr(sb + a_floats), N * 16, 128);
+          const uint64_t dbl0 = umma_desc(smem_addr(sb + a_floats + b_floats), N * 16, 128);
+          const uint32_t ah0 = tmem + static_cast<uint32_t>(2 * N + 64 * st);
+          // one k step (8 of K'): A advances 8 TMEM columns, B' N*32 B (+N*2)
+          for (int kk = 0; kk < KP / 8; ++kk) {
+            const uint32_t ah = ah0 + 8 * kk, al = ah + 32;
+            const uint64_t dbh = dbh0 + static_cast<uint64_t>(kk * 2 * N);
+            const uint64_t dbl = dbl0 + static_cast<uint64_t>(kk * 2 * N);
+            umma_tf32_ts(dcol, al, dbh, idesc, (c > 0 || kk > 0) ? 1u : 0u);
+            umma_tf32_ts(dcol, ah, dbl, idesc, 1u);
+            umma_tf32_ts(dcol, ah, dbh, idesc, 1u);
           }
           asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                            smem_addr(&empty[st]))
@@ -1974,34 +1954,11 @@ __global__ void __launch_bounds__(dtc_threads<kX>(), 1)
     const int r = 32 * quarter + lane;
     int i = 0;
     for (int w = blockIdx.x; w < items; w += gridDim.x, ++i) {
-      const int d = i % ND;
-      wait(&dfull[d], i / ND);
+      const int d = i & 1;
+      wait(&dfull[d], i >> 1);
       if (__any_sync(0xffffffffu, abort_flag != 0)) break;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const uint32_t lane_base = tmem + (static_cast<uint32_t>(32 * quarter) << 16) + static_cast<uint32_t>(d * NM);
-      // 16 accumulator columns from c0: with a merged B' the sum of both halves
-      auto load16 = [&](int c0, uint32_t v[16]) {
-        asm volatile(
-            "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-            "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-              "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-            : "r"(lane_base + c0));
-        if (sh.merged) {
-          uint32_t t[16];
-          asm volatile(
-              "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-              "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-              : "=r"(t[0]), "=r"(t[1]), "=r"(t[2]), "=r"(t[3]), "=r"(t[4]), "=r"(t[5]), "=r"(t[6]), "=r"(t[7]),
-                "=r"(t[8]), "=r"(t[9]), "=r"(t[10]), "=r"(t[11]), "=r"(t[12]), "=r"(t[13]), "=r"(t[14]), "=r"(t[15])
-              : "r"(lane_base + N + c0));
-          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-          for (int q = 0; q < 16; ++q) v[q] = __float_as_uint(__uint_as_float(v[q]) + __uint_as_float(t[q]));
-        } else {
-          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        }
-      };
+      const uint32_t lane_base = tmem + (static_cast<uint32_t>(32 * quarter) << 16) + static_cast<uint32_t>(d * N);
       if (!kX) {
         const int ex = a.ext[0];
         const int xblocks = (ex + 127) / 128;
@@ -2010,7 +1967,14 @@ __global__ void __launch_bounds__(dtc_threads<kX>(), 1)
         float2 *Yp = a.Y + plane * a.nky * ex;
         for (int c0 = 16 * eslot; c0 < N; c0 += 16 * EQ) {
           uint32_t v[16];
-          load16(c0, v);
+          asm volatile(
+              "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+              "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+              : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+                "=r"(v[14]), "=r"(v[15])
+              : "r"(lane_base + c0));
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
           if (x < ex) {
 #pragma unroll
             for (int jj = 0; jj < 8; ++jj) {
@@ -2041,7 +2005,14 @@ __global__ void __launch_bounds__(dtc_threads<kX>(), 1)
         float *ib = a.ibox + ((static_cast<int64_t>(f) * a.nkz + kz) * a.nky + ky) * a.nkx;
         for (int c0 = 16 * eslot; c0 < N; c0 += 16 * EQ) {
           uint32_t v[16];
-          load16(c0, v);
+          asm volatile(
+              "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+              "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+              : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+                "=r"(v[14]), "=r"(v[15])
+              : "r"(lane_base + c0));
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
           for (int jj = 0; jj < 8; ++jj) {
             const int kx = c0 / 2 + jj;
@@ -3010,27 +2981,8 @@ void destroy(SaxsPlan *pl) {
 bool dtc_shape(int nk, int extent, size_t avail, DtcShape *sh, size_t *smem) {
   const int N = round_up(2 * nk, 16);
   const size_t stage_bytes = (128 + 2 * static_cast<size_t>(N)) * 2 * kDtcChunk * sizeof(float);
-  const int S_smem = static_cast<int>((avail - 1024) / stage_bytes);
-  // tensor memory: two accumulators of N' columns and 64 columns of A per stage;
-  // merged B' (2N' <= 256): ND accumulators of 2N' columns.  PYCUSAXS_DTC=split
-  // keeps three MMAs per k step; PYCUSAXS_DTC_ND=1|2 sets ND.
-  const char *mode = std::getenv("PYCUSAXS_DTC");
-  const char *nd_env = std::getenv("PYCUSAXS_DTC_ND");
-  sh->merged = 0;
-  sh->ND = 2;
-  int S = std::min({kDtcMaxStages, S_smem, (512 - 2 * N) / 64});
-  if (!(mode && std::strcmp(mode, "split") == 0) && 2 * N <= 256) {
-    // one accumulator stage by default: it leaves tensor memory for four A
-    // stages, which measured faster on the y pass (0.59 vs 0.64 ms per 100
-    // frames of the 100k-atom workload; two stages: 0.70)
-    const int nd = nd_env ? std::atoi(nd_env) : 1;
-    const int Sm = std::min({kDtcMaxStages, S_smem, (512 - nd * 2 * N) / 64});
-    if ((nd == 1 || nd == 2) && Sm >= 2) {
-      sh->merged = 1;
-      sh->ND = nd;
-      S = Sm;
-    }
-  }
+  // tensor memory: two accumulators of N' columns and 64 columns of A per stage
+  const int S = std::min({kDtcMaxStages, static_cast<int>((avail - 1024) / stage_bytes), (512 - 2 * N) / 64});
   if (N > 256 || S < 2) return false;
   sh->N = N;
   sh->chunks = (extent + kDtcChunk - 1) / kDtcChunk;
@@ -3048,16 +3000,6 @@ std::vector<float> dtc_bprime(const std::vector<float2> &tw, int stride, int ext
   const int KP = 2 * kDtcChunk, Np = sh.N;
   const size_t blk = static_cast<size_t>(Np) * KP;
   std::vector<float> out(static_cast<size_t>(sh.chunks) * 2 * blk, 0.0f);
-  // element (n', k') of the head (part 0) or remainder (part 1) block of chunk c
-  auto at = [&](int c, int part, int np, int kp) {
-    if (sh.merged) {
-      const int n2 = np + part * Np, N2 = 2 * Np;
-      return static_cast<size_t>(c) * 2 * blk + static_cast<size_t>(kp / 4) * (N2 / 8) * 32 + (n2 / 8) * 32 +
-             (n2 % 8) * 4 + kp % 4;
-    }
-    return static_cast<size_t>(c) * 2 * blk + part * blk + static_cast<size_t>(kp / 4) * (Np / 8) * 32 +
-           (np / 8) * 32 + (np % 8) * 4 + kp % 4;
-  };
   for (int c = 0; c < sh.chunks; ++c)
     for (int uu = 0; uu < kDtcChunk; ++uu) {
       const int u = c * kDtcChunk + uu;
@@ -3074,8 +3016,10 @@ std::vector<float> dtc_bprime(const std::vector<float2> &tw, int stride, int ext
             bits &= 0xFFFFE000u;
             float head;
             std::memcpy(&head, &bits, sizeof(head));
-            out[at(c, 0, np, kp)] = head;
-            out[at(c, 1, np, kp)] = v - head;
+            const size_t o = static_cast<size_t>(c) * 2 * blk + static_cast<size_t>(kp / 4) * (Np / 8) * 32 +
+                             (np / 8) * 32 + (np % 8) * 4 + kp % 4;
+            out[o] = head;
+            out[o + blk] = v - head;
           }
       }
     }
