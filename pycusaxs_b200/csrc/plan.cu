@@ -1251,26 +1251,53 @@ __device__ __forceinline__ void spread_prepass_w(const DevArgs &a, const TileAto
 
 // Taps for wide tiles: one lane per (atom, y tap, z tap), four x taps each, into
 // the [m][z] tile (row stride rs, m = 16*lx + ly).  With rs = 4 (mod 32) the 16
-// lanes of an atom write banks 4*ly + z (mod 32), all distinct.
+// lanes of an atom write banks 4*ly + z (mod 32), all distinct.  Each thread
+// takes two units per round and reads both units' table entries before either
+// unit's atomics, so the shared-memory loads of one overlap the other.
+struct TapUnit {
+  float *col;     // tile row start of the unit's (y tap, z tap), or null when outside
+  int lxp;        // the atom's four x-tap columns, one byte each (0xFF outside)
+  float w;        // wy * wz
+  float4 wx;
+};
+
+__device__ __forceinline__ TapUnit tap_unit(const AtomTab &tab, int u, int nu, int nt, float *A, int rs) {
+  TapUnit t;
+  t.col = nullptr;
+  if (u >= nu) return t;
+  const int i = u >> 4, p = (u >> 2) & 3, r = u & 3;
+  if (p >= nt || r >= nt) return t;
+  const int ly = (tab.ly[i] >> (8 * p)) & 0xFF;
+  t.lxp = tab.lx[i];
+  if (ly == 0xFF || t.lxp == -1) return t;
+  const float wy = reinterpret_cast<const float *>(&tab.wy[i])[p];
+  const float wz = reinterpret_cast<const float *>(&tab.wz[i])[r];
+  const int zo = reinterpret_cast<const int *>(&tab.zo[i])[r];
+  t.wx = tab.wx[i];
+  t.w = wy * wz;
+  t.col = A + zo + ly * rs;
+  return t;
+}
+
+__device__ __forceinline__ void tap_apply(const TapUnit &t, int rs) {
+  if (!t.col) return;
+  const float wx[4] = {t.wx.x, t.wx.y, t.wx.z, t.wx.w};
+  const float wy_wz = t.w;
+#pragma unroll
+  for (int o = 0; o < 4; ++o) {
+    const int lx = (t.lxp >> (8 * o)) & 0xFF;
+    if (lx != 0xFF) atomicAdd(t.col + lx * kTwY * rs, wx[o] * wy_wz);
+  }
+}
+
 __device__ __forceinline__ void spread_taps_w(const AtomTab &tab, int nv, int nt, float *A, int rs, int tid,
                                               int nthreads) {
-  for (int u = tid; u < nv * 16; u += nthreads) {
-    const int i = u >> 4, p = (u >> 2) & 3, r = u & 3;
-    if (p >= nt || r >= nt) continue;
-    const int ly = (tab.ly[i] >> (8 * p)) & 0xFF;
-    const int lxp = tab.lx[i];
-    if (ly == 0xFF || lxp == -1) continue;
-    const float wy = reinterpret_cast<const float *>(&tab.wy[i])[p];
-    const float wz = reinterpret_cast<const float *>(&tab.wz[i])[r];
-    const int zo = reinterpret_cast<const int *>(&tab.zo[i])[r];
-    const float4 wx4 = tab.wx[i];
-    const float wx[4] = {wx4.x, wx4.y, wx4.z, wx4.w};
-    float *col = A + zo + ly * rs;
-#pragma unroll
-    for (int o = 0; o < 4; ++o) {
-      const int lx = (lxp >> (8 * o)) & 0xFF;
-      if (lx != 0xFF) atomicAdd(col + lx * kTwY * rs, (wx[o] * wy) * wz);
-    }
+  const int nu = nv * 16;
+  for (int u = tid; u < nu; u += 2 * nthreads) {
+    const TapUnit t0 = tap_unit(tab, u, nu, nt, A, rs);
+    const TapUnit t1 = tap_unit(tab, u + nthreads, nu, nt, A, rs);
+    tap_apply(t0, rs);
+    tap_apply(t1, rs);
   }
 }
 
