@@ -1339,7 +1339,7 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
   __shared__ uint32_t tmem_slot;
   __shared__ volatile int abort_flag;
   __shared__ volatile int released;
-  __shared__ int tab_count[2][2];  // reaching atoms in the table: [group][chunk parity]
+  __shared__ int tab_count[2][2][2];  // reaching atoms in the table: [group][item parity][chunk parity]
   const int NB = a.twN, N = 2 * a.twN, KT = a.tcK, R = a.tcR, RB = a.twRB, RS = a.twRS, G = a.twG;
   const int CH = (KT + kTwChunk - 1) / kTwChunk;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -1387,7 +1387,7 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     abort_flag = 0;
     released = 0;
-    tab_count[0][0] = tab_count[0][1] = tab_count[1][0] = tab_count[1][1] = 0;
+    for (int i = 0; i < 8; ++i) (&tab_count[0][0][0])[i] = 0;
   }
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -1422,40 +1422,53 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
     const int quarter = warp & 3, rq = gw >> 2;
     const int m = 32 * quarter + lane;             // the tile row this lane splits
     float *row = A + static_cast<size_t>(m) * RS;
+    // split warps: rank < 2 in their lane quarter (group threads 0..255); the
+    // group's other warps pre-pass the next item's first table chunk while the
+    // split warps split the current item
+    const bool splitter = rq < 2;
+    const int ns_tid = gtid - 256, ns_threads = gthreads - 256;
     for (int j = group, w = blockIdx.x + group * gridDim.x; w < items; j += G, w += G * gridDim.x) {
-      const int b = j & 1;
+      const int b = j & 1, ip = (j / G) & 1;
       wait(&rec_full[b], j >> 1);
-      const bool skip = producers_sync_or(abort_flag != 0, bar_id, gthreads);
       const TwSlot &sl = slot[b];
+      // chunk k of an item's visible atoms counts its reaching atoms in
+      // tab_count[group][item parity][k & 1]
+      if (!splitter && !__any_sync(0xffffffffu, abort_flag != 0)) {
+        const int nvis = sl.ta.cum[sl.ta.nb];
+        spread_prepass_w(a, sl.ta, recs + static_cast<size_t>(b) * RB, min(nvis, RB), sl.f, 0, min(cap, nvis),
+                         tab, sl.x0, sl.y0, sl.cw, sl.ch, ns_tid, ns_threads, &tab_count[group][ip][0]);
+      }
+      // the first chunk's table is complete and the previous item's split done
+      const bool skip = producers_sync_or(abort_flag != 0, bar_id, gthreads);
+      if (gtid == 0) tab_count[group][ip ^ 1][0] = tab_count[group][ip ^ 1][1] = 0;  // the next item's
       const float mean = sl.mean;
       if (!skip) {
         const int nvis = sl.ta.cum[sl.ta.nb];
         const int nrec = min(nvis, RB);
-        // chunk k of the visible atoms counts its reaching atoms in
-        // tab_count[group][k & 1]; the other counter is cleared meanwhile (its
-        // readers passed the barrier at the top of this chunk)
         for (int v0 = 0, k = 0; v0 < nvis; v0 += cap, ++k) {
-          const int nv = min(cap, nvis - v0);
-          if (v0 > 0) producers_sync(bar_id, gthreads);
-          if (gtid == 0 && k > 0) tab_count[group][(k + 1) & 1] = 0;
-          spread_prepass_w(a, sl.ta, recs + static_cast<size_t>(b) * RB, nrec, sl.f, v0, nv, tab, sl.x0, sl.y0,
-                           sl.cw, sl.ch, gtid, gthreads, &tab_count[group][k & 1]);
-          producers_sync(bar_id, gthreads);
-          spread_taps_w(tab, tab_count[group][k & 1], a.ntaps, A, RS, gtid, gthreads);
+          if (k > 0) {
+            // further chunks: all producer warps; the counter of chunk k - 1's
+            // predecessor is free (its readers passed the barrier above)
+            producers_sync(bar_id, gthreads);
+            if (gtid == 0) tab_count[group][ip][(k + 1) & 1] = 0;
+            spread_prepass_w(a, sl.ta, recs + static_cast<size_t>(b) * RB, nrec, sl.f, v0, min(cap, nvis - v0),
+                             tab, sl.x0, sl.y0, sl.cw, sl.ch, gtid, gthreads, &tab_count[group][ip][k & 1]);
+            producers_sync(bar_id, gthreads);
+          }
+          spread_taps_w(tab, tab_count[group][ip][k & 1], a.ntaps, A, RS, gtid, gthreads);
         }
       }
       producers_sync(bar_id, gthreads);
-      if (gtid == 0) tab_count[group][0] = tab_count[group][1] = 0;  // for the next item
       if (gtid == 0) mbar_arrive(smem_addr(&rec_empty[b]));
+      if (!splitter) continue;
       // rows z in [tcK, tcR) meet no twiddle: cleared for the next item
-      for (int i = gtid; i < 128 * ((R - KT) / 4); i += gthreads) {
+      for (int i = gtid; i < 128 * ((R - KT) / 4); i += 256) {
         const int mm = i / ((R - KT) / 4), zq = i % ((R - KT) / 4);
         reinterpret_cast<float4 *>(A + static_cast<size_t>(mm) * RS + KT)[zq] = make_float4(0.f, 0.f, 0.f, 0.f);
       }
       // split, chunk by chunk through the A ring
       for (int c = 0; c < CH; ++c) {
         const int q = j * CH + c, s = q % kTwRing;
-        if (rq >= 2) break;  // not a split warp
         if (q >= kTwRing) wait_released(q - kTwRing + 1);
         __syncwarp();  // converged for the .sync.aligned tensor-memory stores
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
