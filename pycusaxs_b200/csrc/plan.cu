@@ -93,7 +93,7 @@ struct DevArgs {
   // wide-tile variant (k_spread_zdft_tcw): tile row stride (floats), record buffer,
   // atom table entries, producer groups; y tiles of 16 rows
   int twN, twRS, twRB, twCap, twG, stw;
-  int xtcTP;  // tensor-core x-axis DFT: rows per ky (types padded to 8 or 16)
+  int xtcKyb;  // tensor-core x-axis DFT: ky values per item (rows (ky, type), T per ky)
   int nf[3];
   int dz;
   float dq, qcut;
@@ -1748,11 +1748,12 @@ __global__ void __launch_bounds__(kThreads) k_ydft(DevArgs a) {
 //                  of k) padded to 16.
 // y pass: rows are the x rows of one z-transformed plane Z[x][y] (u = y, k =
 //   ky), 128 per item; the epilogue writes Y[ky][x].
-// x pass: rows are (ky, type) pairs of one (frame, kz), row = (ky - ky0) * TP +
-//   type with the types padded to TP (8 or 16), u = x, k = kx; the epilogue
-//   applies the form factors, sums the types with shuffles across the TP lanes
-//   of a ky, squares and multiplies by the B-spline moduli (the SIMT kernel's
-//   k_xdft_post), writing ibox[kz][ky][kx].
+// x pass: rows are (ky, type) pairs of one (frame, kz), row = (ky - ky0) * T +
+//   type, kyb = 128 / T ky per item (rows beyond T*kyb unused), u = x, k = kx;
+//   the epilogue applies the form factors, then the four warps of an epilogue
+//   slot sum the types of each ky through shared memory, square and multiply by
+//   the B-spline moduli (the SIMT kernel's k_xdft_post), writing
+//   ibox[kz][ky][kx].
 // K is streamed in chunks of kDtcChunk values of u: per chunk the loader warp
 // issues one tensor copy (cp.async.bulk.tensor, no multicast, 128-byte swizzle)
 // of the 128 rows x 32 floats into a raw staging tile (rows outside the data
@@ -1784,7 +1785,7 @@ struct DtcShape {
 // (128-byte swizzle: the 16-byte piece j of row r lands at piece j ^ (r % 8) of
 // the row) (y pass: 3-D map
 // {2*ey floats, ex rows, planes}; x pass: 5-D map {2*ex floats, type, ky, kz,
-// frame} whose box {32, TP, 128/TP, 1, 1} lands rows in (ky, type) order).
+// frame} whose box {32, T, kyb, 1, 1} lands rows in (ky, type) order).
 template <bool kX>
 __device__ __forceinline__ void dtc_tensor_copy(const DevArgs &a, const CUtensorMap *map, int w, int c,
                                                 uint32_t dst, uint32_t bar) {
@@ -1798,7 +1799,7 @@ __device__ __forceinline__ void dtc_tensor_copy(const DevArgs &a, const CUtensor
         "l"(m), "r"(u0), "r"((w % xblocks) * 128), "r"(w / xblocks), "r"(bar)
         : "memory");
   } else {
-    const int kyb = 128 / a.xtcTP;
+    const int kyb = a.xtcKyb;
     const int nblk = (a.nky + kyb - 1) / kyb;
     const int f = w / (a.nkz * nblk), kz = (w / nblk) % a.nkz;
     asm volatile(
@@ -1826,6 +1827,8 @@ template <bool kX>
 __global__ void __launch_bounds__(dtc_threads<kX>(), 1)
     k_dft_tc(DevArgs a, DtcShape sh, const __grid_constant__ CUtensorMap amap, int items) {
   extern __shared__ __align__(16) unsigned char smem[];
+  // x pass: per epilogue slot, the 128 rows x 8 kx of f_t * F summed over types
+  __shared__ float2 xsum[kX ? 3 * 128 * 8 : 1];
   __shared__ __align__(8) uint64_t bars[3 * kDtcMaxStages + 4];
   __shared__ uint32_t tmem_slot;
   __shared__ volatile int abort_flag;
@@ -1921,7 +1924,9 @@ __global__ void __launch_bounds__(dtc_threads<kX>(), 1)
   } else if (warp == kDtcLoaderWarp) {
     if (lane == 0) {
       const uint32_t bbytes = static_cast<uint32_t>(2 * b_floats * sizeof(float));
-      const uint32_t abytes = static_cast<uint32_t>(a_floats * sizeof(float));
+      // the tensor copy lands T*kyb rows in the x pass (128 in the y pass)
+      const int arows = kX ? a.T * a.xtcKyb : 128;
+      const uint32_t abytes = static_cast<uint32_t>(arows * KP * sizeof(float));
       int g = 0;
       for (int w = blockIdx.x; w < items && !abort_flag; w += gridDim.x) {
         for (int c = 0; c < NC; ++c, ++g) {
@@ -1996,7 +2001,9 @@ __global__ void __launch_bounds__(dtc_threads<kX>(), 1)
     for (int w = blockIdx.x; w < items; w += gridDim.x, ++i) {
       const int d = i & 1;
       wait(&dfull[d], i >> 1);
-      if (__any_sync(0xffffffffu, abort_flag != 0)) break;
+      // x pass: the four warps of a slot meet at named barriers, so they decide together
+      if (kX ? producers_sync_or(abort_flag != 0, 1 + eslot, 128) : __any_sync(0xffffffffu, abort_flag != 0))
+        break;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const uint32_t lane_base = tmem + (static_cast<uint32_t>(32 * quarter) << 16) + static_cast<uint32_t>(d * N);
       if (!kX) {
@@ -2026,11 +2033,15 @@ __global__ void __launch_bounds__(dtc_threads<kX>(), 1)
           }
         }
       } else {
-        const int tp = a.xtcTP, kyb = 128 / tp;
+        // rows r = kyl * T + t (kyl < kyb); each lane finishes f_t * F for its row,
+        // the four warps of this epilogue slot (one per lane quarter) meet in
+        // shared memory to sum the types of each ky, square and scale
+        const int T = a.T, kyb = a.xtcKyb;
         const int nblk = (a.nky + kyb - 1) / kyb;
         const int f = w / (a.nkz * nblk), kz = (w / nblk) % a.nkz;
-        const int ky = (w % nblk) * kyb + r / tp, t = r % tp;
-        const bool row_ok = t < a.T && ky < a.nky;
+        const int ky0 = (w % nblk) * kyb;
+        const int kyl = r / T, t = r % T, ky = ky0 + kyl;
+        const bool row_ok = r < T * kyb && ky < a.nky;
         float ocs[9];
 #pragma unroll
         for (int q = 0; q < 9; ++q) ocs[q] = a.geom[f * kGeom + 9 + q];
@@ -2039,10 +2050,10 @@ __global__ void __launch_bounds__(dtc_threads<kX>(), 1)
         const float mean = row_ok ? padding_mean(a, f, t) : 0.0f;
         float ff[9];
 #pragma unroll
-        for (int q = 0; q < 9; ++q) ff[q] = a.ff[9 * (t < a.T ? t : 0) + q];
-        const int jw = ja < 0 ? ja + a.nn[1] : ja;
-        const float mzy = a.mody[jw] * a.modz[kz];
-        float *ib = a.ibox + ((static_cast<int64_t>(f) * a.nkz + kz) * a.nky + ky) * a.nkx;
+        for (int q = 0; q < 9; ++q) ff[q] = a.ff[9 * t + q];
+        float2 *red = xsum + eslot * 128 * 8;  // [row][8 kx]
+        const int rid = 32 * quarter + lane;    // 0..127 over the slot's four warps
+        const uint32_t bar_id = 1 + eslot;
         for (int c0 = 16 * eslot; c0 < N; c0 += 16 * EQ) {
           uint32_t v[16];
           asm volatile(
@@ -2070,16 +2081,27 @@ __global__ void __launch_bounds__(dtc_threads<kX>(), 1)
               A.x = ft * F.x;
               A.y = ft * F.y;
             }
-            // type sum across the tp lanes of this ky
-            for (int o = 1; o < tp; o <<= 1) {
-              A.x += __shfl_xor_sync(0xffffffffu, A.x, o);
-              A.y += __shfl_xor_sync(0xffffffffu, A.y, o);
-            }
-            if (t == 0 && ky < a.nky && kx < a.nkx) {
-              const int iw = ia < 0 ? ia + a.nn[0] : ia;
-              ib[kx] = !(mw > a.qcut) ? (A.x * A.x + A.y * A.y) * (a.modx[iw] * mzy) : 0.0f;
+            red[r * 8 + jj] = A;
+          }
+          asm volatile("bar.sync %0, 128;" ::"r"(bar_id) : "memory");
+          for (int p = rid; p < kyb * 8; p += 128) {
+            const int kl = p >> 3, jj = p & 7;
+            const int kyy = ky0 + kl, kx = c0 / 2 + jj;
+            if (kyy < a.nky && kx < a.nkx) {
+              float2 A = make_float2(0.f, 0.f);
+              for (int tt = 0; tt < T; ++tt) {
+                const float2 e = red[(kl * T + tt) * 8 + jj];
+                A.x += e.x;
+                A.y += e.y;
+              }
+              const int ia = a.kx_lo + kx, jb = a.ky_lo + kyy;
+              const float mw = kpoint_q(ocs, ia, jb, ka);
+              const int iw = ia < 0 ? ia + a.nn[0] : ia, jw = jb < 0 ? jb + a.nn[1] : jb;
+              a.ibox[((static_cast<int64_t>(f) * a.nkz + kz) * a.nky + kyy) * a.nkx + kx] =
+                  !(mw > a.qcut) ? (A.x * A.x + A.y * A.y) * (a.modx[iw] * (a.mody[jw] * a.modz[kz])) : 0.0f;
             }
           }
+          asm volatile("bar.sync %0, 128;" ::"r"(bar_id) : "memory");  // before the next group's writes
         }
       }
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -3322,7 +3344,7 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
     if (!(ym && std::strcmp(ym, "simt") == 0) && a.ext[1] % 2 == 0)
       pl->use_ytc = dtc_shape(a.nky, a.ext[1], optin - static_smem(k_dft_tc<false>), &pl->yshape,
                               &pl->smem_ydft_tc);
-    a.xtcTP = a.T <= 8 ? 8 : 16;
+    a.xtcKyb = 128 / a.T;
     if (!(xm && std::strcmp(xm, "simt") == 0) && a.T <= 16 && a.ext[0] % 2 == 0)
       pl->use_xtc = dtc_shape(a.nkx, a.ext[0], optin - static_smem(k_dft_tc<true>), &pl->xshape,
                               &pl->smem_xdft_tc);
@@ -3696,7 +3718,7 @@ int launch_ydft(const SaxsPlan *pl, const DevArgs &a, int planes, cudaStream_t s
 // the tensor-core kernel when the plan has it, else the FP32 SIMT kernel.
 int launch_xdft(const SaxsPlan *pl, const DevArgs &a, int nframes, cudaStream_t st) {
   if (pl->use_xtc) {
-    const int kyb = 128 / a.xtcTP;
+    const int kyb = a.xtcKyb;
     const int items = nframes * a.nkz * ((a.nky + kyb - 1) / kyb);
     // Y[f][t][kz][ky][x] as {2*ex floats, t, ky, kz, f}
     const cuuint64_t ex = a.ext[0];
@@ -3704,7 +3726,7 @@ int launch_xdft(const SaxsPlan *pl, const DevArgs &a, int nframes, cudaStream_t 
                                 static_cast<cuuint64_t>(a.nkz), static_cast<cuuint64_t>(nframes)};
     const cuuint64_t row = 8 * ex;
     const cuuint64_t strides[4] = {row * a.nky * a.nkz, row, row * a.nky, row * a.nky * a.nkz * a.T};
-    const cuuint32_t box[5] = {2 * kDtcChunk, static_cast<cuuint32_t>(a.xtcTP), static_cast<cuuint32_t>(kyb), 1, 1};
+    const cuuint32_t box[5] = {2 * kDtcChunk, static_cast<cuuint32_t>(a.T), static_cast<cuuint32_t>(kyb), 1, 1};
     CUtensorMap map;
     if (int rc = encode_map(&map, a.Y, 5, dims, strides, box)) return rc;
     k_dft_tc<true><<<std::max(1, std::min(items, pl->xtc_ctas)), dtc_threads<true>(), pl->smem_xdft_tc, st>>>(
