@@ -1776,9 +1776,18 @@ __host__ __device__ constexpr int dtc_threads() { return 32 * (kDtcProducerWarps
 constexpr int kDtcMaxStages = 4;
 
 // One pass's GEMM shape: N', K chunks, stages, TMEM columns, B' table.
+// With `lo_smem` (when 2N' <= 256): only A's TF32 head goes to tensor memory (32
+// columns per stage); the producers write A's remainder back in place into the
+// 128-byte-swizzled tensor-copy tile, which the MMA reads as a K-major SWIZZLE_128B
+// shared-memory operand, and B' holds head and remainder side by side (2N'
+// columns).  A k step is then two MMAs, D += Ah [Bh|Bl] and D += Al [Bh|Bl] (a
+// tf32 MMA costs about the same up to N = 192), instead of three; the epilogue
+// adds the two halves of D.
 struct DtcShape {
   int N, chunks, S, cols;
-  const float *B;  // [chunk][2][N' x 2*kDtcChunk]: head block then remainder block
+  int lo_smem;
+  const float *B;  // [chunk]: head block then remainder block (N' x 2*kDtcChunk
+                   // each), or one block of 2N' x 2*kDtcChunk with lo_smem
 };
 
 // Tensor copy of chunk c of item w's 128 rows into `dst`, 1024-byte aligned
@@ -1833,6 +1842,8 @@ __global__ void __launch_bounds__(dtc_threads<kX>(), 1)
   __shared__ uint32_t tmem_slot;
   __shared__ volatile int abort_flag;
   const int N = sh.N, NS = sh.S, NC = sh.chunks;
+  const int NM = sh.lo_smem ? 2 * N : N;             // MMA N, accumulator stage width
+  const int AW = sh.lo_smem ? 32 : 64;               // tensor-memory columns of an A stage
   const int KP = 2 * kDtcChunk;                      // K' per chunk
   const int a_floats = 128 * KP, b_floats = N * KP;  // raw A tile; B' head or remainder
   const int stage_floats = a_floats + 2 * b_floats;
@@ -1890,12 +1901,13 @@ __global__ void __launch_bounds__(dtc_threads<kX>(), 1)
         if (g >= NS) wait(&empty[st], g / NS - 1);  // the stage's MMAs have read its TMEM columns
         wait(&bfull[st], g / NS);
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const float *raw = stages + static_cast<size_t>(st) * stage_floats;
+        float *raw = stages + static_cast<size_t>(st) * stage_floats;
         uint32_t hi[16], lo[16];
 #pragma unroll
         for (int jj = 0; jj < 4; ++jj) {
           const int j = 4 * half + jj;
-          const float4 v = *reinterpret_cast<const float4 *>(raw + r * KP + 4 * (j ^ (r & 7)));
+          float4 *p = reinterpret_cast<float4 *>(raw + r * KP + 4 * (j ^ (r & 7)));
+          const float4 v = *p;
           const float vv[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
           for (int e = 0; e < 4; ++e) {
@@ -1903,18 +1915,23 @@ __global__ void __launch_bounds__(dtc_threads<kX>(), 1)
             hi[4 * jj + e] = __float_as_uint(h);
             lo[4 * jj + e] = __float_as_uint(vv[e] - h);
           }
+          if (sh.lo_smem)  // the remainder replaces the raw values in the swizzled tile
+            *p = make_float4(__uint_as_float(lo[4 * jj]), __uint_as_float(lo[4 * jj + 1]),
+                             __uint_as_float(lo[4 * jj + 2]), __uint_as_float(lo[4 * jj + 3]));
         }
-        const uint32_t col = tmem + lane_off + static_cast<uint32_t>(2 * N + 64 * st + 16 * half);
+        const uint32_t col = tmem + lane_off + static_cast<uint32_t>(2 * NM + AW * st + 16 * half);
+        if (sh.lo_smem) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         asm volatile(
             "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], "
             "{%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(col),
             "r"(hi[0]), "r"(hi[1]), "r"(hi[2]), "r"(hi[3]), "r"(hi[4]), "r"(hi[5]), "r"(hi[6]), "r"(hi[7]),
             "r"(hi[8]), "r"(hi[9]), "r"(hi[10]), "r"(hi[11]), "r"(hi[12]), "r"(hi[13]), "r"(hi[14]), "r"(hi[15]));
-        asm volatile(
-            "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], "
-            "{%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(col + 32),
-            "r"(lo[0]), "r"(lo[1]), "r"(lo[2]), "r"(lo[3]), "r"(lo[4]), "r"(lo[5]), "r"(lo[6]), "r"(lo[7]),
-            "r"(lo[8]), "r"(lo[9]), "r"(lo[10]), "r"(lo[11]), "r"(lo[12]), "r"(lo[13]), "r"(lo[14]), "r"(lo[15]));
+        if (!sh.lo_smem)
+          asm volatile(
+              "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], "
+              "{%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(col + 32),
+              "r"(lo[0]), "r"(lo[1]), "r"(lo[2]), "r"(lo[3]), "r"(lo[4]), "r"(lo[5]), "r"(lo[6]), "r"(lo[7]),
+              "r"(lo[8]), "r"(lo[9]), "r"(lo[10]), "r"(lo[11]), "r"(lo[12]), "r"(lo[13]), "r"(lo[14]), "r"(lo[15]));
         asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         __syncwarp();
@@ -1950,14 +1967,14 @@ __global__ void __launch_bounds__(dtc_threads<kX>(), 1)
     if (lane == 0) {
       // kind::tf32: D f32, A and B tf32, both K-major, N >> 3 at bit 17, M = 128
       const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) |
-                             (static_cast<uint32_t>(N >> 3) << 17) | (static_cast<uint32_t>(128 >> 4) << 24);
+                             (static_cast<uint32_t>(NM >> 3) << 17) | (static_cast<uint32_t>(128 >> 4) << 24);
       int g = 0, i = 0;
       uint32_t last_bar = 0;
       int last_parity = 0;
       for (int w = blockIdx.x; w < items && !abort_flag; w += gridDim.x, ++i) {
         const int d = i & 1;
         if (i >= 2) wait(&dempty[d], (i - 2) >> 1);
-        const uint32_t dcol = tmem + static_cast<uint32_t>(d * N);
+        const uint32_t dcol = tmem + static_cast<uint32_t>(d * NM);
         for (int c = 0; c < NC; ++c, ++g) {
           const int st = g % NS;
           wait(&bfull[st], g / NS);
@@ -1965,17 +1982,30 @@ __global__ void __launch_bounds__(dtc_threads<kX>(), 1)
           if (abort_flag) break;
           asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
           const float *sb = stages + static_cast<size_t>(st) * stage_floats;
-          const uint64_t dbh0 = umma_desc(smem_addr(sb + a_floats), N * 16, 128);
-          const uint64_t dbl0 = umma_desc(smem_addr(sb + a_floats + b_floats), N * 16, 128);
-          const uint32_t ah0 = tmem + static_cast<uint32_t>(2 * N + 64 * st);
-          // one k step (8 of K'): A advances 8 TMEM columns, B' N*32 B (+N*2)
-          for (int kk = 0; kk < KP / 8; ++kk) {
-            const uint32_t ah = ah0 + 8 * kk, al = ah + 32;
-            const uint64_t dbh = dbh0 + static_cast<uint64_t>(kk * 2 * N);
-            const uint64_t dbl = dbl0 + static_cast<uint64_t>(kk * 2 * N);
-            umma_tf32_ts(dcol, al, dbh, idesc, (c > 0 || kk > 0) ? 1u : 0u);
-            umma_tf32_ts(dcol, ah, dbl, idesc, 1u);
-            umma_tf32_ts(dcol, ah, dbh, idesc, 1u);
+          const uint32_t ah0 = tmem + static_cast<uint32_t>(2 * NM + AW * st);
+          if (sh.lo_smem) {
+            // B' = [Bh | Bl] (2N' columns); Al is the swizzled tile itself: a K-major
+            // SWIZZLE_128B descriptor (layout type 2, 8-row groups 1024 B apart) whose
+            // start advances 32 B per k step of 8 floats within the 128-byte rows
+            const uint64_t db0 = umma_desc(smem_addr(sb + a_floats), NM * 16, 128);
+            const uint64_t dal0 = umma_desc(smem_addr(sb), 16, 1024) | (static_cast<uint64_t>(2) << 61);
+            for (int kk = 0; kk < KP / 8; ++kk) {
+              const uint64_t db = db0 + static_cast<uint64_t>(kk * 2 * NM);
+              umma_tf32_ts(dcol, ah0 + 8 * kk, db, idesc, (c > 0 || kk > 0) ? 1u : 0u);
+              umma_tf32(dcol, dal0 + static_cast<uint64_t>(2 * kk), db, idesc, 1u);
+            }
+          } else {
+            const uint64_t dbh0 = umma_desc(smem_addr(sb + a_floats), N * 16, 128);
+            const uint64_t dbl0 = umma_desc(smem_addr(sb + a_floats + b_floats), N * 16, 128);
+            // one k step (8 of K'): A advances 8 TMEM columns, B' N*32 B (+N*2)
+            for (int kk = 0; kk < KP / 8; ++kk) {
+              const uint32_t ah = ah0 + 8 * kk, al = ah + 32;
+              const uint64_t dbh = dbh0 + static_cast<uint64_t>(kk * 2 * N);
+              const uint64_t dbl = dbl0 + static_cast<uint64_t>(kk * 2 * N);
+              umma_tf32_ts(dcol, al, dbh, idesc, (c > 0 || kk > 0) ? 1u : 0u);
+              umma_tf32_ts(dcol, ah, dbl, idesc, 1u);
+              umma_tf32_ts(dcol, ah, dbh, idesc, 1u);
+            }
           }
           asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                            smem_addr(&empty[st]))
@@ -2005,7 +2035,30 @@ __global__ void __launch_bounds__(dtc_threads<kX>(), 1)
       if (kX ? producers_sync_or(abort_flag != 0, 1 + eslot, 128) : __any_sync(0xffffffffu, abort_flag != 0))
         break;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const uint32_t lane_base = tmem + (static_cast<uint32_t>(32 * quarter) << 16) + static_cast<uint32_t>(d * N);
+      const uint32_t lane_base = tmem + (static_cast<uint32_t>(32 * quarter) << 16) + static_cast<uint32_t>(d * NM);
+      // 16 accumulator columns from c0 (with lo_smem: the sum of the two halves)
+      auto load16 = [&](int c0, uint32_t v[16]) {
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+            "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+              "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+            : "r"(lane_base + c0));
+        if (sh.lo_smem) {
+          uint32_t u[16];
+          asm volatile(
+              "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+              "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+              : "=r"(u[0]), "=r"(u[1]), "=r"(u[2]), "=r"(u[3]), "=r"(u[4]), "=r"(u[5]), "=r"(u[6]), "=r"(u[7]),
+                "=r"(u[8]), "=r"(u[9]), "=r"(u[10]), "=r"(u[11]), "=r"(u[12]), "=r"(u[13]), "=r"(u[14]), "=r"(u[15])
+              : "r"(lane_base + N + c0));
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+          for (int q = 0; q < 16; ++q) v[q] = __float_as_uint(__uint_as_float(v[q]) + __uint_as_float(u[q]));
+        } else {
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        }
+      };
       if (!kX) {
         const int ex = a.ext[0];
         const int xblocks = (ex + 127) / 128;
@@ -2014,14 +2067,7 @@ __global__ void __launch_bounds__(dtc_threads<kX>(), 1)
         float2 *Yp = a.Y + plane * a.nky * ex;
         for (int c0 = 16 * eslot; c0 < N; c0 += 16 * EQ) {
           uint32_t v[16];
-          asm volatile(
-              "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-              "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-              : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
-                "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
-                "=r"(v[14]), "=r"(v[15])
-              : "r"(lane_base + c0));
-          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+          load16(c0, v);
           if (x < ex) {
 #pragma unroll
             for (int jj = 0; jj < 8; ++jj) {
@@ -2056,14 +2102,7 @@ __global__ void __launch_bounds__(dtc_threads<kX>(), 1)
         const uint32_t bar_id = 1 + eslot;
         for (int c0 = 16 * eslot; c0 < N; c0 += 16 * EQ) {
           uint32_t v[16];
-          asm volatile(
-              "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-              "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-              : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
-                "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
-                "=r"(v[14]), "=r"(v[15])
-              : "r"(lane_base + c0));
-          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+          load16(c0, v);
 #pragma unroll
           for (int jj = 0; jj < 8; ++jj) {
             const int kx = c0 / 2 + jj;
@@ -3040,11 +3079,27 @@ void destroy(SaxsPlan *pl) {
 // GEMM shape of a tensor-core DFT pass over `extent` values of u to `nk` values
 // of k: N' = 2*nk padded to 16 (at most 256), two to four K-chunk stages in
 // `avail` bytes of shared memory.  Returns false when the pass does not fit.
-bool dtc_shape(int nk, int extent, size_t avail, DtcShape *sh, size_t *smem) {
+bool dtc_shape(int nk, int extent, size_t avail, DtcShape *sh, size_t *smem, bool allow_lo_smem) {
   const int N = round_up(2 * nk, 16);
   const size_t stage_bytes = (128 + 2 * static_cast<size_t>(N)) * 2 * kDtcChunk * sizeof(float);
-  // tensor memory: two accumulators of N' columns and 64 columns of A per stage
-  const int S = std::min({kDtcMaxStages, static_cast<int>((avail - 1024) / stage_bytes), (512 - 2 * N) / 64});
+  const int S_smem = static_cast<int>((avail - 1024) / stage_bytes);
+  // tensor memory: two accumulators of N' columns and 64 columns of A per stage;
+  // with the A remainder in shared memory (2N' <= 256): two accumulators of 2N'
+  // columns and 32 columns per stage.  PYCUSAXS_DTC=split keeps the first form.
+  // Measured on the 100k-atom workload: the y pass 0.60 ms per 100 frames with
+  // the remainder in shared memory against 0.65 ms; the x pass, whose epilogue
+  // then reads twice the accumulator columns, 0.34 against 0.33 ms, so it keeps
+  // the first form.
+  const char *mode = std::getenv("PYCUSAXS_DTC");
+  int S = std::min({kDtcMaxStages, S_smem, (512 - 2 * N) / 64});
+  sh->lo_smem = 0;
+  if (allow_lo_smem && !(mode && std::strcmp(mode, "split") == 0) && 2 * N <= 256) {
+    const int Sl = std::min({kDtcMaxStages, S_smem, (512 - 4 * N) / 32});
+    if (Sl >= 2) {
+      sh->lo_smem = 1;
+      S = Sl;
+    }
+  }
   if (N > 256 || S < 2) return false;
   sh->N = N;
   sh->chunks = (extent + kDtcChunk - 1) / kDtcChunk;
@@ -3062,6 +3117,13 @@ std::vector<float> dtc_bprime(const std::vector<float2> &tw, int stride, int ext
   const int KP = 2 * kDtcChunk, Np = sh.N;
   const size_t blk = static_cast<size_t>(Np) * KP;
   std::vector<float> out(static_cast<size_t>(sh.chunks) * 2 * blk, 0.0f);
+  // element (n', k') of the head (part 0) or remainder (part 1) of chunk c: two
+  // N'-column blocks, or one 2N'-column block with the parts side by side
+  auto at = [&](int c, int part, int np, int kp) {
+    const int n2 = sh.lo_smem ? np + part * Np : np, N2 = sh.lo_smem ? 2 * Np : Np;
+    const size_t off = static_cast<size_t>(c) * 2 * blk + (sh.lo_smem ? 0 : part * blk);
+    return off + static_cast<size_t>(kp / 4) * (N2 / 8) * 32 + (n2 / 8) * 32 + (n2 % 8) * 4 + kp % 4;
+  };
   for (int c = 0; c < sh.chunks; ++c)
     for (int uu = 0; uu < kDtcChunk; ++uu) {
       const int u = c * kDtcChunk + uu;
@@ -3078,10 +3140,8 @@ std::vector<float> dtc_bprime(const std::vector<float2> &tw, int stride, int ext
             bits &= 0xFFFFE000u;
             float head;
             std::memcpy(&head, &bits, sizeof(head));
-            const size_t o = static_cast<size_t>(c) * 2 * blk + static_cast<size_t>(kp / 4) * (Np / 8) * 32 +
-                             (np / 8) * 32 + (np % 8) * 4 + kp % 4;
-            out[o] = head;
-            out[o + blk] = v - head;
+            out[at(c, 0, np, kp)] = head;
+            out[at(c, 1, np, kp)] = v - head;
           }
       }
     }
@@ -3343,11 +3403,11 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
     // the tensor maps need row strides that are multiples of 16 bytes: even extents
     if (!(ym && std::strcmp(ym, "simt") == 0) && a.ext[1] % 2 == 0)
       pl->use_ytc = dtc_shape(a.nky, a.ext[1], optin - static_smem(k_dft_tc<false>), &pl->yshape,
-                              &pl->smem_ydft_tc);
+                              &pl->smem_ydft_tc, true);
     a.xtcKyb = 128 / a.T;
     if (!(xm && std::strcmp(xm, "simt") == 0) && a.T <= 16 && a.ext[0] % 2 == 0)
       pl->use_xtc = dtc_shape(a.nkx, a.ext[0], optin - static_smem(k_dft_tc<true>), &pl->xshape,
-                              &pl->smem_xdft_tc);
+                              &pl->smem_xdft_tc, false);
   }
   pl->tc_ok = pl->use_tc;
   pl->ytc_ok = pl->use_ytc;

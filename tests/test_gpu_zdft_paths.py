@@ -186,16 +186,20 @@ def test_ytc_batched_frames(cuda):
     _both(s, (32, 32, 32), frames, axis="y", sigma=2.0, qcut=0.6, max_frames=3)
 
 
+@pytest.mark.parametrize("form", ["default", "split"])
 @pytest.mark.parametrize("axis", ["y", "x"])
-def test_yx_tc_many_items_per_cta(cuda, axis):
+def test_yx_tc_many_items_per_cta(cuda, axis, form):
     # 4 frames at grid 128: several hundred items, so every CTA of the persistent
     # y/x kernels processes more than one item and reuses its accumulator and
-    # operand stages (one-frame cases give each CTA at most one item)
+    # operand stages (one-frame cases give each CTA at most one item).  The y
+    # pass by default reads A's remainder from the swizzled shared-memory tile
+    # (two MMAs per k step); "split" (PYCUSAXS_DTC=split) keeps head and
+    # remainder in tensor memory (three MMAs per k step), the x pass's form.
     s = cubic_system(20_000, 100.0, seed=28, jitter=0.4, nframes=4)
     frames = [s.frame(k) for k in range(4)]
     var, bit = _AXES[axis]
     kw = dict(sigma=2.0, qcut=0.5, bin_size=0.002, max_frames=4)
-    with dft_mode(var, None):
+    with dft_mode(var, None), dft_mode("PYCUSAXS_DTC", "split" if form == "split" else None):
         h_tc, n_tc, e = engine_hist(s, (128, 128, 128), frames, **kw)
         assert e.info.path & bit
         e.close()
