@@ -189,12 +189,24 @@ __device__ __forceinline__ float padding_mean(const DevArgs &a, int f, int t) {
                    : static_cast<float>(a.border[static_cast<int64_t>(f) * a.T + t] / a.border_count);
 }
 
+// Programmatic dependent launch: the forward's kernels after the first are
+// launched with programmatic stream serialization, so a kernel's grid may start
+// while the previous one drains.  Each such kernel lets its own successor launch
+// at once (every CTA is then resident, so the successor cannot starve it of
+// SMs) and waits for its predecessor's completion and memory before it reads
+// anything the predecessor wrote; only set-up that touches plan constants,
+// shared and tensor memory runs before the wait.  Both are no-ops for kernels
+// launched without the attribute.
+__device__ __forceinline__ void pdl_release() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // ---------------------------------------------------------------------------
 // kernels
 // ---------------------------------------------------------------------------
 
 // grid (ceil(M/256), frames).  Dynamic shared memory: (warps x T) doubles.
 __global__ void __launch_bounds__(kThreads) k_bin_atoms(DevArgs a) {
+  pdl_release();  // first kernel of a batch: launched plainly, its successor may start early
   extern __shared__ double sh_part[];
   __shared__ float oc[9];
   const int f = blockIdx.y;
@@ -259,6 +271,8 @@ __global__ void __launch_bounds__(kThreads) k_bin_atoms(DevArgs a) {
 
 // grid (frames), block 1024: exclusive scan of counts -> offsets[0..nbins].
 __global__ void __launch_bounds__(1024) k_scan(DevArgs a) {
+  pdl_release();
+  pdl_wait();
   __shared__ int sums[1024];
   const int f = blockIdx.x;
   const int nb = a.nbins;
@@ -289,6 +303,8 @@ __global__ void __launch_bounds__(1024) k_scan(DevArgs a) {
 
 // grid (ceil(M/256), frames): records sorted by (type, home tile).
 __global__ void __launch_bounds__(kThreads) k_scatter_atoms(DevArgs a) {
+  pdl_release();
+  pdl_wait();
   __shared__ float oc[9];
   const int f = blockIdx.y;
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
@@ -397,6 +413,8 @@ __device__ __forceinline__ void spread_tile(const DevArgs &a, const TileAtoms &t
 // done with 4 columns x 6 kz (12 floats) per thread and the z range split
 // `ks` ways across the block, reduced deterministically in shared memory.
 __global__ void __launch_bounds__(kThreads, 2) k_spread_zdft(DevArgs a, int items) {
+  pdl_release();
+  pdl_wait();
   extern __shared__ __align__(16) unsigned char smem[];
   const int nz = a.n[2], ez = a.ext[2];
   const int NP = 2 * a.nkzp;
@@ -845,6 +863,7 @@ __device__ __forceinline__ bool producers_sync_or(bool v, int id, int count) {
 // home-bin tables (stiles[0] + stiles[1] int4) and one atom table per producer
 // group.
 __global__ void __launch_bounds__(kTcThreads, 1) k_spread_zdft_tc(DevArgs a, int items) {
+  pdl_release();
   extern __shared__ __align__(16) unsigned char smem[];  // no-swizzle operands need 16 B
   __shared__ TcSlot slot[2];
   __shared__ __align__(8) uint64_t bars[10];
@@ -898,6 +917,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_spread_zdft_tc(DevArgs a, int
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_slot;
+  pdl_wait();  // set-up above touched only plan constants, shared and tensor memory
 
   // bounded wait; on a timeout the whole block switches to skipping its work
   auto wait = [&](uint64_t *bar, int parity) {
@@ -1333,6 +1353,7 @@ __device__ __forceinline__ void spread_taps_w(const AtomTab &tab, int nv, int nt
 // floats, two record buffers of twRB float4, the home-bin tables (stiles[0] +
 // 2*stw int4) and twG atom tables of twCap entries.
 __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, int items) {
+  pdl_release();
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ TwSlot slot[2];
   __shared__ __align__(8) uint64_t bars[4 + 2 * kTwRing + 4];
@@ -1394,6 +1415,7 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_slot;
+  pdl_wait();  // set-up above touched only plan constants, shared and tensor memory
 
   auto wait = [&](uint64_t *bar, int parity) {
     if (abort_flag) return;
@@ -1670,6 +1692,8 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
 // grid (ceil(ex/64), nkz, frames*T), block 256: y-axis DFT.
 // Y[f,t,kz][ky][x] = sum_y Z[f,t,kz][x][y] * exp(-2 pi i ja y / nny).
 __global__ void __launch_bounds__(kThreads) k_ydft(DevArgs a) {
+  pdl_release();
+  pdl_wait();
   extern __shared__ __align__(16) unsigned char smem[];
   float2 *zs = reinterpret_cast<float2 *>(smem);        // [kYChunk][kYStride]
   float2 *tys = zs + kYChunk * kYStride;                // [kYChunk][nkyp]
@@ -1835,6 +1859,7 @@ __device__ __forceinline__ void dtc_tensor_copy(const DevArgs &a, const CUtensor
 template <bool kX>
 __global__ void __launch_bounds__(dtc_threads<kX>(), 1)
     k_dft_tc(DevArgs a, DtcShape sh, const __grid_constant__ CUtensorMap amap, int items) {
+  pdl_release();
   extern __shared__ __align__(16) unsigned char smem[];
   // x pass: per epilogue slot, the 128 rows x 8 kx of f_t * F summed over types
   __shared__ float2 xsum[kX ? 3 * 128 * 8 : 1];
@@ -1876,6 +1901,7 @@ __global__ void __launch_bounds__(dtc_threads<kX>(), 1)
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_slot;
+  pdl_wait();  // set-up above touched only plan constants, shared and tensor memory
 
   auto wait = [&](uint64_t *bar, int parity) {
     if (abort_flag) return;
@@ -2159,6 +2185,8 @@ __global__ void __launch_bounds__(dtc_threads<kX>(), 1)
 // sum, modulus.  Dynamic shared memory, for an x chunk of `xc` values:
 // twx xc*nkxp | Y rows T*xc | F T*nkxp (all float2).
 __global__ void __launch_bounds__(kThreads) k_xdft_post(DevArgs a, int xc) {
+  pdl_release();
+  pdl_wait();
   extern __shared__ __align__(16) unsigned char smem[];
   const int ex = a.ext[0];
   float2 *txs = reinterpret_cast<float2 *>(smem);
@@ -2250,6 +2278,8 @@ template <typename V>
 __global__ void __launch_bounds__(kThreads)
     k_hist(DevArgs a, const V *vals, const float *geom, int geom_stride, double fact,
            double *hist, double *nhist) {
+  pdl_release();
+  pdl_wait();
   extern __shared__ __align__(16) unsigned char smem[];
   const int npts = a.nky * a.nkx;
   const bool in_smem = a.num_bins <= kHistSmemBins;
@@ -3700,24 +3730,40 @@ struct StageTimer {
   }
 };
 
+// Launch with programmatic stream serialization (see pdl_wait).
+template <typename... KArgs, typename... Args>
+int launch_pdl(const char *name, void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+               Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  const cudaError_t e = cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+  if (e != cudaSuccess) return fail(SAXS_E_CUDA, std::string(name) + ": " + cudaGetErrorString(e));
+  return launch_check(name);
+}
+
 // Spreading + z-axis DFT of `nframes` frames: the wide-tile or 64-column
 // tensor-core kernel the plan is configured for, else the FP32 SIMT kernel.
 int launch_spread(const SaxsPlan *pl, const DevArgs &a, int nframes, cudaStream_t st) {
   if (pl->use_tc && pl->use_tcw) {
     const int items = a.stiles[0] * a.stw * a.T * nframes;
-    k_spread_zdft_tcw<<<std::max(1, std::min(items, pl->tcw_ctas)), kTwThreads, pl->smem_spread_tcw, st>>>(
-        a, items);
-    return launch_check("k_spread_zdft_tcw");
+    return launch_pdl("k_spread_zdft_tcw", k_spread_zdft_tcw, dim3(std::max(1, std::min(items, pl->tcw_ctas))),
+                      dim3(kTwThreads), pl->smem_spread_tcw, st, a, items);
   }
   const int items = a.stiles[0] * a.stiles[1] * a.T * nframes;
   if (pl->use_tc) {
-    k_spread_zdft_tc<<<std::max(1, std::min(items, pl->tc_ctas)), kTcThreads, pl->smem_spread_tc,
-                       st>>>(a, items);
-    return launch_check("k_spread_zdft_tc");
+    return launch_pdl("k_spread_zdft_tc", k_spread_zdft_tc, dim3(std::max(1, std::min(items, pl->tc_ctas))),
+                      dim3(kTcThreads), pl->smem_spread_tc, st, a, items);
   }
-  k_spread_zdft<<<std::max(1, std::min(items, pl->spread_ctas)), kThreads, pl->smem_spread, st>>>(
-      a, items);
-  return launch_check("k_spread_zdft");
+  return launch_pdl("k_spread_zdft", k_spread_zdft, dim3(std::max(1, std::min(items, pl->spread_ctas))),
+                    dim3(kThreads), pl->smem_spread, st, a, items);
 }
 
 // cuTensorMapEncodeTiled, fetched from the driver once (no link to libcuda).
@@ -3765,13 +3811,11 @@ int launch_ydft(const SaxsPlan *pl, const DevArgs &a, int planes, cudaStream_t s
     const cuuint32_t box[3] = {2 * kDtcChunk, 128, 1};
     CUtensorMap map;
     if (int rc = encode_map(&map, a.Z, 3, dims, strides, box)) return rc;
-    k_dft_tc<false><<<std::max(1, std::min(items, pl->ytc_ctas)), dtc_threads<false>(), pl->smem_ydft_tc, st>>>(
-        a, pl->yshape, map, items);
-    return launch_check("k_dft_tc<y>");
+    return launch_pdl("k_dft_tc<y>", k_dft_tc<false>, dim3(std::max(1, std::min(items, pl->ytc_ctas))),
+                      dim3(dtc_threads<false>()), pl->smem_ydft_tc, st, a, pl->yshape, map, items);
   }
   dim3 gy((a.ext[0] + kYRows - 1) / kYRows, a.nkz, planes / a.nkz);
-  k_ydft<<<gy, kThreads, pl->smem_ydft, st>>>(a);
-  return launch_check("k_ydft");
+  return launch_pdl("k_ydft", k_ydft, gy, dim3(kThreads), pl->smem_ydft, st, a);
 }
 
 // x-axis DFT, form factors, type sum and moduli of `nframes` frames into ibox:
@@ -3789,13 +3833,11 @@ int launch_xdft(const SaxsPlan *pl, const DevArgs &a, int nframes, cudaStream_t 
     const cuuint32_t box[5] = {2 * kDtcChunk, static_cast<cuuint32_t>(a.T), static_cast<cuuint32_t>(kyb), 1, 1};
     CUtensorMap map;
     if (int rc = encode_map(&map, a.Y, 5, dims, strides, box)) return rc;
-    k_dft_tc<true><<<std::max(1, std::min(items, pl->xtc_ctas)), dtc_threads<true>(), pl->smem_xdft_tc, st>>>(
-        a, pl->xshape, map, items);
-    return launch_check("k_dft_tc<x>");
+    return launch_pdl("k_dft_tc<x>", k_dft_tc<true>, dim3(std::max(1, std::min(items, pl->xtc_ctas))),
+                      dim3(dtc_threads<true>()), pl->smem_xdft_tc, st, a, pl->xshape, map, items);
   }
   dim3 gx((a.nky + kXRows - 1) / kXRows, a.nkz, nframes);
-  k_xdft_post<<<gx, kThreads, pl->smem_xdft, st>>>(a, pl->xc);
-  return launch_check("k_xdft_post");
+  return launch_pdl("k_xdft_post", k_xdft_post, gx, dim3(kThreads), pl->smem_xdft, st, a, pl->xc);
 }
 
 // Enqueue the memsets and kernels of one batch of `nframes` frames whose
@@ -3817,13 +3859,13 @@ int enqueue_batch(SaxsPlan *pl, const DevArgs &a, int nframes, cudaStream_t st, 
     tm.end(kStBin);
     if (int rc = launch_check("k_bin_atoms")) return rc;
     tm.begin(kStScan);
-    k_scan<<<nframes, 1024, 0, st>>>(a);
+    const int rc_scan = launch_pdl("k_scan", k_scan, dim3(nframes), dim3(1024), 0, st, a);
     tm.end(kStScan);
-    if (int rc = launch_check("k_scan")) return rc;
+    if (rc_scan) return rc_scan;
     tm.begin(kStScatter);
-    k_scatter_atoms<<<gb, kThreads, 0, st>>>(a);
+    const int rc_sc = launch_pdl("k_scatter_atoms", k_scatter_atoms, gb, dim3(kThreads), 0, st, a);
     tm.end(kStScatter);
-    if (int rc = launch_check("k_scatter_atoms")) return rc;
+    if (rc_sc) return rc_sc;
   } else {
     CUDA_TRY(cudaMemsetAsync(a.offsets, 0, sizeof(int) * nframes * (a.nbins + 1), st));
   }
@@ -3848,8 +3890,9 @@ int enqueue_batch(SaxsPlan *pl, const DevArgs &a, int nframes, cudaStream_t st, 
   tm.begin(kStHist);
   if (pl->ensemble == SAXS_NPT) {
     dim3 gh(a.nkz, nframes);
-    k_hist<float><<<gh, kThreads, pl->smem_hist, st>>>(a, a.ibox, a.geom, kGeom, 1.0, a.hist,
-                                                       a.nhist);
+    if (int rc = launch_pdl("k_hist", k_hist<float>, gh, dim3(kThreads), pl->smem_hist, st, a, a.ibox, a.geom,
+                            kGeom, 1.0, a.hist, a.nhist))
+      return rc;
   } else {
     const int64_t npl = static_cast<int64_t>(a.nkz) * a.nky * a.nkx;
     k_accumulate<<<static_cast<unsigned>((npl + kThreads - 1) / kThreads), kThreads, 0, st>>>(a, nframes);
