@@ -3739,11 +3739,15 @@ int launch_pdl(const char *name, void (*kernel)(KArgs...), dim3 grid, dim3 block
   cfg.blockDim = block;
   cfg.dynamicSmemBytes = smem;
   cfg.stream = st;
+  static const bool off = [] {
+    const char *v = std::getenv("PYCUSAXS_PDL");  // PYCUSAXS_PDL=0: plain launches
+    return v && std::strcmp(v, "0") == 0;
+  }();
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
   at[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = at;
-  cfg.numAttrs = 1;
+  cfg.numAttrs = off ? 0 : 1;
   const cudaError_t e = cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
   if (e != cudaSuccess) return fail(SAXS_E_CUDA, std::string(name) + ": " + cudaGetErrorString(e));
   return launch_check(name);
