@@ -196,6 +196,23 @@ def max_over_ranks(v: float, dist) -> float:
     return float(t.item())
 
 
+# DRAM bytes (read + write) per frame from one ncu capture of each kernel on the
+# 20-frame case of the same workload (profiles/k_spread_zdft_tcw_100k_atoms_20frames.md,
+# profiles/k_dft_tc_x_100k_atoms_20frames.md); a launch's traffic grows with its
+# frames, so a full launch is scaled by frames per launch.
+NCU_DRAM_BYTES_PER_FRAME = {
+    "k_spread_zdft_tcw": (32.685056e6 + 270.626816e6) / 20,
+    "k_dft_tc<y>": (330.524416e6 + 84.954112e6) / 20,
+    "k_dft_tc<x>": (106.050560e6 + 3.631104e6) / 20,
+}
+
+
+def traffic_per_launch(kernel: str, frames_per_launch: float):
+    """DRAM bytes per launch of `kernel` (None when no capture exists)."""
+    per_frame = NCU_DRAM_BYTES_PER_FRAME.get(kernel)
+    return None if per_frame is None else round(per_frame * frames_per_launch)
+
+
 def bench_ours(args):
     import torch
 
@@ -301,7 +318,10 @@ def bench_ours(args):
                  "k_xdft_post": "k_dft_tc<x>" if path & 4 else "k_xdft_post"}
     tensor = bool({"k_spread_zdft": 1, "k_ydft": 2, "k_xdft_post": 4}.get(dom, 0) & path)
     roofline = {"bound": "hbm", "kernel": kernel_of.get(dom, dom), "achieved": round(achieved, 1),
-                "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4), "traffic": None,
+                "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
+                "traffic": traffic_per_launch(kernel_of.get(dom, dom), frames_per_launch),
+                "traffic_note": "DRAM bytes per launch: ncu capture of 20 frames, scaled by frames per launch",
+                "algorithmic_bytes": round(algo_bytes.get(dom, 0) * frames_per_launch),
                 "peak_source": "measured" if peaks else "fallback"}
     if dom in algo_flops:
         useful = algo_flops[dom] * frames_per_launch / per_launch_s / 1e12
