@@ -335,6 +335,12 @@ def bench_ours(args):
             roofline["fp32_tflops"] = round(useful, 2)
     stage_share = {k: round(v[0] / max(sum(x[0] for x in prof.values()), 1e-9), 4)
                    for k, v in prof.items()}
+    # every stage with an algorithmic byte count: achieved GB/s and fraction of the HBM peak
+    stage_hbm = {}
+    for k, (ms, n) in prof.items():
+        if k in algo_bytes and ms > 0 and n > 0:
+            gbs = algo_bytes[k] * (frames_timed / n) / (ms / 1e3 / n) / 1e9
+            stage_hbm[kernel_of.get(k, k)] = {"gb_s": round(gbs, 1), "frac": round(gbs / hbm, 4)}
 
     # e2e through the public API from pinned host memory
     host = torch.from_numpy(frames).pin_memory()
@@ -391,6 +397,7 @@ def bench_ours(args):
                    "kbox": [nkx, nky, nkz], "plain_path_frames_per_s": round(plain, 1) if plain else None,
                    "stage_share": stage_share,
                    "stage_kernels": {k: kernel_of.get(k, k) for k in stage_share},
+                   "stage_hbm": stage_hbm,
                    "kernel_config": eng.config(), "autotune": tuned,
                    "parallelism": f"frames sharded over {world} GPU(s)",
                    "adjoint": adj, "multi_system": multi},
