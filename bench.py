@@ -292,10 +292,9 @@ def bench_ours(args):
         "k_spread_zdft": 16 * M + 8 * T * nkz * ex * ey,
         "k_ydft": 8 * T * nkz * ex * ey + 8 * T * nkz * nky * ex,
         "k_xdft_post": 8 * T * nkz * nky * ex + 4 * nkz * nky * nkx,
-        "k_bin_atoms": 12 * M + 8 * M,
-        "k_scatter_atoms": 12 * M + 8 * M + 16 * M,
+        # positions in, (bin, rank) keys out and back, sorted records out
+        "k_sort_atoms": 12 * M + 8 * M + 8 * M + 16 * M,
         "k_hist": 4 * nkz * nky * nkx,
-        "k_scan": 8 * T * (GRID // 8) ** 2,
     }
     algo_flops = {
         "k_spread_zdft": 4 * T * ex * ey * ez * nkz,          # real x complex MAC = 2 FMA

@@ -2,13 +2,13 @@
 //
 // Pipeline of one batch of frames (all kernels hand-written for sm_100a):
 //
-//   k_bin_atoms     atoms -> float32 grid coordinates (the reference's float
-//                   steps, saxsDeviceKernels.cu:355-368), home-tile bin + rank
-//                   (counting sort), per-type FP64 z-border sums for the
-//                   padding mean (saxsDeviceKernels.cu:446-465 evaluated per
-//                   atom instead of per voxel).
-//   k_scan          per-frame exclusive scan of the bin counts.
-//   k_scatter_atoms atoms -> records sorted by (type, home tile).
+//   k_sort_atoms    one CTA per (type, frame): atoms -> float32 grid
+//                   coordinates (the reference's float steps,
+//                   saxsDeviceKernels.cu:355-368), counting sort into
+//                   (type, home tile) order in shared memory, per-type FP64
+//                   z-border sums for the padding mean
+//                   (saxsDeviceKernels.cu:446-465 evaluated per atom instead of
+//                   per voxel).
 //   k_spread_zdft   one CTA per (frame, type, 8x8 column tile): B-spline
 //                   spreading into a shared-memory column tile (no global
 //                   atomics), mean padding folded in as "subtract the mean",
@@ -104,6 +104,7 @@ struct DevArgs {
   const float *xyz;
   const int32_t *entry_atom;
   const int32_t *entry_type;
+  const int *type_start;  // [T + 1]: entries are grouped by type, type t owns [type_start[t], type_start[t+1])
   const float *geom;
   const float2 *twz;  // [ez][nkzp], nkzp a multiple of kKzThread
   const float2 *twy;  // [ey][nkyp]
@@ -117,7 +118,6 @@ struct DevArgs {
   const int4 *home_y;
   const int4 *home_yw; // per 16-row y tile: up to eight home tiles (two int4, -1 padded)
   int2 *key;
-  int *counts;
   int *offsets;
   float4 *rec;
   double *border;
@@ -204,21 +204,35 @@ __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;"
 // kernels
 // ---------------------------------------------------------------------------
 
-// grid (ceil(M/256), frames).  Dynamic shared memory: (warps x T) doubles.
-__global__ void __launch_bounds__(kThreads) k_bin_atoms(DevArgs a) {
-  pdl_release();  // first kernel of a batch: launched plainly, its successor may start early
-  extern __shared__ double sh_part[];
+// grid (T, frames), block kSortThreads: counting sort of one type's atoms of one
+// frame by home bin, all in shared memory (no global atomics, no separate scan
+// or scatter launch): ranks from shared-memory counters, the type's exclusive
+// scan of its bins (its records start at type_start[t] of the frame, fixed by
+// the grouping of the entries), the records written in bin order, and the type's
+// z-border sum.  Each thread handles the same entries in both passes.  Outputs:
+// offsets per global bin t*bins_t + local bin (and the total at offsets[nbins]),
+// records (rx, ry, rz, entry) in bin order, border sums.
+// Dynamic shared memory: bins_t ints.
+constexpr int kSortThreads = 1024;
+__global__ void __launch_bounds__(kSortThreads) k_sort_atoms(DevArgs a) {
+  pdl_release();
+  extern __shared__ int scnt[];
+  __shared__ double wsum[kSortThreads / 32];
+  __shared__ int wscan[kSortThreads / 32];
   __shared__ float oc[9];
-  const int f = blockIdx.y;
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (threadIdx.x < 9) oc[threadIdx.x] = a.geom[f * kGeom + threadIdx.x];
+  const int t = blockIdx.x, f = blockIdx.y;
+  const int nb = a.tiles[0] * a.tiles[1];
+  const int e0 = a.type_start[t], e1 = a.type_start[t + 1];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int b = tid; b < nb; b += kSortThreads) scnt[b] = 0;
+  pdl_wait();
+  if (tid < 9) oc[tid] = a.geom[f * kGeom + tid];
   __syncthreads();
-  int t = -1;
+  const float *xyz = a.xyz + f * a.frame_stride;
+  int2 *key = a.key + static_cast<int64_t>(f) * a.M;
   double contrib = 0.0;
-  if (e < a.M) {
-    const int at = a.entry_atom[e];
-    t = a.entry_type[e];
-    const float *p = a.xyz + f * a.frame_stride + 3ll * at;
+  for (int e = e0 + tid; e < e1; e += kSortThreads) {
+    const float *p = xyz + 3ll * a.entry_atom[e];
     const float x0 = p[0], y0 = p[1], z0 = p[2];
     float r[3];
     int m[3];
@@ -231,11 +245,10 @@ __global__ void __launch_bounds__(kThreads) k_bin_atoms(DevArgs a) {
     if (xf < 0) xf += a.n[0];
     int yf = m[1] - a.order;
     if (yf < 0) yf += a.n[1];
-    const int bin = (t * a.tiles[1] + yf / a.bin_w) * a.tiles[0] + xf / a.bin_w;
-    const int rank = atomicAdd(&a.counts[f * a.nbins + bin], 1);
-    a.key[static_cast<int64_t>(f) * a.M + e] = make_int2(bin, rank);
-    // Contribution of this atom to the z-border planes of its type's grid:
-    // (sum of x weights) * (sum of y weights) * (sum of z weights on border planes).
+    const int bin = (yf / a.bin_w) * a.tiles[0] + xf / a.bin_w;
+    key[e] = make_int2(bin, atomicAdd(&scnt[bin], 1));
+    // the atom's share of its type's z-border planes: (sum of x weights) * (sum of
+    // y weights) * (sum of z weights on border planes)
     float wx[4], wy[4], wz[4];
     cubic_weights(r[0] - static_cast<float>(m[0]), wx);
     cubic_weights(r[1] - static_cast<float>(m[1]), wy);
@@ -251,75 +264,58 @@ __global__ void __launch_bounds__(kThreads) k_bin_atoms(DevArgs a) {
         if (z <= a.dz || z >= a.n[2] - a.dz) sz += wz[o];
       }
     }
-    contrib = static_cast<double>(sx) * static_cast<double>(sy) * static_cast<double>(sz);
+    contrib += static_cast<double>(sx) * static_cast<double>(sy) * static_cast<double>(sz);
   }
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int nw = blockDim.x >> 5;
-  for (int tt = 0; tt < a.T; ++tt) {
-    const unsigned any = __ballot_sync(0xffffffffu, t == tt);
-    double v = 0.0;
-    if (any) v = warp_sum(t == tt ? contrib : 0.0);
-    if (lane == 0) sh_part[warp * a.T + tt] = v;
-  }
+  contrib = warp_sum(contrib);
+  if (lane == 0) wsum[warp] = contrib;
   __syncthreads();
-  for (int tt = threadIdx.x; tt < a.T; tt += blockDim.x) {
-    double s = 0.0;
-    for (int w = 0; w < nw; ++w) s += sh_part[w * a.T + tt];
-    if (s != 0.0) atomicAdd(&a.border[f * a.T + tt], s);
-  }
-}
-
-// grid (frames), block 1024: exclusive scan of counts -> offsets[0..nbins].
-__global__ void __launch_bounds__(1024) k_scan(DevArgs a) {
-  pdl_release();
-  pdl_wait();
-  __shared__ int sums[1024];
-  const int f = blockIdx.x;
-  const int nb = a.nbins;
-  const int *c = a.counts + static_cast<int64_t>(f) * nb;
-  int *o = a.offsets + static_cast<int64_t>(f) * (nb + 1);
-  const int per = (nb + blockDim.x - 1) / blockDim.x;
-  const int s0 = threadIdx.x * per;
+  // exclusive scan of the bin counts: a contiguous segment per thread
+  const int per = (nb + kSortThreads - 1) / kSortThreads, s0 = tid * per;
   int local = 0;
   for (int i = 0; i < per; ++i)
-    if (s0 + i < nb) local += c[s0 + i];
-  sums[threadIdx.x] = local;
-  __syncthreads();
-  for (int off = 1; off < blockDim.x; off <<= 1) {
-    const int v = threadIdx.x >= off ? sums[threadIdx.x - off] : 0;
-    __syncthreads();
-    sums[threadIdx.x] += v;
-    __syncthreads();
+    if (s0 + i < nb) local += scnt[s0 + i];
+  int inc = local;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const int v = __shfl_up_sync(0xffffffffu, inc, d);
+    if (lane >= d) inc += v;
   }
-  int run = sums[threadIdx.x] - local;
+  if (lane == 31) wscan[warp] = inc;
+  __syncthreads();
+  if (warp == 0) {
+    int w = wscan[lane];
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const int v = __shfl_up_sync(0xffffffffu, w, d);
+      if (lane >= d) w += v;
+    }
+    wscan[lane] = w;
+    double b = wsum[lane];
+    b = warp_sum(b);
+    if (lane == 0) a.border[static_cast<int64_t>(f) * a.T + t] = b;
+  }
+  __syncthreads();
+  int run = (warp > 0 ? wscan[warp - 1] : 0) + inc - local;
+  int *off = a.offsets + static_cast<int64_t>(f) * (a.nbins + 1) + static_cast<int64_t>(t) * nb;
   for (int i = 0; i < per; ++i) {
     if (s0 + i < nb) {
-      o[s0 + i] = run;
-      run += c[s0 + i];
+      const int c = scnt[s0 + i];
+      scnt[s0 + i] = run;
+      off[s0 + i] = e0 + run;
+      run += c;
     }
   }
-  if (threadIdx.x == blockDim.x - 1) o[nb] = sums[threadIdx.x];
-}
-
-// grid (ceil(M/256), frames): records sorted by (type, home tile).
-__global__ void __launch_bounds__(kThreads) k_scatter_atoms(DevArgs a) {
-  pdl_release();
-  pdl_wait();
-  __shared__ float oc[9];
-  const int f = blockIdx.y;
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (threadIdx.x < 9) oc[threadIdx.x] = a.geom[f * kGeom + threadIdx.x];
+  if (t == a.T - 1 && tid == 0) a.offsets[static_cast<int64_t>(f) * (a.nbins + 1) + a.nbins] = e1;
   __syncthreads();
-  if (e >= a.M) return;
-  const int at = a.entry_atom[e];
-  const float *p = a.xyz + f * a.frame_stride + 3ll * at;
-  const float x0 = p[0], y0 = p[1], z0 = p[2];
-  const float r0 = grid_coord(oc + 0, x0, y0, z0, a.n[0]);
-  const float r1 = grid_coord(oc + 3, x0, y0, z0, a.n[1]);
-  const float r2 = grid_coord(oc + 6, x0, y0, z0, a.n[2]);
-  const int2 k = a.key[static_cast<int64_t>(f) * a.M + e];
-  const int pos = a.offsets[static_cast<int64_t>(f) * (a.nbins + 1) + k.x] + k.y;
-  a.rec[static_cast<int64_t>(f) * a.M + pos] = make_float4(r0, r1, r2, __int_as_float(e));
+  float4 *rec = a.rec + static_cast<int64_t>(f) * a.M;
+  for (int e = e0 + tid; e < e1; e += kSortThreads) {
+    const float *p = xyz + 3ll * a.entry_atom[e];
+    const float x0 = p[0], y0 = p[1], z0 = p[2];
+    const int2 k = key[e];
+    rec[e0 + scnt[k.x] + k.y] = make_float4(grid_coord(oc + 0, x0, y0, z0, a.n[0]),
+                                            grid_coord(oc + 3, x0, y0, z0, a.n[1]),
+                                            grid_coord(oc + 6, x0, y0, z0, a.n[2]), __int_as_float(e));
+  }
 }
 
 // The atoms of up to 16 home bins of one tile, as one flat range: bin j holds
@@ -2899,9 +2895,8 @@ struct Ring {
 };
 
 // Timed stages of saxs_forward, in launch order.
-enum Stage { kStBin, kStScan, kStScatter, kStSpread, kStYdft, kStXdft, kStHist, kStages };
-const char *kStageNames[kStages] = {"k_bin_atoms", "k_scan", "k_scatter_atoms", "k_spread_zdft",
-                                    "k_ydft", "k_xdft_post", "k_hist"};
+enum Stage { kStSort, kStSpread, kStYdft, kStXdft, kStHist, kStages };
+const char *kStageNames[kStages] = {"k_sort_atoms", "k_spread_zdft", "k_ydft", "k_xdft_post", "k_hist"};
 
 struct StageRecord {
   cudaEvent_t start[kStages] = {};
@@ -2924,7 +2919,7 @@ struct SaxsPlan {
   int frames = 0;            // frames accumulated
   int last_frame_batch = 0;  // frames in the last forward batch
   size_t bytes = 0;
-  size_t smem_spread = 0, smem_ydft = 0, smem_xdft = 0, smem_hist = 0, smem_bin = 0;
+  size_t smem_spread = 0, smem_ydft = 0, smem_xdft = 0, smem_hist = 0;
   std::vector<void *> allocations;
   Ring ring;
   float *d_geom0 = nullptr;
@@ -3443,11 +3438,11 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
   pl->ytc_ok = pl->use_ytc;
   pl->xtc_ok = pl->use_xtc;
   pl->smem_hist = a.num_bins <= kHistSmemBins ? 2 * sizeof(double) * a.num_bins : 0;
-  pl->smem_bin = static_cast<size_t>(kThreads / 32) * a.T * sizeof(double);
+  const size_t smem_sort = sizeof(int) * static_cast<size_t>(a.tiles[0]) * a.tiles[1];
   if (pl->smem_spread + static_smem(k_spread_zdft) > optin ||
       pl->smem_ydft + static_smem(k_ydft) > optin ||
       pl->smem_xdft + static_smem(k_xdft_post) > optin ||
-      pl->smem_hist + static_smem(k_hist<double>) > optin || pl->smem_bin > 40 * 1024) {
+      pl->smem_hist + static_smem(k_hist<double>) > optin || smem_sort + static_smem(k_sort_atoms) > optin) {
     destroy(pl);
     return fail(SAXS_E_INVALID,
                 "grid / q-cut combination exceeds the shared-memory budget (z extent " +
@@ -3475,6 +3470,21 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
   } while (0)
   ALLOC(d_ea, a.M);
   ALLOC(d_et, a.M);
+  int *d_ts = nullptr;
+  ALLOC(d_ts, a.T + 1);
+  // entries grouped by type (stable), the sort kernel's per-type ranges
+  std::vector<int32_t> ea_sorted(a.M), et_sorted(a.M);
+  std::vector<int> type_start(a.T + 1, 0);
+  for (int i = 0; i < a.M; ++i) ++type_start[p.entry_type[i] + 1];
+  for (int t = 0; t < a.T; ++t) type_start[t + 1] += type_start[t];
+  {
+    std::vector<int> fill(type_start.begin(), type_start.end() - 1);
+    for (int i = 0; i < a.M; ++i) {
+      const int k = fill[p.entry_type[i]]++;
+      ea_sorted[k] = p.entry_atom[i];
+      et_sorted[k] = p.entry_type[i];
+    }
+  }
   ALLOC(d_twz, static_cast<size_t>(ez) * a.nkzp);
   ALLOC(d_twy, static_cast<size_t>(ey) * a.nkyp);
   ALLOC(d_twx, static_cast<size_t>(ex) * a.nkxp);
@@ -3500,7 +3510,6 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
   ALLOC(pl->d_geom0, kGeom);
   ALLOC(d_status, 4);
   ALLOC(a.key, static_cast<size_t>(B) * a.M);
-  ALLOC(a.counts, static_cast<size_t>(B) * a.nbins);
   ALLOC(a.offsets, static_cast<size_t>(B) * (a.nbins + 1));
   ALLOC(a.rec, static_cast<size_t>(B) * a.M);
   ALLOC(a.border, static_cast<size_t>(B) * a.T);
@@ -3513,6 +3522,7 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
   if (pl->ensemble == SAXS_NVT) ALLOC(a.iacc, static_cast<size_t>(a.nkz) * a.nky * a.nkx);
 #undef ALLOC
   a.entry_atom = d_ea;
+  a.type_start = d_ts;
   a.entry_type = d_et;
   a.twz = d_twz;
   a.twy = d_twy;
@@ -3615,8 +3625,9 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
     if (e != cudaSuccess) return fail(SAXS_E_CUDA, std::string("upload: ") + cudaGetErrorString(e));
     return SAXS_OK;
   };
-  if ((rc = up(d_ea, p.entry_atom, sizeof(int32_t) * a.M)) ||
-      (rc = up(d_et, p.entry_type, sizeof(int32_t) * a.M)) ||
+  if ((rc = up(d_ea, ea_sorted.data(), sizeof(int32_t) * a.M)) ||
+      (rc = up(d_et, et_sorted.data(), sizeof(int32_t) * a.M)) ||
+      (rc = up(d_ts, type_start.data(), sizeof(int) * (a.T + 1))) ||
       (rc = up(d_twz, twz.data(), sizeof(float2) * twz.size())) ||
       (rc = up(d_twy, twy.data(), sizeof(float2) * twy.size())) ||
       (rc = up(d_twx, twx.data(), sizeof(float2) * twx.size())) ||
@@ -3650,6 +3661,7 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
   // it is raised once to the largest value each kernel allows (the opt-in
   // per-block limit minus the kernel's static shared memory).
   if (e == cudaSuccess) e = raise_smem_limit(k_spread_zdft);
+  if (e == cudaSuccess) e = raise_smem_limit(k_sort_atoms);
   if (e == cudaSuccess) e = raise_smem_limit(k_ydft);
   if (e == cudaSuccess) e = raise_smem_limit(k_xdft_post);
   if (e == cudaSuccess) e = raise_smem_limit(k_hist<float>);
@@ -3753,6 +3765,13 @@ int launch_pdl(const char *name, void (*kernel)(KArgs...), dim3 grid, dim3 block
   return launch_check(name);
 }
 
+// Counting sort of `nframes` frames' atoms into home-bin order (the first kernel
+// of a batch: launched plainly).
+int launch_sort(const SaxsPlan *pl, const DevArgs &a, int nframes, cudaStream_t st) {
+  k_sort_atoms<<<dim3(a.T, nframes), kSortThreads, sizeof(int) * a.tiles[0] * a.tiles[1], st>>>(a);
+  return launch_check("k_sort_atoms");
+}
+
 // Spreading + z-axis DFT of `nframes` frames: the wide-tile or 64-column
 // tensor-core kernel the plan is configured for, else the FP32 SIMT kernel.
 int launch_spread(const SaxsPlan *pl, const DevArgs &a, int nframes, cudaStream_t st) {
@@ -3848,30 +3867,16 @@ int launch_xdft(const SaxsPlan *pl, const DevArgs &a, int nframes, cudaStream_t 
 // geometry is already in (or queued for) a.geom.  Host work free, so that it can
 // be captured in a CUDA graph.
 int enqueue_batch(SaxsPlan *pl, const DevArgs &a, int nframes, cudaStream_t st, bool timed) {
-  CUDA_TRY(cudaMemsetAsync(a.counts, 0, sizeof(int) * nframes * a.nbins, st));
-  CUDA_TRY(cudaMemsetAsync(a.border, 0, sizeof(double) * nframes * a.T, st));
-
   StageTimer tm{pl, nullptr, st};
   if (timed && pl->profiling) {
     pl->prof_pending.emplace_back();
     tm.rec = &pl->prof_pending.back();
   }
-  if (a.M > 0) {
-    dim3 gb((a.M + kThreads - 1) / kThreads, nframes);
-    tm.begin(kStBin);
-    k_bin_atoms<<<gb, kThreads, pl->smem_bin, st>>>(a);
-    tm.end(kStBin);
-    if (int rc = launch_check("k_bin_atoms")) return rc;
-    tm.begin(kStScan);
-    const int rc_scan = launch_pdl("k_scan", k_scan, dim3(nframes), dim3(1024), 0, st, a);
-    tm.end(kStScan);
-    if (rc_scan) return rc_scan;
-    tm.begin(kStScatter);
-    const int rc_sc = launch_pdl("k_scatter_atoms", k_scatter_atoms, gb, dim3(kThreads), 0, st, a);
-    tm.end(kStScatter);
-    if (rc_sc) return rc_sc;
-  } else {
-    CUDA_TRY(cudaMemsetAsync(a.offsets, 0, sizeof(int) * nframes * (a.nbins + 1), st));
+  {
+    tm.begin(kStSort);
+    const int rc = launch_sort(pl, a, nframes, st);
+    tm.end(kStSort);
+    if (rc) return rc;
   }
   {
     tm.begin(kStSpread);
@@ -4201,19 +4206,10 @@ int backward(SaxsPlan *pl, const float *xyz, const float *box, const double *dl,
                            cudaMemcpyHostToDevice, st));
   CUDA_TRY(cudaEventRecord(ring.ev[slot], st));
   CUDA_TRY(cudaMemcpyAsync(pl->d_adj_dl, dl, sizeof(double) * a.num_bins, cudaMemcpyHostToDevice, st));
-  CUDA_TRY(cudaMemsetAsync(a.counts, 0, sizeof(int) * a.nbins, st));
-  CUDA_TRY(cudaMemsetAsync(a.border, 0, sizeof(double) * a.T, st));
   CUDA_TRY(cudaMemsetAsync(pl->d_adj_S, 0, sizeof(double) * a.T, st));
   CUDA_TRY(cudaMemsetAsync(grad, 0, sizeof(float) * 3 * static_cast<size_t>(pl->p.natoms), st));
   // recompute the frame's y-transformed planes (nothing is kept from the forward)
-  if (a.M > 0) {
-    dim3 gb((a.M + kThreads - 1) / kThreads, 1);
-    k_bin_atoms<<<gb, kThreads, pl->smem_bin, st>>>(a);
-    k_scan<<<1, 1024, 0, st>>>(a);
-    k_scatter_atoms<<<gb, kThreads, 0, st>>>(a);
-  } else {
-    CUDA_TRY(cudaMemsetAsync(a.offsets, 0, sizeof(int) * (a.nbins + 1), st));
-  }
+  if (int rc = launch_sort(pl, a, 1, st)) return rc;
   if (int rc = launch_spread(pl, a, 1, st)) return rc;
   if (int rc = launch_ydft(pl, a, a.T * a.nkz, st)) return rc;
   const int items = a.stiles[0] * a.stiles[1] * a.T;  // 8 x 8 column tiles of the z adjoint
@@ -4254,7 +4250,7 @@ namespace {
 
 // Byte offsets of the per-frame buffers inside one scratch block.
 struct ScratchLayout {
-  size_t geom, key, counts, offsets, rec, border, Z, Y, ibox, total;
+  size_t geom, key, offsets, rec, border, Z, Y, ibox, total;
 };
 
 ScratchLayout scratch_layout(const DevArgs &a) {
@@ -4265,8 +4261,6 @@ ScratchLayout scratch_layout(const DevArgs &a) {
   o = up(o + sizeof(float) * kGeom);
   L.key = o;
   o = up(o + sizeof(int2) * static_cast<size_t>(a.M));
-  L.counts = o;
-  o = up(o + sizeof(int) * static_cast<size_t>(a.nbins));
   L.offsets = o;
   o = up(o + sizeof(int) * (static_cast<size_t>(a.nbins) + 1));
   L.rec = o;
@@ -4303,7 +4297,6 @@ int forward_into_scratch(SaxsPlan *pl, const float *xyz, const float *box, unsig
   a.frame_stride = 3ll * pl->p.natoms;
   a.geom = reinterpret_cast<const float *>(scratch + L.geom);
   a.key = reinterpret_cast<int2 *>(scratch + L.key);
-  a.counts = reinterpret_cast<int *>(scratch + L.counts);
   a.offsets = reinterpret_cast<int *>(scratch + L.offsets);
   a.rec = reinterpret_cast<float4 *>(scratch + L.rec);
   a.border = reinterpret_cast<double *>(scratch + L.border);
@@ -4328,21 +4321,9 @@ int forward_into_scratch(SaxsPlan *pl, const float *xyz, const float *box, unsig
                            cudaMemcpyHostToDevice, st));
   CUDA_TRY(cudaEventRecord(ring.ev[slot], st));
   // the block keeps the previous call's contents: clear what accumulates
-  CUDA_TRY(cudaMemsetAsync(a.counts, 0, sizeof(int) * a.nbins, st));
-  CUDA_TRY(cudaMemsetAsync(a.border, 0, sizeof(double) * a.T, st));
   CUDA_TRY(cudaMemsetAsync(hist, 0, sizeof(double) * a.num_bins, st));
   CUDA_TRY(cudaMemsetAsync(nhist, 0, sizeof(double) * a.num_bins, st));
-  if (a.M > 0) {
-    dim3 gb((a.M + kThreads - 1) / kThreads, 1);
-    k_bin_atoms<<<gb, kThreads, pl->smem_bin, st>>>(a);
-    if (int rc = launch_check("k_bin_atoms")) return rc;
-    k_scan<<<1, 1024, 0, st>>>(a);
-    if (int rc = launch_check("k_scan")) return rc;
-    k_scatter_atoms<<<gb, kThreads, 0, st>>>(a);
-    if (int rc = launch_check("k_scatter_atoms")) return rc;
-  } else {
-    CUDA_TRY(cudaMemsetAsync(a.offsets, 0, sizeof(int) * (a.nbins + 1), st));
-  }
+  if (int rc = launch_sort(pl, a, 1, st)) return rc;
   if (int rc = launch_spread(pl, a, 1, st)) return rc;
   if (int rc = launch_ydft(pl, a, a.T * a.nkz, st)) return rc;
   if (int rc = launch_xdft(pl, a, 1, st)) return rc;
