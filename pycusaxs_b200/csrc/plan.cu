@@ -2,13 +2,13 @@
 //
 // Pipeline of one batch of frames (all kernels hand-written for sm_100a):
 //
-//   k_sort_atoms    one CTA per (type, frame): atoms -> float32 grid
-//                   coordinates (the reference's float steps,
+//   k_sort_atoms    one thread-block cluster per (type, frame): atoms ->
+//                   float32 grid coordinates (the reference's float steps,
 //                   saxsDeviceKernels.cu:355-368), counting sort into
-//                   (type, home tile) order in shared memory, per-type FP64
-//                   z-border sums for the padding mean
-//                   (saxsDeviceKernels.cu:446-465 evaluated per atom instead of
-//                   per voxel).
+//                   (type, home tile) order with shared-memory counters shared
+//                   across the cluster, per-type FP64 z-border sums for the
+//                   padding mean (saxsDeviceKernels.cu:446-465 evaluated per
+//                   atom instead of per voxel).
 //   k_spread_zdft   one CTA per (frame, type, 8x8 column tile): B-spline
 //                   spreading into a shared-memory column tile (no global
 //                   atomics), mean padding folded in as "subtract the mean",
