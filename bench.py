@@ -324,11 +324,19 @@ def bench_ours(args):
                 "peak_source": "measured" if peaks else "fallback"}
     if dom in algo_flops:
         useful = algo_flops[dom] * frames_per_launch / per_launch_s / 1e12
-        if tensor:
+        if tensor and dom == "k_spread_zdft" and path & 8:
+            # wide z kernel: f16 head/remainder of both operands, two kind::f16 MMAs per
+            # 16 z against [Bh | Bl], so four f16 products issued per useful one; the
+            # dense f16 rate equals the bf16 one
+            f16_peak = float(peaks.get("bf16_tflops", 1590.0))
+            roofline["tensor"] = {"useful_tflops": round(useful, 2), "issued_tflops": round(4 * useful, 2),
+                                  "mma_kind": "f16", "peak_tflops": f16_peak,
+                                  "issued_frac": round(4 * useful / f16_peak, 4)}
+        elif tensor:
             # 3xTF32: three TF32 MMAs per product; dense TF32 peak = half the bf16 one
             tf32_peak = float(peaks.get("bf16_tflops", 1590.0)) / 2
             roofline["tensor"] = {"useful_tflops": round(useful, 2), "issued_tflops": round(3 * useful, 2),
-                                  "tf32_peak_tflops": tf32_peak,
+                                  "mma_kind": "tf32", "peak_tflops": tf32_peak,
                                   "issued_frac": round(3 * useful / tf32_peak, 4)}
         else:
             roofline["fp32_tflops"] = round(useful, 2)

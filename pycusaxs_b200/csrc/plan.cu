@@ -31,6 +31,7 @@
 // k = 0, evaluated exactly by three pruned DFT passes that never touch the
 // zero region.
 #include <cuda.h>  // CUtensorMap and its enums (the encoder is fetched at run time)
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -113,7 +114,7 @@ struct DevArgs {
   const float *ff;    // [T][9]
   const float *twz_sum; // [2*nkzp]: sum over z < ez of the z twiddles (re, im)
   const float *twz_tc;  // [2][tcK x tcN]: z twiddles as TF32 head / remainder, K-major
-  const float *twz_tcw; // [tcK x 2*twN]: head and remainder side by side (wide tiles)
+  const float *twz_tcw; // [tcK x 2*twN] f16 (wide tiles): head and remainder side by side
   const int4 *home_x; // per spread tile along x: home tiles whose atoms reach it (-1 padded)
   const int4 *home_y;
   const int4 *home_yw; // per 16-row y tile: up to eight home tiles (two int4, -1 padded)
@@ -741,6 +742,17 @@ __device__ __forceinline__ void umma_tf32_ts(uint32_t tmem_d, uint32_t tmem_a, u
       "r"(tmem_a), "l"(db), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
 }
 
+// The same with kind::f16 (f16 A and B, FP32 D, K = 16): A in tensor memory
+// holds two K-consecutive halves per 32-bit column, the even one in the low half.
+__device__ __forceinline__ void umma_f16_ts(uint32_t tmem_d, uint32_t tmem_a, uint64_t db, uint32_t idesc,
+                                            uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
+      "r"(tmem_a), "l"(db), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+
 __device__ __forceinline__ uint64_t global_ns() {
   uint64_t t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -751,18 +763,26 @@ __device__ __forceinline__ uint64_t global_ns() {
 // thread until the phase completes or 0.1 ms pass (so waiting warps do not take
 // issue slots from working ones); gives up after 2^16 tries or 2 s, whichever
 // comes first, and returns false.
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred P1;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2, %3;\n\t"
+      "selp.b32 %0, 1, 0, P1;\n\t}\n"
+      : "=r"(done)
+      : "r"(bar), "r"(parity), "r"(100000)
+      : "memory");
+  return done != 0;
+}
+
+// Bounded wait: at most 2^16 + 1 tries and 2 s.  The global timer is read only
+// once the first try has failed (a read of it costs hundreds of cycles, and most
+// waits in the pipelines below find their phase already complete).
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  if (mbar_try(bar, parity)) return true;
   const uint64_t t0 = global_ns();
   for (int it = 0; it < (1 << 16); ++it) {
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred P1;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2, %3;\n\t"
-        "selp.b32 %0, 1, 0, P1;\n\t}\n"
-        : "=r"(done)
-        : "r"(bar), "r"(parity), "r"(100000)
-        : "memory");
-    if (done) return true;
+    if (mbar_try(bar, parity)) return true;
     if (global_ns() - t0 > 2000000000ull) return false;
   }
   return false;
@@ -1282,6 +1302,7 @@ constexpr int kTwLoaderWarp = kTwProducerWarps + 1;
 constexpr int kTwReleaseWarp = kTwProducerWarps + 6;
 constexpr int kTwThreads = 32 * (kTwProducerWarps + 7);  // producers, MMA, loader, 4 epilogue, release
 constexpr int kTwChunk = 32; // z per A ring slot
+constexpr int kTwSlotCols = 32;  // tensor-memory columns of an A ring slot: 16 head + 16 remainder (f16 pairs)
 constexpr int kTwRing = 4;   // A ring slots
 
 // Record ranges of an item's home bins (up to 4 along x times 8 along y).
@@ -1295,7 +1316,34 @@ struct TwSlot {
   TileAtomsW ta;
   int f, t, x0, y0, cw, ch;
   float mean;
+  float scale;    // fixed-point scale of the item's tile (see tw_scale)
+  float mean_fx;  // mean * scale
 };
+
+// The wide kernel accumulates its tile in 32-bit fixed point: shared-memory
+// integer atomics issue about three times faster than FP32 ones on sm_100
+// (1.97 against 6.6 cycles per warp-wide add per SM, measured).  A voxel of
+// column (x, y) receives taps only from atoms whose home columns lie within
+// four columns of it in x and in y: at most 3 x 3 home bins (2 x 2 unless a
+// partial bin at the periodic edge is crossed), and each tap is a product of
+// three B-spline weights of at most 2/3.  With `most` the largest home-bin
+// count of the item, no voxel exceeds min(nvis, 9 * most) * (8/27) and each
+// rounded tap adds at most 1/2, so the scale 2^e with
+// 2^e * (0.3 * bound + |mean|) <= 2e9 keeps every sum, and every sum minus
+// mean * 2^e, below 2^31 in magnitude.  Each tap is rounded to 1/scale; at the
+// 100k-atom workload (bound ~700, scale 2^23) that is an absolute error of at
+// most 6e-8 per tap.
+__device__ __forceinline__ float tw_scale(int nvis, int most, float mean) {
+  const float bound = static_cast<float>(max(1, min(nvis, 9 * most)));
+  const float e = floorf(log2f(2.0e9f / (0.3f * bound + fabsf(mean))));
+  return exp2f(fminf(e, 30.0f));
+}
+
+// Padding mean of the item's type and frame, and the item's fixed-point scale:
+// the loader and the epilogue evaluate the same expressions (one full warp).
+__device__ __forceinline__ float tw_item_mean(const DevArgs &a, int f, int t) {
+  return a.pad_val ? a.pad_val[t] : static_cast<float>(a.border[static_cast<int64_t>(f) * a.T + t] / a.border_count);
+}
 
 // Loader, first half, for wide tiles: lane 4*iy + ix loads the record range of
 // home bin (hx[ix], hy[iy]); home_y holds eight bins per wide y tile.
@@ -1407,13 +1455,14 @@ __device__ __forceinline__ void spread_prepass_w(const DevArgs &a, const TileAto
 // takes two units per round and reads both units' table entries before either
 // unit's atomics, so the shared-memory loads of one overlap the other.
 struct TapUnit {
-  float *col;     // tile row start of the unit's (y tap, z tap), or null when outside
+  int *col;       // tile row start of the unit's (y tap, z tap), or null when outside
   int lxp;        // the atom's four x-tap columns, one byte each (0xFF outside)
-  float w;        // wy * wz
+  float w;        // wy * wz * scale
   float4 wx;
 };
 
-__device__ __forceinline__ TapUnit tap_unit(const AtomTab &tab, int u, int nu, int nt, float *A, int rs) {
+__device__ __forceinline__ TapUnit tap_unit(const AtomTab &tab, int u, int nu, int nt, int *A, int rs,
+                                            float scale) {
   TapUnit t;
   t.col = nullptr;
   if (u >= nu) return t;
@@ -1426,7 +1475,7 @@ __device__ __forceinline__ TapUnit tap_unit(const AtomTab &tab, int u, int nu, i
   const float wz = reinterpret_cast<const float *>(&tab.wz[i])[r];
   const int zo = reinterpret_cast<const int *>(&tab.zo[i])[r];
   t.wx = tab.wx[i];
-  t.w = wy * wz;
+  t.w = wy * wz * scale;
   t.col = A + zo + ly * rs;
   return t;
 }
@@ -1438,16 +1487,16 @@ __device__ __forceinline__ void tap_apply(const TapUnit &t, int rs) {
 #pragma unroll
   for (int o = 0; o < 4; ++o) {
     const int lx = (t.lxp >> (8 * o)) & 0xFF;
-    if (lx != 0xFF) atomicAdd(t.col + lx * kTwY * rs, wx[o] * wy_wz);
+    if (lx != 0xFF) atomicAdd(t.col + lx * kTwY * rs, __float2int_rn(wx[o] * wy_wz));
   }
 }
 
-__device__ __forceinline__ void spread_taps_w(const AtomTab &tab, int nv, int nt, float *A, int rs, int tid,
-                                              int nthreads) {
+__device__ __forceinline__ void spread_taps_w(const AtomTab &tab, int nv, int nt, int *A, int rs, float scale,
+                                              int tid, int nthreads) {
   const int nu = nv * 16;
   for (int u = tid; u < nu; u += 2 * nthreads) {
-    const TapUnit t0 = tap_unit(tab, u, nu, nt, A, rs);
-    const TapUnit t1 = tap_unit(tab, u + nthreads, nu, nt, A, rs);
+    const TapUnit t0 = tap_unit(tab, u, nu, nt, A, rs, scale);
+    const TapUnit t1 = tap_unit(tab, u + nthreads, nu, nt, A, rs, scale);
     tap_apply(t0, rs);
     tap_apply(t1, rs);
   }
@@ -1494,10 +1543,11 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
   __shared__ volatile int released;
   __shared__ int tab_count[2][2][2];  // reaching atoms in the table: [group][item parity][chunk parity]
   const int NB = a.twN, N = 2 * a.twN, KT = a.tcK, R = a.tcR, RB = a.twRB, RS = a.twRS, G = a.twG;
+  const int SR = 2;  // split warps per lane quarter (16 z of a chunk each); 4 measured slower
   const int CH = (KT + kTwChunk - 1) / kTwChunk;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  float *bh = reinterpret_cast<float *>(smem);  // B' = [Bh | Bl], K-major, N columns
-  float *tiles = bh + KT * N;
+  float *bh = reinterpret_cast<float *>(smem);  // B' = [Bh | Bl], f16, K-major, N columns
+  float *tiles = bh + KT * N / 2;
   float4 *recs = reinterpret_cast<float4 *>(tiles + static_cast<size_t>(G) * 128 * RS);
   int4 *home_x = reinterpret_cast<int4 *>(recs + 2 * RB);
   int4 *home_y = home_x + a.stiles[0];
@@ -1518,7 +1568,7 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
   {
     const float4 *src = reinterpret_cast<const float4 *>(a.twz_tcw);
     float4 *dst = reinterpret_cast<float4 *>(bh);
-    for (int i = tid; i < KT * N / 4; i += blockDim.x) dst[i] = src[i];
+    for (int i = tid; i < KT * N / 8; i += blockDim.x) dst[i] = src[i];
     float4 *t4 = reinterpret_cast<float4 *>(tiles);
     for (int i = tid; i < G * 32 * RS; i += blockDim.x) t4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     for (int i = tid; i < a.stiles[0]; i += blockDim.x) home_x[i] = a.home_x[i];
@@ -1533,7 +1583,7 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
   if (tid == 0) {
     for (int i = 0; i < 4 + 2 * kTwRing + 4; ++i) {
       int cnt = 1;
-      if (i >= 4 && i < 4 + kTwRing) cnt = 8;  // a_full: 4 lane quarters x 2 units
+      if (i >= 4 && i < 4 + kTwRing) cnt = 4 * SR;  // a_full: 4 lane quarters x SR split warps
       if (i >= 4 + 2 * kTwRing + 2) cnt = 4;   // acc_empty: 4 epilogue warps
       asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&bars[i])), "r"(cnt));
     }
@@ -1558,6 +1608,10 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
   };
   // bounded wait until the MMAs of the first `n` chunks are complete
   auto wait_released = [&](int n) {
+    if (released >= n || abort_flag) {
+      __threadfence_block();
+      return;
+    }
     const uint64_t t0 = global_ns();
     while (released < n && !abort_flag) {
       if (global_ns() - t0 > 2000000000ull) {
@@ -1576,11 +1630,11 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
     const int quarter = warp & 3, rq = gw >> 2;
     const int m = 32 * quarter + lane;             // the tile row this lane splits
     float *row = A + static_cast<size_t>(m) * RS;
-    // split warps: rank < 2 in their lane quarter (group threads 0..255); the
-    // group's other warps pre-pass the next item's first table chunk while the
-    // split warps split the current item
-    const bool splitter = rq < 2;
-    const int ns_tid = gtid - 256, ns_threads = gthreads - 256;
+    // split warps: rank < SR in their lane quarter (group threads 0..128*SR-1);
+    // the group's other warps pre-pass the next item's first table chunk while
+    // the split warps split the current item
+    const bool splitter = rq < SR;
+    const int ns_tid = gtid - 128 * SR, ns_threads = gthreads - 128 * SR;
     for (int j = group, w = blockIdx.x + group * gridDim.x; w < items; j += G, w += G * gridDim.x) {
       const int b = j & 1, ip = (j / G) & 1;
       wait(&rec_full[b], j >> 1);
@@ -1595,7 +1649,7 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
       // the first chunk's table is complete and the previous item's split done
       const bool skip = producers_sync_or(abort_flag != 0, bar_id, gthreads);
       if (gtid == 0) tab_count[group][ip ^ 1][0] = tab_count[group][ip ^ 1][1] = 0;  // the next item's
-      const float mean = sl.mean;
+      const float mean_fx = sl.mean_fx;
       if (!skip) {
         const int nvis = sl.ta.cum[sl.ta.nb];
         const int nrec = min(nvis, RB);
@@ -1609,14 +1663,15 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
                              tab, sl.x0, sl.y0, sl.cw, sl.ch, gtid, gthreads, &tab_count[group][ip][k & 1]);
             producers_sync(bar_id, gthreads);
           }
-          spread_taps_w(tab, tab_count[group][ip][k & 1], a.ntaps, A, RS, gtid, gthreads);
+          spread_taps_w(tab, tab_count[group][ip][k & 1], a.ntaps, reinterpret_cast<int *>(A), RS, sl.scale,
+                        gtid, gthreads);
         }
       }
       producers_sync(bar_id, gthreads);
       if (gtid == 0) mbar_arrive(smem_addr(&rec_empty[b]));
       if (!splitter) continue;
       // rows z in [tcK, tcR) meet no twiddle: cleared for the next item
-      for (int i = gtid; i < 128 * ((R - KT) / 4); i += 256) {
+      for (int i = gtid; i < 128 * ((R - KT) / 4); i += 128 * SR) {
         const int mm = i / ((R - KT) / 4), zq = i % ((R - KT) / 4);
         reinterpret_cast<float4 *>(A + static_cast<size_t>(mm) * RS + KT)[zq] = make_float4(0.f, 0.f, 0.f, 0.f);
       }
@@ -1627,38 +1682,42 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
         __syncwarp();  // converged for the .sync.aligned tensor-memory stores
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const int h = rq;
-        // two halves of 8 z: head to the slot's first 32 columns, remainder to the next 32
-#pragma unroll
-        for (int sub = 0; sub < 2; ++sub) {
-          const int z0 = kTwChunk * c + 16 * h + 8 * sub;
+        // 16 z per split warp: (tile - mean) * 2^-17 in fixed-point units, split
+        // into an f16 head and remainder; two halves per tensor-memory column,
+        // head to the slot's first 16 columns, remainder to the next 16
+        {
+          const int z0 = kTwChunk * c + 16 * h;
           uint32_t hi[8], lo[8];
+          // all four loads, then the zeroing stores, then the arithmetic
+          int4 iv[4];
+          int4 *p = reinterpret_cast<int4 *>(row + z0);
+          const int nq = z0 < KT ? 4 : 0;  // KT is a multiple of 16: all or none of the 16 z
 #pragma unroll
-          for (int k4 = 0; k4 < 2; ++k4) {
-            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (z0 + 4 * k4 < KT) {
-              float4 *p = reinterpret_cast<float4 *>(row + z0 + 4 * k4);
-              v = *p;
-              *p = make_float4(0.f, 0.f, 0.f, 0.f);
-              v.x -= mean;
-              v.y -= mean;
-              v.z -= mean;
-              v.w -= mean;
-            }
-            const float vv[4] = {v.x, v.y, v.z, v.w};
+          for (int k4 = 0; k4 < 4; ++k4) iv[k4] = k4 < nq ? p[k4] : make_int4(0, 0, 0, 0);
 #pragma unroll
-            for (int e = 0; e < 4; ++e) {
-              const float hh = tf32_head(vv[e]);
-              hi[4 * k4 + e] = __float_as_uint(hh);
-              lo[4 * k4 + e] = __float_as_uint(vv[e] - hh);
+          for (int k4 = 0; k4 < 4; ++k4)
+            if (k4 < nq) p[k4] = make_int4(0, 0, 0, 0);
+          const float mz = z0 < KT ? mean_fx : 0.0f;
+#pragma unroll
+          for (int k4 = 0; k4 < 4; ++k4) {
+            const float v[4] = {(__int2float_rn(iv[k4].x) - mz) * 0x1p-17f, (__int2float_rn(iv[k4].y) - mz) * 0x1p-17f,
+                                (__int2float_rn(iv[k4].z) - mz) * 0x1p-17f, (__int2float_rn(iv[k4].w) - mz) * 0x1p-17f};
+#pragma unroll
+            for (int e = 0; e < 4; e += 2) {
+              const __half2 hh = __floats2half2_rn(v[e], v[e + 1]);
+              const float2 hf = __half22float2(hh);
+              const __half2 ll = __floats2half2_rn(v[e] - hf.x, v[e + 1] - hf.y);
+              hi[2 * k4 + e / 2] = *reinterpret_cast<const uint32_t *>(&hh);
+              lo[2 * k4 + e / 2] = *reinterpret_cast<const uint32_t *>(&ll);
             }
           }
           const uint32_t dst = tmem + (static_cast<uint32_t>(32 * quarter) << 16) +
-                               static_cast<uint32_t>(64 * s + 16 * h + 8 * sub);
+                               static_cast<uint32_t>(kTwSlotCols * s + 8 * h);
           asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"r"(dst),
                        "r"(hi[0]), "r"(hi[1]), "r"(hi[2]), "r"(hi[3]), "r"(hi[4]), "r"(hi[5]), "r"(hi[6]),
                        "r"(hi[7])
                        : "memory");
-          asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"r"(dst + 32),
+          asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"r"(dst + 16),
                        "r"(lo[0]), "r"(lo[1]), "r"(lo[2]), "r"(lo[3]), "r"(lo[4]), "r"(lo[5]), "r"(lo[6]),
                        "r"(lo[7])
                        : "memory");
@@ -1671,11 +1730,11 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
     }
   } else if (warp == kTwMmaWarp) {
     if (lane == 0) {
-      // kind::tf32, D f32, A from tensor memory, B' K-major, N >> 3 at bit 17, M = 128
-      const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) |
-                             (static_cast<uint32_t>(N >> 3) << 17) | (static_cast<uint32_t>(128 >> 4) << 24);
+      // kind::f16 (f16 A and B), D f32, A from tensor memory, B' K-major, N >> 3 at bit 17, M = 128
+      const uint32_t idesc = (1u << 4) | (static_cast<uint32_t>(N >> 3) << 17) |
+                             (static_cast<uint32_t>(128 >> 4) << 24);
       const uint64_t db0 = umma_desc(smem_addr(bh), N * 16, 128);
-      const uint64_t bstep = static_cast<uint64_t>(N) * 2;  // 8 z of B' in 16-byte units
+      const uint64_t bstep = static_cast<uint64_t>(N) * 2;  // 16 z of f16 B' in 16-byte units
       int j = 0;
       uint32_t last_bar = 0;
       int last_parity = 0;
@@ -1688,12 +1747,12 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
           if (c == 0 && j >= 2) wait(&acc_empty[d], (j - 2) >> 1);
           if (abort_flag) break;
           asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-          const int ks = min(kTwChunk, KT - kTwChunk * c) / 8;
+          const int ks = min(kTwChunk, KT - kTwChunk * c) / 16;
           for (int kk = 0; kk < ks; ++kk) {
-            const uint32_t ahi = tmem + static_cast<uint32_t>(64 * s + 8 * kk);
-            const uint64_t db = db0 + static_cast<uint64_t>(kTwChunk / 8 * c + kk) * bstep;
-            umma_tf32_ts(dcol, ahi + 32, db, idesc, (c | kk) ? 1u : 0u);
-            umma_tf32_ts(dcol, ahi, db, idesc, 1u);
+            const uint32_t ahi = tmem + static_cast<uint32_t>(kTwSlotCols * s + 8 * kk);
+            const uint64_t db = db0 + static_cast<uint64_t>(kTwChunk / 16 * c + kk) * bstep;
+            umma_f16_ts(dcol, ahi + 16, db, idesc, (c | kk) ? 1u : 0u);
+            umma_f16_ts(dcol, ahi, db, idesc, 1u);
           }
           asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                            smem_addr(&a_empty[s]))
@@ -1718,8 +1777,9 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
       int s0, cnt;
       bool valid;
       home_ranges_load_w(a, home_x, home_y, it.f, it.t, it.tx, it.ty, s0, cnt, valid);
-      const float pmean = a.pad_val ? a.pad_val[it.t] : 0.0f;
-      const double bsum = a.pad_val ? 0.0 : a.border[static_cast<int64_t>(it.f) * a.T + it.t];
+      const int most = __reduce_max_sync(0xffffffffu, static_cast<unsigned>(valid ? cnt : 0));
+      const int nall = __reduce_add_sync(0xffffffffu, static_cast<unsigned>(valid ? cnt : 0));
+      const float mean = tw_item_mean(a, it.f, it.t);
       if (j >= 2) wait(&rec_empty[b], (j - 2) >> 1);
       if (__any_sync(0xffffffffu, abort_flag != 0)) break;
       TwSlot &sl = slot[b];
@@ -1731,7 +1791,9 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
         sl.y0 = y0;
         sl.cw = min(kTwX, a.ext[0] - x0);
         sl.ch = min(kTwY, a.ext[1] - y0);
-        sl.mean = a.pad_val ? pmean : static_cast<float>(bsum / a.border_count);
+        sl.mean = mean;
+        sl.scale = tw_scale(nall, most, mean);
+        sl.mean_fx = mean * sl.scale;
       }
       __syncwarp();
       if (lane == 0) {
@@ -1777,6 +1839,17 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
     int j = 0;
     for (int w = blockIdx.x; w < items; w += gridDim.x, ++j, it.next()) {
       const int d = j & 1;
+      // the item's fixed-point scale, as the loader computed it (before the wait,
+      // so that its loads overlap it): Z = D * 2^17 / scale
+      float unscale;
+      {
+        int s0, cnt;
+        bool valid;
+        home_ranges_load_w(a, home_x, home_y, it.f, it.t, it.tx, it.ty, s0, cnt, valid);
+        const int most = __reduce_max_sync(0xffffffffu, static_cast<unsigned>(valid ? cnt : 0));
+        const int nall = __reduce_add_sync(0xffffffffu, static_cast<unsigned>(valid ? cnt : 0));
+        unscale = 131072.0f / tw_scale(nall, most, tw_item_mean(a, it.f, it.t));
+      }
       wait(&acc_full[d], j >> 1);
       if (__any_sync(0xffffffffu, abort_flag != 0)) break;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -1804,8 +1877,8 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
             const int kz = c0 / 2 + jj;
             if (kz < a.nkz)
               Zft[kz * zplane + cell] =
-                  make_float2(__uint_as_float(r[2 * jj]) + __uint_as_float(t[2 * jj]),
-                              __uint_as_float(r[2 * jj + 1]) + __uint_as_float(t[2 * jj + 1]));
+                  make_float2((__uint_as_float(r[2 * jj]) + __uint_as_float(t[2 * jj])) * unscale,
+                              (__uint_as_float(r[2 * jj + 1]) + __uint_as_float(t[2 * jj + 1])) * unscale);
           }
         }
       }
@@ -3481,7 +3554,7 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
     const bool narrow_only = mode && std::strcmp(mode, "narrow") == 0;
     const int N = round_up(2 * a.nkz, 8);
     const int NW = round_up(2 * a.nkz, 16);  // M = 128 needs N a multiple of 16
-    const int KT = round_up(a.ext[2], 8);
+    const int KT = round_up(a.ext[2], 16);  // K = 16 per f16 MMA of the wide kernel
     const int R = std::max(KT, round_up(a.n[2], 8));
     const size_t avail = optin - static_smem(k_spread_zdft_tc);
     const size_t b_bytes = 2 * static_cast<size_t>(KT) * N * sizeof(float);
@@ -3508,7 +3581,7 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
     // the largest record buffer that fit beside the groups' FP32 tiles
     const int RSW = R + 4;
     const size_t home_w = static_cast<size_t>(a.stiles[0] + 2 * a.stw) * sizeof(int4);
-    const size_t bw_bytes = 2 * static_cast<size_t>(KT) * NW * sizeof(float);
+    const size_t bw_bytes = 2 * static_cast<size_t>(KT) * NW * sizeof(uint16_t);  // f16 B''
     auto wide_bytes = [&](int g, int rb, int cap) {
       return bw_bytes + static_cast<size_t>(g) * 128 * RSW * sizeof(float) + 2 * static_cast<size_t>(rb) * 16 +
              home_w + static_cast<size_t>(g) * cap * kTcAtomBytes;
@@ -3724,20 +3797,21 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
   };
   const std::vector<float> twtc = pl->tcn_ok ? z_operand(a.tcN) : std::vector<float>();
   // wide tiles: B' = [Bh | Bl] as one K-major operand of 2*twN columns
-  std::vector<float> twtcw;
+  // wide kernel: B' = [Bh | Bl] in f16, Bh the twiddle rounded to f16 and Bl the
+  // rounded remainder; element (z, n) at half ((z / 8) * 2twN + n) * 8 + z % 8
+  // (K-major, 16-byte K blocks of 2twN rows)
+  std::vector<__half> twtcw;
   if (pl->tcw_ok) {
-    const std::vector<float> hl = z_operand(a.twN);
     const int NB = a.twN, N2 = 2 * a.twN;
-    const size_t half = static_cast<size_t>(a.tcK) * NB;
-    twtcw.assign(2 * half, 0.0f);
-    for (int z = 0; z < a.tcK; ++z)
-      for (int n = 0; n < NB; ++n) {
-        const size_t o = static_cast<size_t>(z / 4) * (NB / 8) * 32 + (n / 8) * 32 + (n % 8) * 4 + z % 4;
-        for (int part = 0; part < 2; ++part) {
-          const int n2 = n + part * NB;
-          const size_t o2 = static_cast<size_t>(z / 4) * (N2 / 8) * 32 + (n2 / 8) * 32 + (n2 % 8) * 4 + z % 4;
-          twtcw[o2] = hl[part * half + o];
-        }
+    twtcw.assign(static_cast<size_t>(a.tcK) * N2, __float2half_rn(0.0f));
+    for (int z = 0; z < ez; ++z)
+      for (int n = 0; n < 2 * a.nkz; ++n) {
+        const float2 w = twz[z * a.nkzp + n / 2];
+        const float v = (n & 1) ? w.y : w.x;
+        const __half h = __float2half_rn(v);
+        const __half l = __float2half_rn(v - __half2float(h));
+        twtcw[(static_cast<size_t>(z / 8) * N2 + n) * 8 + z % 8] = h;
+        twtcw[(static_cast<size_t>(z / 8) * N2 + n + NB) * 8 + z % 8] = l;
       }
   }
   std::vector<float2> twy(static_cast<size_t>(ey) * a.nkyp, make_float2(0.f, 0.f));
@@ -3780,7 +3854,7 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
       (rc = up(d_hx, hxt.data(), sizeof(int4) * hxt.size())) ||
       (rc = up(d_twzs, twzs.data(), sizeof(float) * twzs.size())) ||
       (rc = up(d_twztc, twtc.data(), sizeof(float) * twtc.size())) ||
-      (rc = up(d_twztcw, twtcw.data(), sizeof(float) * twtcw.size())) ||
+      (rc = up(d_twztcw, twtcw.data(), sizeof(__half) * twtcw.size())) ||
       (rc = up(d_twytc, twytc.data(), sizeof(float) * twytc.size())) ||
       (rc = up(d_twxtc, twxtc.data(), sizeof(float) * twxtc.size())) ||
       (rc = up(d_hy, hyt.data(), sizeof(int4) * hyt.size())) ||

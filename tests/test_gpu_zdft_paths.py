@@ -121,10 +121,12 @@ def test_tc_supercell_smaller_than_grid(cuda, zmode):
 
 
 def test_tc_single_operand_stage_long_z(cuda, zmode):
-    # z extent 256, 17 kz values (N = 48): twiddles 96 KB + one 128 KB operand stage
-    # fit shared memory, two stages do not; a wide tile (133 KB) does not fit
+    # z extent 256, 17 kz values (N = 48): the 64-column kernel's twiddles 96 KB +
+    # one 128 KB operand stage fit shared memory, two stages do not; the wide
+    # kernel's f16 twiddles (48 KB) fit beside its 133 KB tile: eight ring chunks
+    # per item
     s = _line_system(4000, (80.0, 80.0, 320.0), 16)
-    _both(s, (32, 32, 256), [s.positions], sigma=2.0, qcut=0.15, zmode=zmode, expect_wide=False)
+    _both(s, (32, 32, 256), [s.positions], sigma=2.0, qcut=0.15, zmode=zmode, expect_wide=True)
 
 
 def test_tc_many_kz_wide_n(cuda, zmode):
