@@ -260,7 +260,7 @@ __device__ __forceinline__ void cluster_st(uint32_t addr, double v) {
 // parameters (gp.g[j]) and CTA 0 of type 0 stores them to a.geom for the later
 // kernels, so that no host-to-device copy of them queues behind other transfers
 // on the copy engines; otherwise a.geom already holds them.
-constexpr int kSortThreads = 512, kSortU = 4, kSortMaxCluster = 8, kSortParamFrames = 96;
+constexpr int kSortThreads = 512, kSortU = 4, kSortMaxCluster = 8, kSortParamFrames = 128;
 struct SortGeom {
   float g[kSortParamFrames * kGeom];
 };
@@ -1326,17 +1326,28 @@ struct TwSlot {
 // column (x, y) receives taps only from atoms whose home columns lie within
 // four columns of it in x and in y: at most 3 x 3 home bins (2 x 2 unless a
 // partial bin at the periodic edge is crossed), and each tap is a product of
-// three B-spline weights of at most 2/3.  With `most` the largest home-bin
-// count of the item, no voxel exceeds min(nvis, 9 * most) * (8/27) and each
-// rounded tap adds at most 1/2, so the scale 2^e with
-// 2^e * (0.3 * bound + |mean|) <= 2e9 keeps every sum, and every sum minus
-// mean * 2^e, below 2^31 in magnitude.  Each tap is rounded to 1/scale; at the
-// 100k-atom workload (bound ~700, scale 2^23) that is an absolute error of at
-// most 6e-8 per tap.
-__device__ __forceinline__ float tw_scale(int nvis, int most, float mean) {
+// three B-spline weights: at most (2/3)^3 with two or more taps per axis, and
+// (1/6)^3 with one (only the first cubic weight is used).  With `most` the
+// largest home-bin count of the item, no voxel exceeds
+// min(nvis, 9 * most) * tapmax and each rounded tap adds at most 1/2, so the
+// scale 2^e with 2^e * (tapmax * bound + |mean|) <= 2e9 keeps every sum, and
+// every sum minus mean * 2^e, below 2^31 in magnitude.  The scale is also kept
+// at or below 2^22 / tapmax, so that a tap (below 2^22 units) can be rounded to
+// an integer by adding 1.5 * 2^23 in FP32 (tap_fixed).  Each tap is rounded to
+// 1/scale; at the 100k-atom workload (bound ~700, scale 2^23) that is an
+// absolute error of at most 6e-8 per tap.
+__device__ __forceinline__ float tw_scale(int nvis, int most, float mean, int ntaps) {
+  const float tapmax = ntaps >= 2 ? 0.2964f : 0.00464f;
   const float bound = static_cast<float>(max(1, min(nvis, 9 * most)));
-  const float e = floorf(log2f(2.0e9f / (0.3f * bound + fabsf(mean))));
-  return exp2f(fminf(e, 30.0f));
+  const float e = floorf(log2f(2.0e9f / (tapmax * bound + fabsf(mean))));
+  const float cap = floorf(log2f(4194304.0f / tapmax));
+  return exp2f(fminf(e, cap));
+}
+
+// round(a * b) for 0 <= a * b < 2^22: one FMA with 1.5 * 2^23 leaves the rounded
+// integer in the low mantissa bits (round to nearest even, as __float2int_rn).
+__device__ __forceinline__ int tap_fixed(float a, float b) {
+  return __float_as_int(fmaf(a, b, 12582912.0f)) - 0x4B400000;
 }
 
 // Padding mean of the item's type and frame, and the item's fixed-point scale:
@@ -1487,7 +1498,7 @@ __device__ __forceinline__ void tap_apply(const TapUnit &t, int rs) {
 #pragma unroll
   for (int o = 0; o < 4; ++o) {
     const int lx = (t.lxp >> (8 * o)) & 0xFF;
-    if (lx != 0xFF) atomicAdd(t.col + lx * kTwY * rs, __float2int_rn(wx[o] * wy_wz));
+    if (lx != 0xFF) atomicAdd(t.col + lx * kTwY * rs, tap_fixed(wx[o], wy_wz));
   }
 }
 
@@ -1792,7 +1803,7 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
         sl.cw = min(kTwX, a.ext[0] - x0);
         sl.ch = min(kTwY, a.ext[1] - y0);
         sl.mean = mean;
-        sl.scale = tw_scale(nall, most, mean);
+        sl.scale = tw_scale(nall, most, mean, a.ntaps);
         sl.mean_fx = mean * sl.scale;
       }
       __syncwarp();
@@ -1848,7 +1859,7 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
         home_ranges_load_w(a, home_x, home_y, it.f, it.t, it.tx, it.ty, s0, cnt, valid);
         const int most = __reduce_max_sync(0xffffffffu, static_cast<unsigned>(valid ? cnt : 0));
         const int nall = __reduce_add_sync(0xffffffffu, static_cast<unsigned>(valid ? cnt : 0));
-        unscale = 131072.0f / tw_scale(nall, most, tw_item_mean(a, it.f, it.t));
+        unscale = 131072.0f / tw_scale(nall, most, tw_item_mean(a, it.f, it.t), a.ntaps);
       }
       wait(&acc_full[d], j >> 1);
       if (__any_sync(0xffffffffu, abort_flag != 0)) break;

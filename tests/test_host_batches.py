@@ -4,7 +4,7 @@ The schedule must cover every frame exactly once, in order, with no sub-batch
 above the plan's max_frames; by default its sizes double from 4 so that the
 first (unoverlapped) copy is small.  On the GPU, frames fed from host memory in
 that schedule, in single frames, and from device memory in one batch (more than
-the 96 frames the sort kernel takes per launch in its parameters) must give the
+the 128 frames the sort kernel takes per launch in its parameters) must give the
 same histogram: exact bin counts and intensities within 1e-6 relative (the
 batches only change the order of the FP64 accumulation).
 """
