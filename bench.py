@@ -197,13 +197,15 @@ def max_over_ranks(v: float, dist) -> float:
 
 
 # DRAM bytes (read + write) per frame from one ncu capture of each kernel on the
-# 20-frame case of the same workload (profiles/k_spread_zdft_tcw_100k_atoms_20frames.md,
-# profiles/k_dft_tc_x_100k_atoms_20frames.md); a launch's traffic grows with its
-# frames, so a full launch is scaled by frames per launch.
+# 20-frame case of the same workload (`bench.py --batch 20`; profiles/
+# k_spread_zdft_tcw_100k_atoms_20frames.md and the y, x and sort summaries beside
+# it); a launch's traffic grows with its frames, so a full launch is scaled by
+# frames per launch.
 NCU_DRAM_BYTES_PER_FRAME = {
-    "k_spread_zdft_tcw": (32.685056e6 + 270.626816e6) / 20,
-    "k_dft_tc<y>": (330.524416e6 + 84.954112e6) / 20,
-    "k_dft_tc<x>": (106.050560e6 + 3.631104e6) / 20,
+    "k_spread_zdft_tcw": (32.726272e6 + 271.028736e6) / 20,
+    "k_dft_tc<y>": (330.531840e6 + 83.763456e6) / 20,
+    "k_dft_tc<x>": (106.054400e6 + 3.732224e6) / 20,
+    "k_sort_atoms": (24.467968e6 + 2.618624e6) / 20,
 }
 
 
