@@ -1292,8 +1292,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_spread_zdft_tc(DevArgs a, int
 // operands; the epilogue adds the two halves of D:
 // D[:, n] + D[:, twN + n] = (Ah + Al)(Bh + Bl), all four products.
 // Tensor memory (512 columns):
-//   [0, 256)    A ring: kTwRing slots of kTwChunk z, head in the first 32
-//               columns of a slot, remainder in the next 32
+//   [0, 256)    A ring: kTwRing = 8 slots of kTwChunk z (f16 pairs), head in
+//               the first 16 columns of a slot, remainder in the next 16
 //   [256, 512)  two accumulator stages of 2*twN <= 128 columns
 constexpr int kTwX = 8, kTwY = 16;  // wide tile: x-columns, y-rows (M = 128)
 constexpr int kTwProducerWarps = 24;
@@ -1303,7 +1303,8 @@ constexpr int kTwReleaseWarp = kTwProducerWarps + 6;
 constexpr int kTwThreads = 32 * (kTwProducerWarps + 7);  // producers, MMA, loader, 4 epilogue, release
 constexpr int kTwChunk = 32; // z per A ring slot
 constexpr int kTwSlotCols = 32;  // tensor-memory columns of an A ring slot: 16 head + 16 remainder (f16 pairs)
-constexpr int kTwRing = 4;   // A ring slots
+constexpr int kTwRing = 8;   // A ring slots (two items of 128 z in flight)
+static_assert(kTwRing * kTwSlotCols <= 256, "A ring and accumulator stages share 512 TMEM columns");
 
 // Record ranges of an item's home bins (up to 4 along x times 8 along y).
 struct TileAtomsW {
@@ -1617,21 +1618,25 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
       atomicExch(a.status, 1);
     }
   };
-  // bounded wait until the MMAs of the first `n` chunks are complete
+  // bounded wait until the MMAs of the first `n` chunks are complete: an acquire
+  // load of the counter the release lane publishes with a release store (a
+  // fence here would also wait for this warp's outstanding tap reductions)
+  const uint32_t released_addr = smem_addr(const_cast<const int *>(&released));
+  auto released_acquire = [&]() {
+    int v;
+    asm volatile("ld.acquire.cta.shared::cta.b32 %0, [%1];" : "=r"(v) : "r"(released_addr) : "memory");
+    return v;
+  };
   auto wait_released = [&](int n) {
-    if (released >= n || abort_flag) {
-      __threadfence_block();
-      return;
-    }
+    if (released_acquire() >= n || abort_flag) return;
     const uint64_t t0 = global_ns();
-    while (released < n && !abort_flag) {
+    while (released_acquire() < n && !abort_flag) {
       if (global_ns() - t0 > 2000000000ull) {
         abort_flag = 1;
         atomicExch(a.status, 1);
       }
       __nanosleep(64);
     }
-    __threadfence_block();
   };
 
   if (warp < kTwProducerWarps) {
@@ -1838,8 +1843,7 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
       for (int q = 0; q < mine * CH && !abort_flag; ++q) {
         wait(&a_empty[q % kTwRing], q / kTwRing);
         if (abort_flag) break;
-        __threadfence_block();
-        released = q + 1;
+        asm volatile("st.release.cta.shared::cta.b32 [%0], %1;" ::"r"(released_addr), "r"(q + 1) : "memory");
       }
     }
   } else {
