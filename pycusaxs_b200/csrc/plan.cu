@@ -890,6 +890,17 @@ struct AtomTab {
   int *lx, *ly;          // tile column of each x / y tap, one byte each, 0xFF outside
 };
 
+// Atom table of the wide kernel: x weights pre-multiplied by the item's
+// fixed-point scale, and the four x taps' tile offsets (lx * 16 * row stride,
+// -1 outside) precomputed, so that a tap costs no byte extraction or multiply.
+struct AtomTabW {
+  float4 *wxs, *wy, *wz;  // scale * x weights, y and z weights
+  int4 *zo;               // z row of each z tap
+  int4 *xo;               // tile offset of each x tap's column, -1 outside
+  int *ly;                // tile row (16 * lx + ly) y part of each y tap, one byte each, 0xFF outside
+};
+constexpr int kTwAtomBytes = 5 * 16 + 4;
+
 // Spreading pre-pass: atom v0 + i (i < nv) -> weights, z offsets and in-tile tap
 // columns.  Records [0, nrec_smem) come from the staged copy, the rest from
 // global memory.
@@ -1404,9 +1415,9 @@ __device__ __forceinline__ void home_ranges_publish_w(TileAtomsW &ta, int s0, in
 // kept: each warp appends its reaching atoms to the table at *count (a
 // shared-memory counter that starts at 0).
 __device__ __forceinline__ void spread_prepass_w(const DevArgs &a, const TileAtomsW &ta, const float4 *srec,
-                                                 int nrec_smem, int f, int v0, int nv, const AtomTab &tab,
-                                                 int x0, int y0, int cw, int ch, int tid, int nthreads,
-                                                 int *count) {
+                                                 int nrec_smem, int f, int v0, int nv, const AtomTabW &tab,
+                                                 int x0, int y0, int cw, int ch, int rs, float scale, int tid,
+                                                 int nthreads, int *count) {
   const int P = a.order, nt = a.ntaps, nz = a.n[2];
   const int lane = tid & 31;
   for (int i0 = tid - lane; i0 < nv; i0 += nthreads) {
@@ -1425,14 +1436,19 @@ __device__ __forceinline__ void spread_prepass_w(const DevArgs &a, const TileAto
     cubic_weights(q.x - static_cast<float>(m0), wx);
     cubic_weights(q.y - static_cast<float>(m1), wy);
     cubic_weights(q.z - static_cast<float>(m2), wz);
-    int lxp = 0, lyp = 0, zo[4];
+    int xo[4], lyp = 0, zo[4];
+    bool anyx = false;
 #pragma unroll
     for (int o = 0; o < 4; ++o) {
-      int bx = 0xFF, by = 0xFF, zz = 0;
+      int by = 0xFF, zz = 0;
+      xo[o] = -1;
       if (o < nt) {
         int x = m0 - P + o;
         if (x < 0) x += a.n[0];
-        if (static_cast<unsigned>(x - x0) < static_cast<unsigned>(cw)) bx = x - x0;
+        if (static_cast<unsigned>(x - x0) < static_cast<unsigned>(cw)) {
+          xo[o] = (x - x0) * kTwY * rs;
+          anyx = true;
+        }
         int y = m1 - P + o;
         if (y < 0) y += a.n[1];
         if (static_cast<unsigned>(y - y0) < static_cast<unsigned>(ch)) by = y - y0;
@@ -1440,22 +1456,21 @@ __device__ __forceinline__ void spread_prepass_w(const DevArgs &a, const TileAto
         if (z < 0) z += nz;
         zz = z;
       }
-      lxp |= bx << (8 * o);
       lyp |= by << (8 * o);
       zo[o] = zz;
     }
-    const bool reach = i < nv && lxp != -1 && lyp != -1;
+    const bool reach = i < nv && anyx && lyp != -1;
     const unsigned m = __ballot_sync(0xffffffffu, reach);
     int base = 0;
     if (lane == 0 && m) base = atomicAdd(count, __popc(m));
     base = __shfl_sync(0xffffffffu, base, 0);
     if (reach) {
       const int e = base + __popc(m & ((1u << lane) - 1u));
-      tab.wx[e] = make_float4(wx[0], wx[1], wx[2], wx[3]);
+      tab.wxs[e] = make_float4(wx[0] * scale, wx[1] * scale, wx[2] * scale, wx[3] * scale);
       tab.wy[e] = make_float4(wy[0], wy[1], wy[2], wy[3]);
       tab.wz[e] = make_float4(wz[0], wz[1], wz[2], wz[3]);
       tab.zo[e] = make_int4(zo[0], zo[1], zo[2], zo[3]);
-      tab.lx[e] = lxp;
+      tab.xo[e] = make_int4(xo[0], xo[1], xo[2], xo[3]);
       tab.ly[e] = lyp;
     }
   }
@@ -1467,50 +1482,47 @@ __device__ __forceinline__ void spread_prepass_w(const DevArgs &a, const TileAto
 // takes two units per round and reads both units' table entries before either
 // unit's atomics, so the shared-memory loads of one overlap the other.
 struct TapUnit {
-  int *col;       // tile row start of the unit's (y tap, z tap), or null when outside
-  int lxp;        // the atom's four x-tap columns, one byte each (0xFF outside)
-  float w;        // wy * wz * scale
-  float4 wx;
+  int *col;  // tile row start of the unit's (y tap, z tap), or null when outside
+  int i;     // the atom's table entry
+  float w;   // wy * wz
 };
 
-__device__ __forceinline__ TapUnit tap_unit(const AtomTab &tab, int u, int nu, int nt, int *A, int rs,
-                                            float scale) {
+__device__ __forceinline__ TapUnit tap_unit(const AtomTabW &tab, int u, int nu, int nt, int *A, int rs) {
   TapUnit t;
   t.col = nullptr;
   if (u >= nu) return t;
   const int i = u >> 4, p = (u >> 2) & 3, r = u & 3;
   if (p >= nt || r >= nt) return t;
   const int ly = (tab.ly[i] >> (8 * p)) & 0xFF;
-  t.lxp = tab.lx[i];
-  if (ly == 0xFF || t.lxp == -1) return t;
+  if (ly == 0xFF) return t;
   const float wy = reinterpret_cast<const float *>(&tab.wy[i])[p];
   const float wz = reinterpret_cast<const float *>(&tab.wz[i])[r];
   const int zo = reinterpret_cast<const int *>(&tab.zo[i])[r];
-  t.wx = tab.wx[i];
-  t.w = wy * wz * scale;
+  t.i = i;
+  t.w = wy * wz;
   t.col = A + zo + ly * rs;
   return t;
 }
 
-__device__ __forceinline__ void tap_apply(const TapUnit &t, int rs) {
+__device__ __forceinline__ void tap_apply(const AtomTabW &tab, const TapUnit &t) {
   if (!t.col) return;
-  const float wx[4] = {t.wx.x, t.wx.y, t.wx.z, t.wx.w};
-  const float wy_wz = t.w;
+  const float4 w4 = tab.wxs[t.i];
+  const int4 x4 = tab.xo[t.i];
+  const float wx[4] = {w4.x, w4.y, w4.z, w4.w};
+  const int xo[4] = {x4.x, x4.y, x4.z, x4.w};
 #pragma unroll
-  for (int o = 0; o < 4; ++o) {
-    const int lx = (t.lxp >> (8 * o)) & 0xFF;
-    if (lx != 0xFF) atomicAdd(t.col + lx * kTwY * rs, tap_fixed(wx[o], wy_wz));
-  }
+  for (int o = 0; o < 4; ++o)
+    if (xo[o] >= 0) atomicAdd(t.col + xo[o], tap_fixed(wx[o], t.w));
 }
 
-__device__ __forceinline__ void spread_taps_w(const AtomTab &tab, int nv, int nt, int *A, int rs, float scale,
-                                              int tid, int nthreads) {
+__device__ __forceinline__ void spread_taps_w(const AtomTabW &tab, int nv, int nt, int *A, int rs, int tid,
+                                              int nthreads) {
   const int nu = nv * 16;
   for (int u = tid; u < nu; u += 2 * nthreads) {
-    const TapUnit t0 = tap_unit(tab, u, nu, nt, A, rs, scale);
-    const TapUnit t1 = tap_unit(tab, u + nthreads, nu, nt, A, rs, scale);
-    tap_apply(t0, rs);
-    tap_apply(t1, rs);
+    const TapUnit t0 = tap_unit(tab, u, nu, nt, A, rs);
+    const TapUnit t1 = tap_unit(tab, u + nthreads, nu, nt, A, rs);
+    tap_apply(tab, t0);
+    tap_apply(tab, t1);
   }
 }
 
@@ -1567,14 +1579,14 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
   const int group = warp < kTwProducerWarps ? warp / gwarps : 0;
   const int gthreads = 32 * gwarps, gtid = tid - group * gthreads;
   const int cap = a.twCap;
-  AtomTab tab;
-  tab.wx = reinterpret_cast<float4 *>(reinterpret_cast<unsigned char *>(home_y + 2 * a.stw) +
-                                      static_cast<size_t>(group) * cap * kTcAtomBytes);
-  tab.wy = tab.wx + cap;
+  AtomTabW tab;
+  tab.wxs = reinterpret_cast<float4 *>(reinterpret_cast<unsigned char *>(home_y + 2 * a.stw) +
+                                       static_cast<size_t>(group) * cap * kTwAtomBytes);
+  tab.wy = tab.wxs + cap;
   tab.wz = tab.wy + cap;
   tab.zo = reinterpret_cast<int4 *>(tab.wz + cap);
-  tab.lx = reinterpret_cast<int *>(tab.zo + cap);
-  tab.ly = tab.lx + cap;
+  tab.xo = tab.zo + cap;
+  tab.ly = reinterpret_cast<int *>(tab.xo + cap);
   uint64_t *rec_full = bars, *rec_empty = bars + 2, *a_full = bars + 4, *a_empty = bars + 4 + kTwRing,
            *acc_full = bars + 4 + 2 * kTwRing, *acc_empty = acc_full + 2;
   {
@@ -1660,7 +1672,7 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
       if (!splitter && !__any_sync(0xffffffffu, abort_flag != 0)) {
         const int nvis = sl.ta.cum[sl.ta.nb];
         spread_prepass_w(a, sl.ta, recs + static_cast<size_t>(b) * RB, min(nvis, RB), sl.f, 0, min(cap, nvis),
-                         tab, sl.x0, sl.y0, sl.cw, sl.ch, ns_tid, ns_threads, &tab_count[group][ip][0]);
+                         tab, sl.x0, sl.y0, sl.cw, sl.ch, RS, sl.scale, ns_tid, ns_threads, &tab_count[group][ip][0]);
       }
       // the first chunk's table is complete and the previous item's split done
       const bool skip = producers_sync_or(abort_flag != 0, bar_id, gthreads);
@@ -1676,11 +1688,12 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
             producers_sync(bar_id, gthreads);
             if (gtid == 0) tab_count[group][ip][(k + 1) & 1] = 0;
             spread_prepass_w(a, sl.ta, recs + static_cast<size_t>(b) * RB, nrec, sl.f, v0, min(cap, nvis - v0),
-                             tab, sl.x0, sl.y0, sl.cw, sl.ch, gtid, gthreads, &tab_count[group][ip][k & 1]);
+                             tab, sl.x0, sl.y0, sl.cw, sl.ch, RS, sl.scale, gtid, gthreads,
+                             &tab_count[group][ip][k & 1]);
             producers_sync(bar_id, gthreads);
           }
-          spread_taps_w(tab, tab_count[group][ip][k & 1], a.ntaps, reinterpret_cast<int *>(A), RS, sl.scale,
-                        gtid, gthreads);
+          spread_taps_w(tab, tab_count[group][ip][k & 1], a.ntaps, reinterpret_cast<int *>(A), RS, gtid,
+                        gthreads);
         }
       }
       producers_sync(bar_id, gthreads);
@@ -3599,7 +3612,7 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
     const size_t bw_bytes = 2 * static_cast<size_t>(KT) * NW * sizeof(uint16_t);  // f16 B''
     auto wide_bytes = [&](int g, int rb, int cap) {
       return bw_bytes + static_cast<size_t>(g) * 128 * RSW * sizeof(float) + 2 * static_cast<size_t>(rb) * 16 +
-             home_w + static_cast<size_t>(g) * cap * kTcAtomBytes;
+             home_w + static_cast<size_t>(g) * cap * kTwAtomBytes;
     };
     int GW = 0;
     if (a.stw > 0 && NW <= 64) {  // two accumulator stages of 2*NW columns
