@@ -1455,6 +1455,8 @@ __device__ __forceinline__ void spread_prepass_w(const DevArgs &a, const TileAto
         int z = m2 - P + o;
         if (z < 0) z += nz;
         zz = z;
+      } else {
+        wz[o] = 0.0f;  // a missing z tap adds 0 at row 0; a missing y tap is outside
       }
       lyp |= by << (8 * o);
       zo[o] = zz;
@@ -1487,12 +1489,11 @@ struct TapUnit {
   float w;   // wy * wz
 };
 
-__device__ __forceinline__ TapUnit tap_unit(const AtomTabW &tab, int u, int nu, int nt, int *A, int rs) {
+__device__ __forceinline__ TapUnit tap_unit(const AtomTabW &tab, int u, int nu, int *A, int rs) {
   TapUnit t;
   t.col = nullptr;
   if (u >= nu) return t;
   const int i = u >> 4, p = (u >> 2) & 3, r = u & 3;
-  if (p >= nt || r >= nt) return t;
   const int ly = (tab.ly[i] >> (8 * p)) & 0xFF;
   if (ly == 0xFF) return t;
   const float wy = reinterpret_cast<const float *>(&tab.wy[i])[p];
@@ -1515,12 +1516,12 @@ __device__ __forceinline__ void tap_apply(const AtomTabW &tab, const TapUnit &t)
     if (xo[o] >= 0) atomicAdd(t.col + xo[o], tap_fixed(wx[o], t.w));
 }
 
-__device__ __forceinline__ void spread_taps_w(const AtomTabW &tab, int nv, int nt, int *A, int rs, int tid,
+__device__ __forceinline__ void spread_taps_w(const AtomTabW &tab, int nv, int *A, int rs, int tid,
                                               int nthreads) {
   const int nu = nv * 16;
   for (int u = tid; u < nu; u += 2 * nthreads) {
-    const TapUnit t0 = tap_unit(tab, u, nu, nt, A, rs);
-    const TapUnit t1 = tap_unit(tab, u + nthreads, nu, nt, A, rs);
+    const TapUnit t0 = tap_unit(tab, u, nu, A, rs);
+    const TapUnit t1 = tap_unit(tab, u + nthreads, nu, A, rs);
     tap_apply(tab, t0);
     tap_apply(tab, t1);
   }
@@ -1692,8 +1693,7 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
                              &tab_count[group][ip][k & 1]);
             producers_sync(bar_id, gthreads);
           }
-          spread_taps_w(tab, tab_count[group][ip][k & 1], a.ntaps, reinterpret_cast<int *>(A), RS, gtid,
-                        gthreads);
+          spread_taps_w(tab, tab_count[group][ip][k & 1], reinterpret_cast<int *>(A), RS, gtid, gthreads);
         }
       }
       producers_sync(bar_id, gthreads);
