@@ -1494,7 +1494,7 @@ __device__ __forceinline__ TapUnit tap_unit(const AtomTabW &tab, int u, int nu, 
   t.col = nullptr;
   if (u >= nu) return t;
   const int i = u >> 4, p = (u >> 2) & 3, r = u & 3;
-  const int ly = reinterpret_cast<const unsigned char *>(&tab.ly[i])[p]  // byte p;
+  const int ly = reinterpret_cast<const unsigned char *>(&tab.ly[i])[p];  // byte p
   if (ly == 0xFF) return t;
   const float wy = reinterpret_cast<const float *>(&tab.wy[i])[p];
   const float wz = reinterpret_cast<const float *>(&tab.wz[i])[r];
