@@ -202,10 +202,10 @@ def max_over_ranks(v: float, dist) -> float:
 # it); a launch's traffic grows with its frames, so a full launch is scaled by
 # frames per launch.
 NCU_DRAM_BYTES_PER_FRAME = {
-    "k_spread_zdft_tcw": (32.726272e6 + 271.028736e6) / 20,
-    "k_dft_tc<y>": (330.531840e6 + 83.763456e6) / 20,
-    "k_dft_tc<x>": (106.054400e6 + 3.732224e6) / 20,
-    "k_sort_atoms": (24.467968e6 + 2.618624e6) / 20,
+    "k_spread_zdft_tcw": (32.623360e6 + 270.978304e6) / 20,
+    "k_dft_tc<y>": (330.528256e6 + 83.254272e6) / 20,
+    "k_dft_tc<x>": (106.054656e6 + 4.113408e6) / 20,
+    "k_sort_atoms": (24.513536e6 + 3.240704e6) / 20,
 }
 
 
