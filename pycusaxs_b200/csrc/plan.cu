@@ -1291,17 +1291,19 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_spread_zdft_tc(DevArgs a, int
 // The same GEMM as k_spread_zdft_tc with M = 128 columns per work item (a tile
 // of 8 x-columns by 16 y-rows, column m = 16*lx + ly in TMEM lane m): twice the
 // columns per item halve the per-item fixed work and the halo share of the
-// atoms, and M = 128 runs the tensor core at its full rate.  The FP32 tile is
-// accumulated in shared memory as [m][z] rows of twRS floats (twRS = tcR + 4, so
-// that 8 consecutive rows of 16-byte loads and the 16 taps of one atom fall in
-// distinct banks), then split into the TF32 head and remainder straight into
-// tensor memory, where the MMAs read A.
-// A tf32 MMA costs about the same up to N = 192 (it is bound by its issue and
+// atoms, and M = 128 runs the tensor core at its full rate.  The tile is
+// accumulated in shared memory in 32-bit fixed point (integer atomics; see
+// tw_scale) as [m][z] rows of twRS words (twRS = tcR + 4, so that 8 consecutive
+// rows of 16-byte loads and the 16 taps of one atom fall in distinct banks),
+// then split into an f16 head and remainder straight into tensor memory, where
+// the kind::f16 MMAs (K = 16) read A.
+// An MMA costs about the same up to N = 192 (it is bound by its issue and
 // accumulator latency, not by its N), so B holds the twiddle head and
 // remainder side by side, B' = [Bh | Bl] (N' = 2*twN), and one k step is two
 // MMAs, D += Ah * B' and D += Al * B', where three were needed with separate
 // operands; the epilogue adds the two halves of D:
-// D[:, n] + D[:, twN + n] = (Ah + Al)(Bh + Bl), all four products.
+// D[:, n] + D[:, twN + n] = (Ah + Al)(Bh + Bl), all four products, and scales
+// the sum back by 2^17 / scale.
 // Tensor memory (512 columns):
 //   [0, 256)    A ring: kTwRing = 8 slots of kTwChunk z (f16 pairs), head in
 //               the first 16 columns of a slot, remainder in the next 16
@@ -1529,17 +1531,17 @@ __device__ __forceinline__ void spread_taps_w(const AtomTabW &tab, int nv, int *
 
 // Persistent, warp-specialized like k_spread_zdft_tc; grid = min(work items,
 // SMs), block kTwThreads.  Work items w = ((f*T + t)*stw + ty)*stiles[0] + tx.
-//   producer warps: twG groups on alternate items, each with its own FP32 tile
-//               and atom table: pre-pass and shared-memory taps into the
+//   producer warps: twG groups on alternate items, each with its own fixed-point
+//               tile and atom table: pre-pass and shared-memory taps into the
 //               tile, then the split, chunk by chunk of kTwChunk z: chunk q
 //               (q = j*CH + c over the CTA's items j) goes to ring slot
 //               q % kTwRing once the MMAs of chunk q - kTwRing are complete;
 //               warp q (mod 4) with rank h < 2 among the group's warps of that
 //               lane quarter converts rows 32q..32q+31, z in [32c + 16h, +16)
-//               (tile - mean -> TF32 head and remainder) with tcgen05.st and
-//               zeroes what it read
-//   MMA warp    one lane issues per chunk 2 x (kTwChunk/8) MMAs with A from
-//               tensor memory (M = 128, N = 2*twN, K = 8) into the item's
+//               ((tile - mean) * 2^-17 -> f16 head and remainder) with
+//               tcgen05.st and zeroes what it read
+//   MMA warp    one lane issues per chunk 2 x (kTwChunk/16) kind::f16 MMAs with A
+//               from tensor memory (M = 128, N = 2*twN, K = 16) into the item's
 //               accumulator stage, chunk by chunk as the split delivers them
 //   loader warp home-bin record ranges (up to 32 bins), item data, bulk copies
 //   4 epilogue  accumulator halves summed -> Z (lane m = column 16*lx + ly)
@@ -1555,9 +1557,9 @@ __device__ __forceinline__ void spread_taps_w(const AtomTabW &tab, int nv, int *
 // can neither fall two phases behind nor run two ahead (parity waits cannot
 // tell those apart); the ring slots, filled by both groups, are handed back
 // through the monotonic counter instead.
-// Dynamic shared memory: B' (tcK x 2*twN floats), twG tiles of 128 x twRS
-// floats, two record buffers of twRB float4, the home-bin tables (stiles[0] +
-// 2*stw int4) and twG atom tables of twCap entries.
+// Dynamic shared memory: B' (tcK x 2*twN halves), twG tiles of 128 x twRS
+// words, two record buffers of twRB float4, the home-bin tables (stiles[0] +
+// 2*stw int4) and twG atom tables of twCap entries (kTwAtomBytes each).
 __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, int items) {
   pdl_release();
   extern __shared__ __align__(16) unsigned char smem[];
@@ -3602,11 +3604,10 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
             RB = rb;
             CAP = cap;
           }
-    // wide tiles: twG FP32 tiles of 128 x (R + 4) floats; two producer groups
-    // before larger record buffers and atom tables
-    // wide tiles, for one and for two producer groups: the largest atom table
-    // (each table chunk costs a latency-bound pre-pass and two barriers), then
-    // the largest record buffer that fit beside the groups' FP32 tiles
+    // wide tiles, for one and for two producer groups: twG fixed-point tiles of
+    // 128 x (R + 4) words, then the largest atom table (each table chunk costs a
+    // latency-bound pre-pass and two barriers), then the largest record buffer
+    // that fit beside them
     const int RSW = R + 4;
     const size_t home_w = static_cast<size_t>(a.stiles[0] + 2 * a.stw) * sizeof(int4);
     const size_t bw_bytes = 2 * static_cast<size_t>(KT) * NW * sizeof(uint16_t);  // f16 B''
