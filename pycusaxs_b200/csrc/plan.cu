@@ -2532,31 +2532,57 @@ __global__ void __launch_bounds__(kThreads)
   const int kx_hi = a.kx_lo + a.nkx - 1, ky_hi = a.ky_lo + a.nky - 1;
   double *dh = in_smem ? sh : hist;
   double *dn = in_smem ? sn : nhist;
-  for (int p = tid; p < npts; p += blockDim.x) {
-    const int ky = p / a.nkx, kx = p % a.nkx;
-    const int ia = a.kx_lo + kx, ja = a.ky_lo + ky;
-    const float mw = kpoint_q(ocs, ia, ja, ka);
-    if (mw > a.qcut) continue;
-    if (a.dq <= 0.0f) continue;
-    const int h0 = static_cast<int>(mw / a.dq);
-    if (h0 < 0 || h0 >= a.num_bins) continue;
-    double v, c;
-    if (ia == 0 && ja == 0 && ka == 0) {
-      v = static_cast<double>(pl[p]) * fact;
-      c = 1.0;
-    } else {
-      int ib = -ia, jb = -ja;
-      if (ib > kx_hi) ib = ia;
-      if (jb > ky_hi) jb = ja;
-      const int pm = (jb - a.ky_lo) * a.nkx + (ib - a.kx_lo);
-      if (sizeof(V) == 4)
-        v = static_cast<double>(static_cast<float>(pl[p]) + static_cast<float>(pl[pm])) * fact;
-      else
-        v = (static_cast<double>(pl[p]) + static_cast<double>(pl[pm])) * fact;
-      c = 2.0;
+  // Neighbouring k-points (consecutive lanes) mostly fall in the same bin: each
+  // warp sums runs of equal bins in lane order (a segmented shuffle scan) and
+  // the last lane of a run adds the run's sums, so the FP64 atomics contend
+  // far less.
+  const int lane = tid & 31;
+  for (int p0 = tid - lane; p0 < npts; p0 += blockDim.x) {
+    const int p = p0 + lane;
+    int h0 = -1;
+    double v = 0.0, c = 0.0;
+    if (p < npts && a.dq > 0.0f) {
+      const int ky = p / a.nkx, kx = p % a.nkx;
+      const int ia = a.kx_lo + kx, ja = a.ky_lo + ky;
+      const float mw = kpoint_q(ocs, ia, ja, ka);
+      const int hb = static_cast<int>(mw / a.dq);
+      if (!(mw > a.qcut) && hb >= 0 && hb < a.num_bins) {
+        h0 = hb;
+        if (ia == 0 && ja == 0 && ka == 0) {
+          v = static_cast<double>(pl[p]) * fact;
+          c = 1.0;
+        } else {
+          int ib = -ia, jb = -ja;
+          if (ib > kx_hi) ib = ia;
+          if (jb > ky_hi) jb = ja;
+          const int pm = (jb - a.ky_lo) * a.nkx + (ib - a.kx_lo);
+          if (sizeof(V) == 4)
+            v = static_cast<double>(static_cast<float>(pl[p]) + static_cast<float>(pl[pm])) * fact;
+          else
+            v = (static_cast<double>(pl[p]) + static_cast<double>(pl[pm])) * fact;
+          c = 2.0;
+        }
+      }
     }
-    atomicAdd(dh + h0, v);
-    atomicAdd(dn + h0, c);
+    // first lane of this lane's run of equal bins
+    const int hprev = __shfl_up_sync(0xffffffffu, h0, 1);
+    int start = (lane == 0 || hprev != h0) ? lane : 0;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) start = max(start, __shfl_up_sync(0xffffffffu, start, d));
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const double vo = __shfl_up_sync(0xffffffffu, v, d);
+      const double co = __shfl_up_sync(0xffffffffu, c, d);
+      if (lane - d >= start) {
+        v += vo;
+        c += co;
+      }
+    }
+    const int hnext = __shfl_down_sync(0xffffffffu, h0, 1);
+    if (h0 >= 0 && (lane == 31 || hnext != h0)) {
+      atomicAdd(dh + h0, v);
+      atomicAdd(dn + h0, c);
+    }
   }
   if (in_smem) {
     __syncthreads();
