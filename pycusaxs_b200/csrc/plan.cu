@@ -1570,7 +1570,7 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
   __shared__ volatile int released;
   __shared__ int tab_count[2][2][2];  // reaching atoms in the table: [group][item parity][chunk parity]
   const int NB = a.twN, N = 2 * a.twN, KT = a.tcK, R = a.tcR, RB = a.twRB, RS = a.twRS, G = a.twG;
-  const int SR = 2;  // split warps per lane quarter (16 z of a chunk each); 4 measured slower
+  const int SR = 2;  // split warps per lane quarter (16 z of a chunk each); 4 measured no faster
   const int CH = (KT + kTwChunk - 1) / kTwChunk;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   float *bh = reinterpret_cast<float *>(smem);  // B' = [Bh | Bl], f16, K-major, N columns
