@@ -106,6 +106,7 @@ struct SaxsPlan {
   size_t smem_yadj = 0, smem_zadj = 0;
   int spread_ctas = 1;  // resident CTAs of the persistent spreading kernel
   int sort_slots = 1;    // resident k_sort_atoms CTAs on the device
+  int sort_cluster = 1;  // largest k_sort_atoms cluster size the device can schedule (<= kSortMaxCluster)
   int sort_max_type = 0; // entries of the largest type
   bool use_tc = false;   // z-axis DFT on the tensor cores
   bool use_tcw = false;  // ... with the wide-tile kernel (k_spread_zdft_tcw), else k_spread_zdft_tc
@@ -859,6 +860,27 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
       e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sort_per_sm, k_sort_atoms, kSortThreads,
                                                         2 * sizeof(int) * a.tiles[0] * a.tiles[1]);
     pl->sort_slots = std::max(1, sort_per_sm) * std::max(1, sms);
+    // the largest cluster size with at least one schedulable cluster at this
+    // plan's shared-memory size
+    for (int c = kSortMaxCluster; e == cudaSuccess && c >= 1; c /= 2) {
+      cudaLaunchConfig_t occ = {};
+      occ.gridDim = dim3(c);
+      occ.blockDim = dim3(kSortThreads);
+      occ.dynamicSmemBytes = 2 * sizeof(int) * a.tiles[0] * a.tiles[1];
+      cudaLaunchAttribute cat[1];
+      cat[0].id = cudaLaunchAttributeClusterDimension;
+      cat[0].val.clusterDim.x = c;
+      cat[0].val.clusterDim.y = 1;
+      cat[0].val.clusterDim.z = 1;
+      occ.attrs = cat;
+      occ.numAttrs = 1;
+      int nclusters = 0;
+      if (cudaOccupancyMaxActiveClusters(&nclusters, k_sort_atoms, &occ) == cudaSuccess && nclusters > 0) {
+        pl->sort_cluster = c;
+        break;
+      }
+      cudaGetLastError();  // a size the device cannot schedule is not an error of the plan
+    }
     if (e == cudaSuccess && pl->tcw_ok) pl->tcw_ctas = std::max(1, sms);  // 512 TMEM columns: one per SM
     if (e == cudaSuccess && pl->tcn_ok) {
       // resident CTAs whose tensor-memory allocations fit the SM's 512 columns together
@@ -961,9 +983,11 @@ int launch_sort(const SaxsPlan *pl, const DevArgs &a, int nframes, cudaStream_t 
   for (int f0 = 0; f0 < nframes; f0 += step) {
     const int n = std::min(step, nframes - f0);
     if (host_geom) std::memcpy(gp.g, host_geom + static_cast<size_t>(f0) * kGeom, sizeof(float) * n * kGeom);
-    int C = 4;  // at least 4: measured slightly faster than 2 at 100 frames of 100k atoms
+    // at least 4 (measured slightly faster than 2 at 100 frames of 100k atoms),
+    // at most what the device can schedule at this shared-memory size
+    int C = std::min(4, pl->sort_cluster);
     const long long total = static_cast<long long>(a.M) * n;
-    while (C < kSortMaxCluster &&
+    while (C < pl->sort_cluster &&
            static_cast<long long>(pl->sort_max_type) * pl->sort_slots > static_cast<long long>(C) * total)
       C *= 2;
     cudaLaunchConfig_t cfg = {};
