@@ -59,3 +59,31 @@ def test_host_schedules_and_device_batch_agree(cuda):
     for h, n in out[1:]:
         np.testing.assert_array_equal(n, n0)
         np.testing.assert_allclose(h[sel], h0[sel], rtol=1e-6)
+
+
+@pytest.mark.gpu
+def test_batch_above_the_sort_parameter_frames(cuda):
+    # 130 frames in one call: the sort kernel takes 128 frames' geometry per launch
+    # in its parameters, so this batch needs two sort launches (128 + 2 frames)
+    import torch
+
+    from pycusaxs_b200 import SaxsEngine
+    from pycusaxs_b200.synthetic import cubic_system
+
+    nf = 130
+    s = cubic_system(1500, 36.0, seed=92, jitter=0.4, nframes=nf)
+    frames = s.frames(0, nf)
+    boxes = np.stack([s.box] * nf)
+    out = []
+    for batch in (nf, 1):
+        e = SaxsEngine((32, 32, 32), s.atom_index(), s.natoms, s.box, scale_factor=2.0, qcut=0.6,
+                       max_frames=batch)
+        x = torch.from_numpy(frames).cuda()
+        for k in range(0, nf, batch):
+            e.forward(x[k:k + batch], boxes[k:k + batch])
+        out.append(e.histogram())
+        e.close()
+    (h0, n0), (h1, n1) = out
+    np.testing.assert_array_equal(n0, n1)
+    sel = n0 > 0
+    np.testing.assert_allclose(h0[sel], h1[sel], rtol=1e-6)
