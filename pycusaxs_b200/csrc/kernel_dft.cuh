@@ -93,7 +93,7 @@ __global__ void __launch_bounds__(kThreads) k_ydft(DevArgs a) {
 //   the B-spline moduli (the SIMT kernel's k_xdft_post), writing
 //   ibox[kz][ky][kx].
 // K is streamed in chunks of kDtcChunk values of u: per chunk the loader warp
-// issues one tensor copy (cp.async.bulk.tensor, no multicast, 128-byte swizzle)
+// issues one tensor copy (cp.async.bulk.tensor into this CTA only, 128-byte swizzle)
 // of the 128 rows x 32 floats into a raw staging tile (rows outside the data
 // zero-filled by the tensor map) and one bulk copy of the B' chunk.  The
 // producers split the raw rows into a TF32 head and remainder and store them to
