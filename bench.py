@@ -10,6 +10,9 @@ histogram in FP64 - all through the batched fused forward.
          L2 flushed between steps)
   e2e    frames/s through the public API from pinned host buffers: every step
          copies its frames host->device and reads the histogram back
+  dropin frames/s through the drop-in pycusaxs_cuda.run (the reference's own
+         entry point, here re-implemented), per-frame slope of two runs, the
+         same method as the reference arm
 
 usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 Under torchrun each rank processes its own 100 frames (weak scaling); the FP64
@@ -55,6 +58,7 @@ def parse():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-multi", action="store_true")
+    ap.add_argument("--no-dropin", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="keep the plan's default kernels")
     return ap.parse_args()
 
@@ -197,16 +201,18 @@ def max_over_ranks(v: float, dist) -> float:
 
 
 # DRAM bytes (read + write) per frame from one ncu capture of each kernel on the
-# 20-frame case of the same workload (`bench.py --batch 20`; profiles/
-# k_spread_zdft_tcw_100k_atoms_20frames.md and the y, x and sort summaries beside
-# it); a launch's traffic grows with its frames, so a full launch is scaled by
-# frames per launch.
+# 20-frame case of the same workload (`bench.py --batch 20`); a launch's traffic
+# grows with its frames, so a full launch is scaled by frames per launch.  These
+# are constants of the capture named in NCU_CAPTURE, not live measurements.
 NCU_DRAM_BYTES_PER_FRAME = {
     "k_spread_zdft_tcw": (32.623360e6 + 270.978304e6) / 20,
     "k_dft_tc<y>": (330.528256e6 + 83.254272e6) / 20,
     "k_dft_tc<x>": (106.054656e6 + 4.113408e6) / 20,
     "k_sort_atoms": (24.513536e6 + 3.240704e6) / 20,
 }
+
+
+NCU_CAPTURE = "ncu --section MemoryWorkloadAnalysis of bench.py --batch 20 (one kernel per capture)"
 
 
 def traffic_per_launch(kernel: str, frames_per_launch: float):
@@ -321,7 +327,8 @@ def bench_ours(args):
     roofline = {"bound": "hbm", "kernel": kernel_of.get(dom, dom), "achieved": round(achieved, 1),
                 "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
                 "traffic": traffic_per_launch(kernel_of.get(dom, dom), frames_per_launch),
-                "traffic_note": "DRAM bytes per launch: ncu capture of 20 frames, scaled by frames per launch",
+                "traffic_note": "DRAM bytes per launch, a constant from one capture (" + NCU_CAPTURE +
+                                "), scaled by frames per launch",
                 "algorithmic_bytes": round(algo_bytes.get(dom, 0) * frames_per_launch),
                 "peak_source": "measured" if peaks else "fallback"}
     if dom in algo_flops:
@@ -383,6 +390,9 @@ def bench_ours(args):
         plain = FRAMES / (a.elapsed_time(b) / 1e3)
         eng1.close()
 
+    dropin = None
+    if rank == 0 and world == 1 and not args.no_dropin:
+        dropin = dropin_rate(system, frames, args)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(system)
@@ -410,7 +420,7 @@ def bench_ours(args):
                    "kernel_config": eng.config(), "autotune": tuned,
                    "parallelism": f"frames sharded over {world} GPU(s)",
                    "adjoint": adj, "multi_system": multi},
-        "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": ck,
+        "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "dropin": dropin, "clocks": ck,
         "gpu_launches": int(launches),
     }
     eng.close()
@@ -546,10 +556,64 @@ def multi_system(launches: int = 3) -> dict:
             "speedup": round(batched / plain, 2)}
 
 
+def _silenced(fn, *args, **kw):
+    """fn(*args, **kw) with file descriptor 1 sent to /dev/null (both drop-ins
+    print per-frame banners, the reference's from C++)."""
+    sys.stdout.flush()
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    saved = os.dup(1)
+    os.dup2(devnull, 1)
+    try:
+        return fn(*args, **kw)
+    finally:
+        sys.stdout.flush()
+        os.dup2(saved, 1)
+        os.close(devnull)
+        os.close(saved)
+
+
+def slope_rate(run_module, topo, sample: int, steps: int, warmup: int, out: str) -> tuple:
+    """Frames/s of run_module.run on `topo` by the per-frame slope: (run of
+    2 + sample frames - run of 2 frames) / sample, wall clock, median of `steps`;
+    the run's set-up (plan creation, tables) cancels."""
+    def run(nframes):
+        t0 = time.perf_counter()
+        _silenced(run_module.run, topo, "synthetic.tpr", "synthetic.xtc", [GRID], begin=0,
+                  end=nframes - 1, stride=1, output=out, scale_factor=SCALE, bin_size=BIN,
+                  qcut=QCUT)
+        return time.perf_counter() - t0
+
+    for _ in range(max(1, warmup)):
+        run(2)
+    per_frame = []
+    for _ in range(max(1, steps)):
+        t_small = run(2)
+        t_big = run(2 + sample)
+        per_frame.append((t_big - t_small) / sample)
+    return 1.0 / statistics.median(per_frame), per_frame
+
+
+def dropin_rate(system, frames, args) -> dict:
+    """This repo's pycusaxs_cuda.run (the drop-in) on the same workload, timed
+    like the reference arm: the topology serves the 100 precomputed frames."""
+    from pycusaxs_b200 import pycusaxs_cuda
+    from pycusaxs_b200.synthetic import SyntheticTopology
+
+    topo = SyntheticTopology(system, frames=frames)
+    sample = FRAMES - 2
+    value, per = slope_rate(pycusaxs_cuda, topo, sample, min(args.steps, 5), 1, "/tmp/dropin_bench.dat")
+    return {"value": round(value, 1), "unit": "frames/s",
+            "method": f"per-frame slope: (run of {2 + sample} frames - run of 2 frames) / {sample}, "
+                      "wall clock, median of steps; frames served from host memory by the topology",
+            "h2d_bytes_per_frame": int(frames[0].nbytes)}
+
+
 def cpu_baseline(system) -> dict:
     """The FP64 oracle on one frame of the same workload, on this host's cores."""
     from oracle import saxs_oracle as O
 
+    cores = os.cpu_count() or 1
+    O.FFT_WORKERS = cores
     names = sorted({str(e) for e in system.elements})
     ff = O.load_form_factors()
     plan = O.OraclePlan(grid=(GRID,) * 3, types=names, coeffs=np.stack([ff[n] for n in names]),
@@ -558,8 +622,10 @@ def cpu_baseline(system) -> dict:
     t0 = time.perf_counter()
     O.run_frames(plan, [(system.frame(0), system.box)], toa)
     dt = time.perf_counter() - t0
-    return {"value": round(1.0 / dt, 4), "unit": "frames/s", "cores": 1, "kind": "port",
-            "sample": f"1 frame of the workload through the FP64 NumPy oracle ({dt:.1f} s)"}
+    return {"value": round(1.0 / dt, 4), "unit": "frames/s", "cores": cores, "kind": "port",
+            "sample": f"1 frame of the workload through the FP64 NumPy oracle ({dt:.2f} s): "
+                      f"R2C transforms on {cores} threads (scipy pocketfft), spreading and "
+                      "binning in single-threaded NumPy"}
 
 
 def bench_reference(args):
@@ -578,32 +644,10 @@ def bench_reference(args):
     from pycusaxs_b200.synthetic import SyntheticTopology, cubic_system
 
     system = cubic_system(NATOMS, BOX, seed=1000, jitter=JITTER, nframes=FRAMES)
-    topo = SyntheticTopology(system)
+    topo = SyntheticTopology(system, frames=system.frames(0, FRAMES))
     sample = 10
-
-    def run(nframes):
-        devnull = os.open(os.devnull, os.O_WRONLY)
-        saved = os.dup(1)
-        os.dup2(devnull, 1)
-        try:
-            t0 = time.perf_counter()
-            pycusaxs_cuda.run(topo, "synthetic.tpr", "synthetic.xtc", [GRID], begin=0,
-                              end=nframes - 1, stride=1, output="/tmp/ref_bench.dat",
-                              scale_factor=SCALE, bin_size=BIN, qcut=QCUT)
-            return time.perf_counter() - t0
-        finally:
-            os.dup2(saved, 1)
-            os.close(devnull)
-            os.close(saved)
-
-    for _ in range(max(1, args.warmup)):
-        run(2)
-    per_frame = []
-    for _ in range(args.steps):
-        t_small = run(2)
-        t_big = run(2 + sample)
-        per_frame.append((t_big - t_small) / sample)
-    value = 1.0 / statistics.median(per_frame)
+    value, per_frame = slope_rate(pycusaxs_cuda, topo, sample, args.steps, args.warmup,
+                                  "/tmp/ref_bench.dat")
     out = {"metric": METRIC, "value": round(value, 2), "unit": "frames/s", "n_gpus": 1,
            "steps": args.steps, "warmup": args.warmup,
            "ms_per_step": round(statistics.median(per_frame) * 1e3 * sample, 3),
@@ -611,12 +655,13 @@ def bench_reference(args):
            "data": "synthetic", "impl": "reference",
            "config": {"workload": "100k atoms, 12 nm cubic box, grid 128, order 4, scale 2 "
                                   "(256^3 supercell), qcut 0.5/A, npt",
-                      "method": "per-frame slope: (run of 12 frames - run of 2 frames) / 10"},
+                      "method": "per-frame slope: (run of 12 frames - run of 2 frames) / 10, "
+                                "frames served from host memory by the topology"},
            "cpu_baseline": {"value": round(value, 2), "unit": "frames/s", "cores": 1,
-                            "kind": "reference",
+                            "kind": "reference", "device": "the GPU (the reference has no CPU path)",
                             "sample": f"{sample} frames per step through the reference's own "
-                                      "pycusaxs_cuda.run (its CUDA build, oracle/_ref; the "
-                                      "reference has no CPU path)"},
+                                      "pycusaxs_cuda.run: its unmodified CUDA build (oracle/_ref) "
+                                      "on this box's GPU, one host thread"},
            "e2e": {"value": round(value, 2), "unit": "frames/s", "h2d_bytes_per_step": 0,
                    "d2h_bytes_per_step": 0}}
     print(json.dumps(out))

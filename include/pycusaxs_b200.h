@@ -29,10 +29,12 @@ extern "C" {
 /* status codes */
 #define SAXS_OK 0
 #define SAXS_E_INVALID (-1)   /* bad argument (the reference raises ValueError) */
-#define SAXS_E_CUDA (-2)      /* CUDA runtime or cuFFT failure */
+#define SAXS_E_CUDA (-2)      /* CUDA runtime or driver failure */
 #define SAXS_E_NOMEM (-3)     /* device allocation refused (saxsKernel.cu:301-314) */
 #define SAXS_E_RANGE (-4)     /* a frame left the planned k-box or capacity */
-#define SAXS_E_DEVICE (-5)    /* a kernel reported an error through its status word */
+#define SAXS_E_DEVICE (-5)    /* a kernel reported an error through the plan's status word:
+                                 a bounded wait gave up, or a position was NaN/infinite;
+                                 saxs_last_error() names the kernel, saxs_reset clears it */
 
 /* ensembles (cpp-src/Exec/Options.cpp:16, cudaSAXS.cu:84-87) */
 #define SAXS_NPT 0 /* one histogram per frame, summed over frames (saxsKernel.cu:190-196) */
@@ -58,7 +60,11 @@ typedef struct SaxsParams {
   const int32_t *entry_type; /* host: type index 0..ntypes-1 of each entry         */
   float box0[9];        /* first-frame box: fixes Delta-q, q-cut and the k-box     */
   int max_frames;       /* frames per saxs_forward call (batch capacity)           */
-  float box_margin;     /* relative box shrink the k-box tolerates (e.g. 0.05)     */
+  float box_margin;     /* relative box growth the k-box covers (e.g. 0.05); a frame */
+                        /* beyond it makes saxs_forward / saxs_backward widen the   */
+                        /* plan (new buffers, same accumulators; waits for the      */
+                        /* stream), saxs_graph_launch and saxs_forward_noalloc      */
+                        /* return SAXS_E_RANGE                                      */
   /* Opt-in physics extensions (no counterpart in the reference's output; 0 keeps
    * the reference's behaviour):                                                  */
   int box_mode;         /* SAXS_BOX_PARITY: oc from the box's upper triangle       */
@@ -137,10 +143,12 @@ int saxs_forward(SaxsPlan *plan, const float *xyz_dev, int64_t frame_stride, int
 /* Finish the run: for nvt bin the summed intensities with the first-frame box
  * (saxsKernel::getHistogram, saxsKernel.cu:17-39); then copy the FP64
  * histogram and counts (num_bins each) to host memory and wait for them
- * (saxsKernel::getSaxs, saxsKernel.cu:210-225).  The accumulators are kept. */
+ * (saxsKernel::getSaxs, saxsKernel.cu:210-225).  The accumulators are kept.
+ * Returns SAXS_E_DEVICE when a kernel of a processed frame reported an error
+ * (the histogram is then invalid; saxs_last_error() names the kernel). */
 int saxs_histogram(SaxsPlan *plan, double *hist_host, double *nhist_host, void *stream);
 
-/* Zero the accumulators so the plan can serve another run. */
+/* Zero the accumulators and the status word so the plan can serve another run. */
 int saxs_reset(SaxsPlan *plan, void *stream);
 
 /* Intensities |sum_t f_t F_t|^2 * M of the last frame processed by
@@ -150,6 +158,21 @@ int saxs_debug_kbox_intensity(SaxsPlan *plan, float *out_host, void *stream);
 
 /* Per-type FP64 z-border sums of the last frame (saxsDeviceKernels.cu:446-465). */
 int saxs_debug_border_sums(SaxsPlan *plan, double *out_host, void *stream);
+
+/* Kernel diagnostics since plan creation or the last saxs_reset (no reference
+ * counterpart; waits for `stream`): out_host[0] = the status word (0: no error;
+ * bit 1: spreading/z pass, 2: y pass, 4: x pass gave up on a bounded wait,
+ * 8: the wait probe below, 16: a NaN or infinite position), out_host[1] = the
+ * most atom-table chunks one item of the wide spreading kernel needed (0: every
+ * item's atoms fit its table at once), out_host[2..3] reserved (0). */
+int saxs_debug_counters(SaxsPlan *plan, int *out_host, void *stream);
+
+/* Run the bounded mbarrier wait that the pipelined kernels use, on a barrier
+ * nothing arrives at, for `limit_seconds` (0 < limit <= 2): it gives up and sets
+ * bit 8 of the plan's status word, so that the next saxs_histogram reports
+ * SAXS_E_DEVICE; saxs_reset clears it.  Tests the device-side failure path
+ * without faulting or hanging the GPU (no reference counterpart). */
+int saxs_debug_wait_probe(SaxsPlan *plan, double limit_seconds, void *stream);
 
 /* Reverse-mode derivative with respect to the positions of one frame.  Given
  * dL/dhist for each histogram bin of that frame (num_bins doubles, host memory;
@@ -194,10 +217,15 @@ void saxs_graph_destroy(SaxsGraph *graph);
  * accumulators are left alone.  Every temporary comes from one fixed device
  * array of SAXS_NOALLOC_SCRATCH_BYTES held by every GPU that loads the library
  * until exit; plans needing more per frame get SAXS_E_RANGE.  Calls share that
- * array, so calls that overlap on the GPU must be serialised by the caller.  The
- * first call on a device looks the array up (cudaGetSymbolAddress) and should
- * come before any stream capture.  Allocates nothing; the plan is created,
- * with allocation, beforehand by saxs_plan_create. */
+ * array, so calls that overlap on the GPU must be serialised by the caller.
+ * saxs_plan_create looks the array up (cudaGetSymbolAddress), which loads it
+ * onto the plan's device; only if that failed does the first call look it up
+ * (that call should then come before any stream capture).  cudaDeviceReset
+ * invalidates plans and the cached address; plans created afterwards refresh
+ * it.  The call is asynchronous: a kernel error of the frame (a bounded wait
+ * that gave up, or NaN/infinite positions) makes hist_dev and nhist_dev NaN.
+ * Allocates nothing; the plan is created, with allocation, beforehand by
+ * saxs_plan_create. */
 #define SAXS_NOALLOC_SCRATCH_BYTES ((size_t)32 << 20)
 int saxs_forward_noalloc(SaxsPlan *plan, const float *xyz_dev, const float *box_host,
                          double *hist_dev, double *nhist_dev, void *stream);

@@ -52,6 +52,10 @@ FORM_FACTOR_JSON = _REPO / "pycusaxs_b200" / "data" / "it1992.json"
 # Pinned against the reference's compiled kernel by tests/test_gpu_bins.py.
 DEFAULT_CONTRACTION = 1
 
+# Threads of the FP64 R2C transform (scipy's pocketfft; numpy's rfftn, the same
+# algorithm single-threaded, when scipy is absent).  None: every host core.
+FFT_WORKERS: int | None = None
+
 SHELL = np.float32(0.07)  # include/Parameters.h:8
 KCUT = 50                 # Utilities/BSpmod.h:22
 TINY = np.float32(1.0e-7)  # Utilities/BSpmod.cpp:21
@@ -321,6 +325,20 @@ def supercell(grid, mean, nn) -> np.ndarray:
     return sup
 
 
+def fft_workers() -> int:
+    return int(FFT_WORKERS) if FFT_WORKERS else (os.cpu_count() or 1)
+
+
+def rfftn(a) -> np.ndarray:
+    """Unnormalised FP64 R2C transform over all axes (the half spectrum along the
+    last axis), as cuFFT's R2C at saxsKernel.cu:171."""
+    try:
+        import scipy.fft as sf
+    except ImportError:
+        return np.fft.rfftn(a)
+    return sf.rfftn(a, workers=fft_workers())
+
+
 def form_factor(q, coeffs) -> np.ndarray:
     """f(q) = sum_i a_i exp(-b_i (q/4pi)^2) + c  (opsfact.cu:30-35), FP64."""
     c = np.asarray(coeffs, dtype=np.float64)
@@ -429,7 +447,8 @@ def frame_intensity(plan: OraclePlan, xyz, type_of_atom, box, *, return_parts=Fa
         mean = border_mean(g) if plan.padding is None else float(plan.padding[t])
         means.append(mean)
         sup = supercell(g, mean, nn)
-        ft = np.fft.rfftn(sup)
+        ft = rfftn(sup)
+        del sup
         f = form_factor(mw[inside], plan.coeffs[t])
         acc[inside] += f * ft[inside]
     modx, mody, modz = plan.mod

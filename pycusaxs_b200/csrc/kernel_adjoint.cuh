@@ -279,9 +279,10 @@ __global__ void __launch_bounds__(kThreads) k_gather(DevArgs a, AdjArgs j) {
   const float x0 = p[0], y0 = p[1], z0 = p[2];
   float r[3], w[3][4], dw[3][4];
   int m[3];
+  bool bad = false;  // a non-finite position: placed at 0 (the forward reports it)
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
-    r[d] = grid_coord(oc + 3 * d, x0, y0, z0, a.n[d]);
+    r[d] = grid_coord_checked(oc + 3 * d, x0, y0, z0, a.n[d], bad);
     m[d] = static_cast<int>(r[d]);
     const float u = r[d] - static_cast<float>(m[d]);
     cubic_weights(u, w[d]);

@@ -221,7 +221,7 @@ __global__ void __launch_bounds__(dtc_threads<kX>(), 1)
     if (abort_flag) return;
     if (!mbar_wait(smem_addr(bar), static_cast<uint32_t>(parity & 1))) {
       abort_flag = 1;
-      atomicExch(a.status, 1);
+      atomicOr(a.status, kX ? kStatusX : kStatusY);
     }
   };
 
@@ -684,3 +684,33 @@ __global__ void k_accumulate(DevArgs a, int nframes) {
   a.iacc[p] = s;
 }
 
+// grid 1, block 256: the last launch of the allocation-free single-frame
+// forward.  When a kernel of the frame reported an error through the status
+// word, the frame's histogram is overwritten with NaN: the caller of that
+// asynchronous call receives no status code for it, so the error travels in
+// the output itself.
+__global__ void k_flag_invalid(const int *status, double *hist, double *nhist, int nb) {
+  if (status[0] == 0) return;
+  const double nan = __longlong_as_double(0x7ff8000000000000ll);
+  for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+    hist[b] = nan;
+    nhist[b] = nan;
+  }
+}
+
+// grid 1, block 32: the bounded mbarrier wait of the pipelined kernels
+// (mbar_wait_for) on a barrier that no thread arrives at, so that it gives up
+// after `limit_ns` and sets kStatusProbe in the status word, as those kernels
+// set their bits.  Nothing else is in flight in this kernel, so giving up
+// leaves no copy or tensor-core operation behind.
+__global__ void k_wait_probe(int *status, unsigned long long limit_ns) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&bar)), "r"(1));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && !mbar_wait_for(smem_addr(&bar), 0u, limit_ns)) atomicOr(status, kStatusProbe);
+  __syncthreads();
+  if (threadIdx.x == 0) asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(&bar)) : "memory");
+}

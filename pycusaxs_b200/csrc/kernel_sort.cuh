@@ -94,6 +94,7 @@ __global__ void __launch_bounds__(kSortThreads, 2)
   int2 *key = a.key + static_cast<int64_t>(f) * a.M;
   const int bsh = __ffs(a.bin_w) - 1;  // bins are 4 or 8 columns wide
   double contrib = 0.0;
+  bool bad = false;  // a NaN or infinite position among this thread's atoms
   // kSortU entries per thread per round, their loads issued before any of their
   // arithmetic so that the position gathers overlap
   for (int eb = s0e + tid; eb < s1e; eb += kSortU * kSortThreads) {
@@ -119,7 +120,7 @@ __global__ void __launch_bounds__(kSortThreads, 2)
       int m[3];
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
-        rr[d] = grid_coord(oc + 3 * d, px[u][0], px[u][1], px[u][2], a.n[d]);
+        rr[d] = grid_coord_checked(oc + 3 * d, px[u][0], px[u][1], px[u][2], a.n[d], bad);
         m[d] = static_cast<int>(rr[d]);
       }
       int xf = m[0] - a.order;
@@ -148,6 +149,7 @@ __global__ void __launch_bounds__(kSortThreads, 2)
       contrib += static_cast<double>(sx) * static_cast<double>(sy) * static_cast<double>(sz);
     }
   }
+  if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(a.status, kStatusInput);
   contrib = warp_sum(contrib);
   if (lane == 0) wsum[warp] = contrib;
   __syncthreads();
@@ -245,13 +247,15 @@ __global__ void __launch_bounds__(kSortThreads, 2)
         px[u][1] = p[1];
         px[u][2] = p[2];
       }
+    // (a non-finite coordinate was reported in pass 1; here it only becomes 0)
 #pragma unroll
     for (int u = 0; u < kSortU; ++u)
       if (at[u] >= 0)
-        rec[sbase[k[u].x] + k[u].y] = make_float4(grid_coord(oc + 0, px[u][0], px[u][1], px[u][2], a.n[0]),
-                                                  grid_coord(oc + 3, px[u][0], px[u][1], px[u][2], a.n[1]),
-                                                  grid_coord(oc + 6, px[u][0], px[u][1], px[u][2], a.n[2]),
-                                                  __int_as_float(eb + u * kSortThreads));
+        rec[sbase[k[u].x] + k[u].y] =
+            make_float4(grid_coord_checked(oc + 0, px[u][0], px[u][1], px[u][2], a.n[0], bad),
+                        grid_coord_checked(oc + 3, px[u][0], px[u][1], px[u][2], a.n[1], bad),
+                        grid_coord_checked(oc + 6, px[u][0], px[u][1], px[u][2], a.n[2], bad),
+                        __int_as_float(eb + u * kSortThreads));
   }
   cluster_wait();
 }

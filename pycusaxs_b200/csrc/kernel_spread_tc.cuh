@@ -90,17 +90,23 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
   return done != 0;
 }
 
-// Bounded wait: at most 2^16 + 1 tries and 2 s.  The global timer is read only
-// once the first try has failed (a read of it costs hundreds of cycles, and most
-// waits in the pipelines below find their phase already complete).
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+// Bounded wait: at most 2^16 + 1 tries and `limit_ns`.  The global timer is
+// read only once the first try has failed (a read of it costs hundreds of
+// cycles, and most waits in the pipelines below find their phase already
+// complete).
+__device__ __forceinline__ bool mbar_wait_for(uint32_t bar, uint32_t parity, unsigned long long limit_ns) {
   if (mbar_try(bar, parity)) return true;
   const uint64_t t0 = global_ns();
   for (int it = 0; it < (1 << 16); ++it) {
     if (mbar_try(bar, parity)) return true;
-    if (global_ns() - t0 > 2000000000ull) return false;
+    if (global_ns() - t0 > limit_ns) return false;
   }
   return false;
+}
+
+// The pipelines' waits: 2 s.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  return mbar_wait_for(bar, parity, 2000000000ull);
 }
 
 __device__ __forceinline__ float tf32_head(float v) {
@@ -402,7 +408,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_spread_zdft_tc(DevArgs a, int
     if (abort_flag) return;
     if (!mbar_wait(smem_addr(bar), static_cast<uint32_t>(parity & 1))) {
       abort_flag = 1;
-      atomicExch(a.status, 1);
+      atomicOr(a.status, kStatusZ);
     }
   };
 

@@ -348,7 +348,7 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
     if (abort_flag) return;
     if (!mbar_wait(smem_addr(bar), static_cast<uint32_t>(parity & 1))) {
       abort_flag = 1;
-      atomicExch(a.status, 1);
+      atomicOr(a.status, kStatusZ);
     }
   };
   // bounded wait until the MMAs of the first `n` chunks are complete: an acquire
@@ -366,7 +366,7 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
     while (released_acquire() < n && !abort_flag) {
       if (global_ns() - t0 > 2000000000ull) {
         abort_flag = 1;
-        atomicExch(a.status, 1);
+        atomicOr(a.status, kStatusZ);
       }
       __nanosleep(64);
     }
@@ -415,6 +415,8 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
           }
           spread_taps_w(tab, tab_count[group][ip][k & 1], reinterpret_cast<int *>(A), RS, gtid, gthreads);
         }
+        // diagnostic: the most table chunks an item needed
+        if (gtid == 0 && nvis > cap) atomicMax(a.status + 1, (nvis + cap - 1) / cap);
       }
       producers_sync(bar_id, gthreads);
       if (gtid == 0) mbar_arrive(smem_addr(&rec_empty[b]));

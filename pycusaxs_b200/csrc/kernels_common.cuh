@@ -17,6 +17,17 @@ constexpr int kYStride = kYRows + 2;      // padded shared row (float2), 16-byte
 constexpr int kXRows = 4;                 // ky rows per CTA in k_xdft_post
 constexpr int kHistSmemBins = 2048;       // bins held in shared memory by k_hist
 
+// Bits of the status word (DevArgs::status[0]) a kernel sets when one of its
+// bounded waits gives up; the work of that launch, and every result that
+// depends on it, is then invalid.  status[1] holds the most atom-table chunks
+// one item of the wide spreading kernel needed (a diagnostic, not an error).
+constexpr int kStatusZ = 1;      // spreading + z-axis DFT (tensor-core kernels)
+constexpr int kStatusY = 2;      // y-axis DFT (tensor-core kernel)
+constexpr int kStatusX = 4;      // x-axis DFT + post (tensor-core kernel)
+constexpr int kStatusProbe = 8;  // the bounded-wait probe (saxs_debug_wait_probe)
+constexpr int kStatusInput = 16; // a position was NaN or infinite (k_sort_atoms)
+constexpr int kStatusWords = 4;
+
 thread_local std::string g_err;
 
 int fail(int code, const std::string &msg) {
@@ -95,6 +106,17 @@ struct DevArgs {
 __device__ __forceinline__ float grid_coord(const float *oc, float x0, float y0, float z0, int n) {
   float x1 = oc[0] * x0 + oc[1] * y0 + oc[2] * z0;
   return static_cast<float>(n * (x1 - rint(x1 - 0.5)));
+}
+
+// The same, with a result outside [0, n] - only a NaN or infinite position
+// gives one - replaced by 0 and reported in `bad`.  Stencil indices are derived
+// from these values by truncation, so they must stay inside the cell.
+__device__ __forceinline__ float grid_coord_checked(const float *oc, float x0, float y0, float z0, int n,
+                                                   bool &bad) {
+  const float r = grid_coord(oc, x0, y0, z0, n);
+  if (r >= 0.0f && r <= static_cast<float>(n)) return r;
+  bad = true;
+  return 0.0f;
 }
 
 // |q| of the k-point with signed indices (ia, ja, ka), in the reference's

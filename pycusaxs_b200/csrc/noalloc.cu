@@ -19,9 +19,17 @@
 //    left in it; the call clears the parts that accumulate.  Two calls whose
 //    work overlaps on the GPU (different streams, or different host threads on
 //    the same device) overwrite each other's temporaries: serialise them.
-//  * The first call on a device looks up the array's device address with that
-//    device current (cudaGetSymbolAddress) and caches it; make that first call
-//    before any stream capture begins.
+//  * The array's device address is looked up (cudaGetSymbolAddress, with the
+//    device current) by saxs_plan_create, which also loads the array onto the
+//    device then, at a time when the caller accepts allocations; the address is
+//    cached per device.  Only if that look-up failed does the first call do it
+//    (and that call should then come before any stream capture).  A device
+//    reset (cudaDeviceReset) invalidates plans and the cached address alike;
+//    plans created after it refresh the address.
+//  * A kernel of the frame that gives up on a bounded wait, or positions that
+//    hold NaN or infinity, make the call's histogram NaN: the call is
+//    asynchronous and cannot return that status itself.  The plan's own status
+//    word and accumulators are untouched.
 //  * The call allocates nothing: no cudaMalloc, cudaFree or allocating library
 //    routine is reached from it.  The plan itself is created (and allocates)
 //    with saxs_plan_create beforehand, at a time when allocating is acceptable.
@@ -46,12 +54,13 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 std::mutex g_mu;
 void *g_scratch_ptr[kMaxDevices] = {};
 
-// Device address of the scratch block on `device` (which must be current).
-int scratch_address(int device, unsigned char **out) {
+// Device address of the scratch block on `device` (which must be current);
+// `refresh` looks it up again even when an address is cached.
+int scratch_address(int device, unsigned char **out, bool refresh = false) {
   if (device < 0 || device >= kMaxDevices)
     return saxs::record_error(SAXS_E_INVALID, "device ordinal out of range");
   std::lock_guard<std::mutex> lock(g_mu);
-  if (!g_scratch_ptr[device]) {
+  if (!g_scratch_ptr[device] || refresh) {
     void *p = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess || !p) {
@@ -68,8 +77,18 @@ int scratch_address(int device, unsigned char **out) {
 
 }  // namespace
 
+namespace saxs {
+
+int noalloc_attach(int device) {
+  unsigned char *p = nullptr;
+  return scratch_address(device, &p, true);
+}
+
+}  // namespace saxs
+
 extern "C" int saxs_forward_noalloc(SaxsPlan *plan, const float *xyz_dev, const float *box_host,
                                     double *hist_dev, double *nhist_dev, void *stream) {
+  saxs::clear_error();
   if (!plan) return saxs::record_error(SAXS_E_INVALID, "null plan");
   const size_t need = saxs::single_frame_scratch_bytes(plan);
   if (need > kScratchBytes) {

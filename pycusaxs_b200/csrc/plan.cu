@@ -39,6 +39,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <string>
@@ -84,6 +85,8 @@ struct SaxsPlan {
   SaxsParams p{};
   std::vector<float> ff;
   std::vector<float> pad;  // given padding densities per type (empty: z-border mean)
+  std::vector<int32_t> ea_host, et_host;  // the caller's atom lists, kept to re-plan a wider k-box
+  int graph_refs = 0;      // graphs (saxs_graph_create) holding this plan's buffers
   DevArgs a{};
   int ensemble = SAXS_NPT;
   long long half[3] = {0, 0, 0};
@@ -349,7 +352,9 @@ std::vector<float> dtc_bprime(const std::vector<float2> &tw, int stride, int ext
   return out;
 }
 
-int create(const SaxsParams *prm, SaxsPlan **out) {
+// `min_half`, when given, is the smallest k-box half-width per axis the plan
+// must have (a re-plan for a frame whose box grew past the margin).
+int create(const SaxsParams *prm, SaxsPlan **out, const long long *min_half = nullptr) {
   if (!prm || !out) return fail(SAXS_E_INVALID, "null argument");
   *out = nullptr;
   const SaxsParams &p = *prm;
@@ -410,6 +415,10 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
   pl->p.padding_values = nullptr;  // the caller's array is not kept
   pl->ensemble = p.ensemble;
   pl->ff.assign(p.form_factors, p.form_factors + 9 * p.ntypes);
+  pl->ea_host.assign(p.entry_atom, p.entry_atom + p.nentries);
+  pl->et_host.assign(p.entry_type, p.entry_type + p.nentries);
+  pl->p.form_factors = nullptr;  // nor are the caller's arrays
+  pl->p.entry_atom = pl->p.entry_type = nullptr;
   DevArgs &a = pl->a;
   for (int d = 0; d < 3; ++d) {
     a.n[d] = p.grid[d];
@@ -466,6 +475,8 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
   // for boxes up to `box_margin` smaller.
   const double margin = std::max(0.0f, p.box_margin) + 1e-5;
   saxs::kbox_halfwidths(ocs0, a.qcut, margin, pl->half);
+  if (min_half)
+    for (int d = 0; d < 3; ++d) pl->half[d] = std::max(pl->half[d], min_half[d]);
   for (int d = 0; d < 2; ++d) {
     const long long hmax = a.nf[d] - 1;
     if (pl->half[d] >= hmax) {
@@ -631,6 +642,28 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
 
   const int B = p.max_frames;
   const int ex = a.ext[0], ey = a.ext[1], ez = a.ext[2];
+  {
+    // free-memory check before allocating, as the reference does
+    // (saxsKernel.cu:284-314), over the buffers that grow with the frames per call
+    const size_t per_frame = (sizeof(int2) + sizeof(float4)) * static_cast<size_t>(a.M) +
+                             sizeof(int) * (static_cast<size_t>(a.nbins) + 1) + sizeof(double) * a.T +
+                             sizeof(float2) * static_cast<size_t>(a.T) * a.nkz * ex * ey +
+                             sizeof(float2) * static_cast<size_t>(a.T) * a.nkz * a.nky * ex +
+                             sizeof(float) * static_cast<size_t>(a.nkz) * a.nky * a.nkx;
+    const double need = static_cast<double>(per_frame) * B;
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+      cudaGetLastError();
+    } else if (need > static_cast<double>(fr)) {
+      destroy(pl);
+      char msg[256];
+      std::snprintf(msg, sizeof(msg),
+                    "not enough device memory: %d frames per call need %.3g GB of frame buffers, "
+                    "%.3g GB of %.3g GB are free (lower max_frames)",
+                    B, need / 1e9, fr / 1e9, tot / 1e9);
+      return fail(SAXS_E_NOMEM, msg);
+    }
+  }
   int rc = SAXS_OK;
   int32_t *d_ea = nullptr, *d_et = nullptr;
   float2 *d_twz = nullptr, *d_twy = nullptr, *d_twx = nullptr;
@@ -849,6 +882,12 @@ int create(const SaxsParams *prm, SaxsPlan **out) {
   if (e == cudaSuccess) e = raise_smem_limit(k_spread_zdft_tcw);
   if (e == cudaSuccess) e = raise_smem_limit(k_dft_tc<false>);
   if (e == cudaSuccess) e = raise_smem_limit(k_dft_tc<true>);
+  // load the allocation-free forward's last kernel now (under lazy module
+  // loading a kernel's code is loaded at its first use), so that call loads nothing
+  if (e == cudaSuccess) {
+    cudaFuncAttributes fa{};
+    e = cudaFuncGetAttributes(&fa, k_flag_invalid);
+  }
   if (e == cudaSuccess) {
     int per_sm = 0, sms = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_spread_zdft, kThreads,
@@ -1149,6 +1188,99 @@ int enqueue_batch(SaxsPlan *pl, const DevArgs &a, int nframes, cudaStream_t st, 
   return SAXS_OK;
 }
 
+// Widen the plan's k-box in place to half-widths of at least `need` (plus 5%
+// headroom): a new plan with the same parameters and atoms, the kernel
+// configuration kept where the new plan can run it, the accumulators, status
+// words, frame count and pending profile records carried over; the caller's
+// SaxsPlan pointer stays valid.  Waits for `st`.  Refused for plans whose
+// buffers a graph holds.
+int regrow(SaxsPlan *pl, const long long need[3], cudaStream_t st) {
+  if (pl->graph_refs > 0)
+    return fail(SAXS_E_RANGE, "a frame's box grew beyond the planned k-box margin and the plan is "
+                              "captured in a graph, whose buffers cannot move; create the plan with a "
+                              "larger box_margin");
+  CUDA_TRY(cudaStreamSynchronize(st));
+  SaxsParams p = pl->p;
+  p.form_factors = pl->ff.data();
+  p.entry_atom = pl->ea_host.data();
+  p.entry_type = pl->et_host.data();
+  p.padding_values = pl->pad.empty() ? nullptr : pl->pad.data();
+  long long minh[3];
+  for (int d = 0; d < 3; ++d) minh[d] = std::max(pl->half[d], need[d] + need[d] / 20 + 1);
+  SaxsPlan *np = nullptr;
+  if (int rc = create(&p, &np, minh)) return rc;
+  const DevArgs &o = pl->a;
+  DevArgs &n = np->a;
+  int rc = SAXS_OK;
+  auto cuda = [&](cudaError_t e, const char *what) {
+    if (e != cudaSuccess && rc == SAXS_OK) rc = fail(SAXS_E_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+  };
+  // accumulators: Delta-q, q-cut and the bins depend on the first box only, so
+  // the histograms carry over as they are; an nvt intensity sum moves into the
+  // matching k-points of the wider box
+  cuda(cudaMemcpyAsync(n.hist, o.hist, sizeof(double) * o.num_bins, cudaMemcpyDeviceToDevice, st), "regrow");
+  cuda(cudaMemcpyAsync(n.nhist, o.nhist, sizeof(double) * o.num_bins, cudaMemcpyDeviceToDevice, st), "regrow");
+  cuda(cudaMemcpyAsync(n.status, o.status, sizeof(int) * kStatusWords, cudaMemcpyDeviceToDevice, st), "regrow");
+  if (o.iacc && rc == SAXS_OK) {
+    std::vector<double> src(static_cast<size_t>(o.nkz) * o.nky * o.nkx);
+    std::vector<double> dst(static_cast<size_t>(n.nkz) * n.nky * n.nkx, 0.0);
+    cuda(cudaMemcpy(src.data(), o.iacc, sizeof(double) * src.size(), cudaMemcpyDeviceToHost), "regrow");
+    const int dx = o.kx_lo - n.kx_lo, dy = o.ky_lo - n.ky_lo;
+    for (int kz = 0; kz < o.nkz; ++kz)
+      for (int ky = 0; ky < o.nky; ++ky)
+        for (int kx = 0; kx < o.nkx; ++kx)
+          dst[(static_cast<size_t>(kz) * n.nky + ky + dy) * n.nkx + kx + dx] =
+              src[(static_cast<size_t>(kz) * o.nky + ky) * o.nkx + kx];
+    cuda(cudaMemcpy(n.iacc, dst.data(), sizeof(double) * dst.size(), cudaMemcpyHostToDevice), "regrow");
+  }
+  cuda(cudaStreamSynchronize(st), "regrow");
+  if (rc != SAXS_OK) {
+    destroy(np);
+    return rc;
+  }
+  // the kernel configuration in use (an autotuned choice), where it still fits
+  if ((!pl->use_tc || (pl->use_tcw ? np->tcw_ok : np->tcn_ok)) && (!pl->use_ytc || np->ytc_ok) &&
+      (!pl->use_xtc || np->xtc_ok)) {
+    np->use_tc = pl->use_tc;
+    np->use_tcw = pl->use_tcw;
+    np->use_ytc = pl->use_ytc;
+    np->use_xtc = pl->use_xtc;
+    if (np->use_tc && np->use_tcw && pl->a.twG <= np->twG_max) set_wide_groups(np, pl->a.twG);
+    if (np->use_tc && !np->use_tcw && np->a.tcS == 2) np->a.tcG = pl->a.tcG;
+  }
+  np->frames = pl->frames;
+  np->profiling = pl->profiling;
+  np->prof_pending.swap(pl->prof_pending);
+  np->event_pool.swap(pl->event_pool);
+  std::swap(*pl, *np);
+  destroy(np);  // the old buffers
+  return SAXS_OK;
+}
+
+// Check the boxes of `nframes` frames against the plan's k-box; when one needs
+// a larger k-box, widen the plan (`grow`) or return SAXS_E_RANGE.
+int fit_kbox(SaxsPlan *pl, const float *boxes, int nframes, cudaStream_t st, bool grow) {
+  long long need[3] = {0, 0, 0};
+  bool over = false;
+  for (int f = 0; f < nframes; ++f) {
+    const float *box = boxes + 9 * f;
+    if (int rc = check_box(box)) return rc;
+    float g[kGeom];
+    frame_geometry(pl, box, g);
+    long long h[3];
+    saxs::kbox_halfwidths(g + 9, pl->a.qcut, 1e-5, h);
+    for (int d = 0; d < 3; ++d) {
+      need[d] = std::max(need[d], h[d]);
+      over |= !pl->full_axis[d] && h[d] > pl->half[d];
+    }
+  }
+  if (!over) return SAXS_OK;
+  if (!grow)
+    return fail(SAXS_E_RANGE, "a frame's box grew beyond the planned k-box margin; create the plan "
+                              "with a larger box_margin, or use saxs_forward, which widens the plan");
+  return regrow(pl, need, st);
+}
+
 int forward(SaxsPlan *pl, const float *xyz, int64_t stride, int nframes, const float *boxes,
             cudaStream_t st) {
   if (!pl) return fail(SAXS_E_INVALID, "null plan");
@@ -1156,6 +1288,7 @@ int forward(SaxsPlan *pl, const float *xyz, int64_t stride, int nframes, const f
     return fail(SAXS_E_INVALID, "nframes must be in [1, max_frames]");
   if (!boxes || (!xyz && pl->a.M > 0)) return fail(SAXS_E_INVALID, "null positions or boxes");
   if (stride < 3ll * pl->p.natoms) return fail(SAXS_E_INVALID, "frame stride smaller than 3*natoms");
+  if (int rc = fit_kbox(pl, boxes, nframes, st, true)) return rc;
   DevArgs a = pl->a;
   a.xyz = xyz;
   a.frame_stride = stride;
@@ -1165,18 +1298,7 @@ int forward(SaxsPlan *pl, const float *xyz, int64_t stride, int nframes, const f
   ring.next = (ring.next + 1) % kRing;
   CUDA_TRY(cudaEventSynchronize(ring.ev[slot]));
   float *g = ring.host + static_cast<size_t>(slot) * pl->p.max_frames * kGeom;
-  for (int f = 0; f < nframes; ++f) {
-    const float *box = boxes + 9 * f;
-    if (int rc = check_box(box)) return rc;
-    frame_geometry(pl, box, g + f * kGeom);
-    long long h[3];
-    saxs::kbox_halfwidths(g + f * kGeom + 9, a.qcut, 1e-5, h);
-    for (int d = 0; d < 3; ++d) {
-      if (!pl->full_axis[d] && h[d] > pl->half[d])
-        return fail(SAXS_E_RANGE, "frame box shrank beyond the planned k-box margin; "
-                                  "create the plan with a larger box_margin");
-    }
-  }
+  for (int f = 0; f < nframes; ++f) frame_geometry(pl, boxes + 9 * f, g + f * kGeom);
   // the geometry travels as k_sort_atoms' kernel parameters
   if (int rc = enqueue_batch(pl, a, nframes, st, true, g)) return rc;
   pl->frames += nframes;
@@ -1197,12 +1319,15 @@ struct SaxsGraph {
   cudaGraphExec_t exec[2] = {nullptr, nullptr};
   cudaEvent_t done[2] = {nullptr, nullptr};
   int next = 0;
+  bool holds_plans = false;  // the plans' graph_refs count this graph
 };
 
 namespace {
 
 void graph_destroy(SaxsGraph *g) {
   if (!g) return;
+  if (g->holds_plans)
+    for (SaxsPlan *pl : g->plans) --pl->graph_refs;
   int prev = 0;
   cudaGetDevice(&prev);
   cudaSetDevice(g->device);
@@ -1297,6 +1422,8 @@ int graph_create(SaxsPlan *const *plans, const float *const *xyz, const int64_t 
     cudaGetLastError();
     return fail(SAXS_E_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
   }
+  for (SaxsPlan *pl : g->plans) ++pl->graph_refs;  // their buffers may no longer move
+  g->holds_plans = true;
   *out = g;
   return SAXS_OK;
 }
@@ -1318,7 +1445,9 @@ int graph_launch(SaxsGraph *g, const float *boxes, cudaStream_t st) {
       saxs::kbox_halfwidths(geo + 9, pl->a.qcut, 1e-5, h);
       for (int d = 0; d < 3; ++d)
         if (!pl->full_axis[d] && h[d] > pl->half[d])
-          return fail(SAXS_E_RANGE, "frame box shrank beyond the planned k-box margin");
+          return fail(SAXS_E_RANGE, "a frame's box grew beyond the planned k-box margin of plan " +
+                                        std::to_string(i) + "; a graph's buffers cannot move: create "
+                                        "the plan with a larger box_margin");
     }
   }
   CUDA_TRY(cudaGraphLaunch(g->exec[slot], st));
@@ -1328,6 +1457,21 @@ int graph_launch(SaxsGraph *g, const float *boxes, cudaStream_t st) {
     g->plans[i]->last_frame_batch = g->nframes[i];
   }
   return SAXS_OK;
+}
+
+// The message of a non-zero status word (kStatus* bits).
+std::string status_message(int bits) {
+  std::string who;
+  auto add = [&](const char *name) {
+    if (!who.empty()) who += "; ";
+    who += name;
+  };
+  if (bits & kStatusInput) add("k_sort_atoms: a position was NaN or infinite (placed at the cell origin)");
+  if (bits & kStatusZ) add("the spreading + z-axis DFT kernel (k_spread_zdft_tcw / k_spread_zdft_tc): a bounded wait gave up");
+  if (bits & kStatusY) add("the y-axis DFT kernel (k_dft_tc<y>): a bounded wait gave up");
+  if (bits & kStatusX) add("the x-axis DFT kernel (k_dft_tc<x>): a bounded wait gave up");
+  if (bits & kStatusProbe) add("the bounded-wait probe (k_wait_probe) gave up, as asked");
+  return who + "; the frames processed since then are invalid (saxs_reset clears this error)";
 }
 
 int histogram(SaxsPlan *pl, double *hist, double *nhist, cudaStream_t st) {
@@ -1353,8 +1497,7 @@ int histogram(SaxsPlan *pl, double *hist, double *nhist, cudaStream_t st) {
   int status = 0;
   CUDA_TRY(cudaMemcpyAsync(&status, a.status, sizeof(int), cudaMemcpyDeviceToHost, st));
   CUDA_TRY(cudaStreamSynchronize(st));
-  if (status != 0)
-    return fail(SAXS_E_CUDA, "tensor-core z-DFT: an MMA completion wait ran out; results are invalid");
+  if (status != 0) return fail(SAXS_E_DEVICE, status_message(status));
   return SAXS_OK;
 }
 
@@ -1408,7 +1551,7 @@ int ensure_adjoint(SaxsPlan *pl) {
 int backward(SaxsPlan *pl, const float *xyz, const float *box, const double *dl, float *grad,
              cudaStream_t st) {
   if (!pl || !box || !dl || !grad || (!xyz && pl->a.M > 0)) return fail(SAXS_E_INVALID, "null argument");
-  if (int rc = check_box(box)) return rc;
+  if (int rc = fit_kbox(pl, box, 1, st, true)) return rc;
   if (int rc = ensure_adjoint(pl)) return rc;
   DevArgs a = pl->a;
   a.xyz = xyz;
@@ -1433,11 +1576,6 @@ int backward(SaxsPlan *pl, const float *xyz, const float *box, const double *dl,
   CUDA_TRY(cudaEventSynchronize(ring.ev[slot]));
   float *g = ring.host + static_cast<size_t>(slot) * pl->p.max_frames * kGeom;
   frame_geometry(pl, box, g);
-  long long h[3];
-  saxs::kbox_halfwidths(g + 9, a.qcut, 1e-5, h);
-  for (int d = 0; d < 3; ++d)
-    if (!pl->full_axis[d] && h[d] > pl->half[d])
-      return fail(SAXS_E_RANGE, "frame box shrank beyond the planned k-box margin");
   CUDA_TRY(cudaMemcpyAsync(const_cast<float *>(a.geom), g, sizeof(float) * kGeom,
                            cudaMemcpyHostToDevice, st));
   CUDA_TRY(cudaEventRecord(ring.ev[slot], st));
@@ -1486,13 +1624,15 @@ namespace {
 
 // Byte offsets of the per-frame buffers inside one scratch block.
 struct ScratchLayout {
-  size_t geom, key, offsets, rec, border, Z, Y, ibox, total;
+  size_t status, geom, key, offsets, rec, border, Z, Y, ibox, total;
 };
 
 ScratchLayout scratch_layout(const DevArgs &a) {
   auto up = [](size_t v) { return (v + 255) / 256 * 256; };
   ScratchLayout L{};
   size_t o = 0;
+  L.status = o;
+  o = up(o + sizeof(int) * kStatusWords);
   L.geom = o;
   o = up(o + sizeof(float) * kGeom);
   L.key = o;
@@ -1521,11 +1661,14 @@ size_t single_frame_scratch_bytes(const SaxsPlan *plan) { return scratch_layout(
 
 int record_error(int code, const char *msg) { return fail(code, msg); }
 
+void clear_error() { g_err.clear(); }
+
 int forward_into_scratch(SaxsPlan *pl, const float *xyz, const float *box, unsigned char *scratch,
                          size_t scratch_bytes, double *hist, double *nhist, cudaStream_t st) {
   if (!pl || !box || !scratch || !hist || !nhist || (!xyz && pl->a.M > 0))
     return fail(SAXS_E_INVALID, "null argument");
-  if (int rc = check_box(box)) return rc;
+  // widening the k-box would allocate: a box beyond the margin is refused
+  if (int rc = fit_kbox(pl, box, 1, st, false)) return rc;
   DevArgs a = pl->a;
   const ScratchLayout L = scratch_layout(a);
   if (L.total > scratch_bytes) return fail(SAXS_E_RANGE, "scratch too small for this plan");
@@ -1541,6 +1684,9 @@ int forward_into_scratch(SaxsPlan *pl, const float *xyz, const float *box, unsig
   a.ibox = reinterpret_cast<float *>(scratch + L.ibox);
   a.hist = hist;
   a.nhist = nhist;
+  // the frame's own status words: the plan's are left alone, and a frame whose
+  // kernels report an error gets a NaN histogram (k_flag_invalid)
+  a.status = reinterpret_cast<int *>(scratch + L.status);
   // frame geometry, checked against the k-box, staged through the plan's pinned ring
   Ring &ring = pl->ring;
   const int slot = ring.next;
@@ -1548,24 +1694,22 @@ int forward_into_scratch(SaxsPlan *pl, const float *xyz, const float *box, unsig
   CUDA_TRY(cudaEventSynchronize(ring.ev[slot]));
   float *g = ring.host + static_cast<size_t>(slot) * pl->p.max_frames * kGeom;
   frame_geometry(pl, box, g);
-  long long h[3];
-  kbox_halfwidths(g + 9, a.qcut, 1e-5, h);
-  for (int d = 0; d < 3; ++d)
-    if (!pl->full_axis[d] && h[d] > pl->half[d])
-      return fail(SAXS_E_RANGE, "frame box shrank beyond the planned k-box margin");
   CUDA_TRY(cudaMemcpyAsync(const_cast<float *>(a.geom), g, sizeof(float) * kGeom,
                            cudaMemcpyHostToDevice, st));
   CUDA_TRY(cudaEventRecord(ring.ev[slot], st));
   // the block keeps the previous call's contents: clear what accumulates
   CUDA_TRY(cudaMemsetAsync(hist, 0, sizeof(double) * a.num_bins, st));
   CUDA_TRY(cudaMemsetAsync(nhist, 0, sizeof(double) * a.num_bins, st));
+  CUDA_TRY(cudaMemsetAsync(a.status, 0, sizeof(int) * kStatusWords, st));
   if (int rc = launch_sort(pl, a, 1, st)) return rc;
   if (int rc = launch_spread(pl, a, 1, st)) return rc;
   if (int rc = launch_ydft(pl, a, a.T * a.nkz, st)) return rc;
   if (int rc = launch_xdft(pl, a, 1, st)) return rc;
   dim3 gh(a.nkz, 1);
   k_hist<float><<<gh, kThreads, pl->smem_hist, st>>>(a, a.ibox, a.geom, kGeom, 1.0, hist, nhist);
-  return launch_check("k_hist");
+  if (int rc = launch_check("k_hist")) return rc;
+  k_flag_invalid<<<1, kThreads, 0, st>>>(a.status, hist, nhist, a.num_bins);
+  return launch_check("k_flag_invalid");
 }
 
 }  // namespace saxs
@@ -1577,7 +1721,12 @@ extern "C" {
 
 int saxs_plan_create(const SaxsParams *params, SaxsPlan **plan) {
   g_err.clear();
-  return create(params, plan);
+  const int rc = create(params, plan);
+  // look up the allocation-free entry point's scratch array now, while the
+  // caller can afford a load of it onto the device (a failure is not the
+  // plan's: that entry point tries again and reports it)
+  if (rc == SAXS_OK && saxs::noalloc_attach((*plan)->device) != SAXS_OK) g_err.clear();
+  return rc;
 }
 
 void saxs_plan_destroy(SaxsPlan *plan) { destroy(plan); }
@@ -1664,8 +1813,32 @@ int saxs_reset(SaxsPlan *pl, void *stream) {
   CUDA_TRY(cudaMemsetAsync(a.hist, 0, sizeof(double) * a.num_bins, st));
   CUDA_TRY(cudaMemsetAsync(a.nhist, 0, sizeof(double) * a.num_bins, st));
   if (a.iacc) CUDA_TRY(cudaMemsetAsync(a.iacc, 0, sizeof(double) * a.nkz * a.nky * a.nkx, st));
+  CUDA_TRY(cudaMemsetAsync(a.status, 0, sizeof(int) * kStatusWords, st));
   pl->frames = 0;
   return SAXS_OK;
+}
+
+int saxs_debug_counters(SaxsPlan *pl, int *out, void *stream) {
+  if (!pl || !out) return fail(SAXS_E_INVALID, "null argument");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  CUDA_TRY(cudaMemcpyAsync(out, pl->a.status, sizeof(int) * kStatusWords, cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  return SAXS_OK;
+}
+
+int saxs_debug_wait_probe(SaxsPlan *pl, double limit_seconds, void *stream) {
+  g_err.clear();
+  if (!pl) return fail(SAXS_E_INVALID, "null plan");
+  if (!(limit_seconds > 0.0) || limit_seconds > 2.0)
+    return fail(SAXS_E_INVALID, "the probe's wait limit must be in (0, 2] seconds");
+  int prev = 0;
+  cudaGetDevice(&prev);
+  if (prev != pl->device) cudaSetDevice(pl->device);
+  k_wait_probe<<<1, 32, 0, static_cast<cudaStream_t>(stream)>>>(
+      pl->a.status, static_cast<unsigned long long>(limit_seconds * 1e9));
+  const int rc = launch_check("k_wait_probe");
+  if (prev != pl->device) cudaSetDevice(prev);
+  return rc;
 }
 
 int saxs_debug_kbox_intensity(SaxsPlan *pl, float *out, void *stream) {

@@ -23,7 +23,13 @@ int forward_into_scratch(SaxsPlan *plan, const float *xyz_dev, const float *box_
                          unsigned char *scratch, size_t scratch_bytes, double *hist_dev,
                          double *nhist_dev, cudaStream_t st);
 
-// Record a failure for saxs_last_error() and return `code`.
+// Record a failure for saxs_last_error() and return `code`; clear it.
 int record_error(int code, const char *msg);
+void clear_error();
+
+// Resolve (and cache) the device address of the allocation-free entry point's
+// scratch array on `device`, which loads the array onto that device.  Called
+// at plan creation; returns SAXS_OK or the error code (message recorded).
+int noalloc_attach(int device);
 
 }  // namespace saxs

@@ -143,9 +143,14 @@ class SaxsEngine:
         self.stream = torch.cuda.Stream(device=self.device)
         self._copy_stream = torch.cuda.Stream(device=self.device)
         self._staging = None
-        self.info = self._info()
 
     # -- plan information -------------------------------------------------
+    @property
+    def info(self) -> PlanInfo:
+        """Sizes of the plan.  Read afresh on every access: a frame whose box
+        grows beyond the k-box margin makes the plan widen its k-box."""
+        return self._info()
+
     def _info(self) -> PlanInfo:
         i = _native.SaxsPlanInfo()
         _native.check(self.lib.saxs_plan_info(self._plan, ctypes.byref(i)))
@@ -191,7 +196,6 @@ class SaxsEngine:
             if k in cfg:
                 setattr(c, k, int(cfg[k]))
         _native.check(self.lib.saxs_plan_set_config(self._plan, ctypes.byref(c)))
-        self.info = self._info()
 
     def tuning_key(self) -> str:
         """What a tuned configuration depends on: the grids, k-box, atoms, element
@@ -412,6 +416,24 @@ class SaxsEngine:
             self._plan, out.ctypes.data_as(_native.c_float_p),
             ctypes.c_void_p(self.stream.cuda_stream)))
         return out.reshape(nkz, nky, nkx)
+
+    def counters(self) -> dict:
+        """Kernel diagnostics since creation or the last reset (waits for the
+        device): ``status`` (0, or the bits of the kernels that reported an
+        error: 1 spreading/z pass, 2 y pass, 4 x pass, 8 wait probe, 16 a NaN or
+        infinite position) and ``table_chunks`` (the most atom-table chunks one
+        item of the wide spreading kernel needed; 0 when all fitted at once)."""
+        out = np.zeros(4, dtype=np.int32)
+        _native.check(self.lib.saxs_debug_counters(self._plan, out.ctypes.data_as(_native.c_int_p),
+                                                   ctypes.c_void_p(self.stream.cuda_stream)))
+        return {"status": int(out[0]), "table_chunks": int(out[1])}
+
+    def wait_probe(self, limit_s: float = 0.001) -> None:
+        """Run the kernels' bounded wait on a barrier nothing arrives at, so
+        that it gives up after ``limit_s`` and sets the plan's status word (the
+        next ``histogram()`` raises; ``reset()`` clears it)."""
+        _native.check(self.lib.saxs_debug_wait_probe(self._plan, float(limit_s),
+                                                     ctypes.c_void_p(self.stream.cuda_stream)))
 
     def border_sums(self) -> np.ndarray:
         out = np.zeros(len(self.type_names), dtype=np.float64)

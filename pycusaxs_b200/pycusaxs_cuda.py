@@ -184,6 +184,87 @@ class _PythonCallbackError(Exception):
     pass
 
 
+# Host bytes of positions one pinned batch of run() holds at most.
+_BATCH_BYTES = 64 << 20
+_BATCH_MAX = 32
+
+
+def _batch_frames(natoms: int, total: int) -> int:
+    """Frames per batch of run(): up to 32, at most 64 MB of positions, at
+    most the frames requested."""
+    per = max(1, 12 * int(natoms))
+    return int(max(1, min(_BATCH_MAX, _BATCH_BYTES // per, max(1, total))))
+
+
+def _frame_problem(pos, box, natoms: int) -> str:
+    """Why a frame cannot be processed (the checks saxs_forward would make),
+    or "" - so that a batch never fails for one bad frame."""
+    if pos.shape[0] < natoms:
+        return f"positions hold {pos.shape[0]} atoms, the topology indexes {natoms}"
+    if not np.all(np.isfinite(box)):
+        return "box contains a non-finite value"
+    if not (box[0, 0] > 0 and box[1, 1] > 0 and box[2, 2] > 0):
+        return "box diagonal must be positive"
+    return ""
+
+
+class _PinnedBatches:
+    """Frames of run() gathered into two alternating pinned host batches: a
+    full batch goes to the device in one ``forward_host`` call (its copy runs
+    on the engine's copy stream) while the next one fills; a batch is refilled
+    only after its copy has completed.  A batch that fails as a whole is
+    processed frame by frame, so that only the failing frames are reported and
+    skipped (RunSaxs.cu:195-199)."""
+
+    def __init__(self, engine, natoms: int, size: int):
+        import torch
+
+        self.engine = engine
+        self.natoms = natoms
+        self.size = size
+        self.host = [torch.empty((size, natoms, 3), dtype=torch.float32).pin_memory() for _ in range(2)]
+        self.view = [h.numpy() for h in self.host]
+        self.boxes = [np.zeros((size, 3, 3), dtype=np.float32) for _ in range(2)]
+        self.nums = [[], []]
+        self.copied = [None, None]
+        self.cur = 0
+
+    def add(self, fnum, pos, box):
+        b = self.cur
+        n = len(self.nums[b])
+        if n == 0 and self.copied[b] is not None:
+            self.copied[b].synchronize()  # the batch's previous copy is complete
+            self.copied[b] = None
+        self.view[b][n] = pos[: self.natoms]
+        self.boxes[b][n] = box
+        self.nums[b].append(fnum)
+        if n + 1 == self.size:
+            self.flush()
+
+    def flush(self):
+        import torch
+
+        b = self.cur
+        n = len(self.nums[b])
+        if n == 0:
+            return
+        eng = self.engine
+        try:
+            eng.forward_host(self.host[b][:n], self.boxes[b][:n])
+        except Exception:
+            eng._copy_stream.synchronize()
+            for k, fnum in enumerate(self.nums[b]):
+                try:
+                    eng.forward_host(self.view[b][k], self.boxes[b][k])
+                except Exception as exc:
+                    print(f"Error processing frame {fnum}: {exc}", file=sys.stderr)
+        ev = torch.cuda.Event()
+        ev.record(eng._copy_stream)  # the batch's copies are queued before this
+        self.copied[b] = ev
+        self.nums[b] = []
+        self.cur ^= 1
+
+
 def _call(fn, *args):
     try:
         return fn(*args)
@@ -216,9 +297,11 @@ def _run_frames(topo, grid, scaled, begin, end, stride, order, sigma, dq, qcut, 
                                                       {"Na": sodium, "Cl": chlorine})
             elif padding != "average":
                 raise ValueError(f"padding must be 'average' or 'given', not {padding!r}")
+            total = len(range(begin, end + 1, stride))
+            batch = _batch_frames(natoms, total)
             engine = SaxsEngine(grid, index, natoms, box0, scaled_grid=scaled or (0, 0, 0),
                                 order=order, scale_factor=sigma, bin_size=dq, qcut=qcut,
-                                ensemble=ensemble or "npt", max_frames=1, **ext)
+                                ensemble=ensemble or "npt", max_frames=batch, **ext)
         except KeyError as exc:
             raise RuntimeError(f"CuSAXS error: {exc.args[0]}") from None
         except ValueError as exc:
@@ -237,7 +320,7 @@ def _run_frames(topo, grid, scaled, begin, end, stride, order, sigma, dq, qcut, 
               f"(supercell); k-box {info.kbox[0]}x{info.kbox[1]}x{info.kbox[2]}; "
               f"device memory {info.device_bytes / 2**30:.2f} GB")
         frames_iter = iter(_call(topo.iter_frames_stream, begin, end + 1, stride))
-        nframes = 0
+        batches = _PinnedBatches(engine, natoms, batch)
         while True:
             try:
                 fr = next(frames_iter)
@@ -248,7 +331,7 @@ def _run_frames(topo, grid, scaled, begin, end, stride, order, sigma, dq, qcut, 
             try:
                 fnum = int(fr["frame"])
                 ftime = float(fr["time"])
-                pos = np.ascontiguousarray(np.asarray(fr["positions"], dtype=np.float32))
+                pos = np.asarray(fr["positions"], dtype=np.float32)
                 box = np.asarray(fr["box"], dtype=np.float32).reshape(3, 3)
                 if pos.ndim != 2 or pos.shape[1] != 3:
                     raise ValueError("positions must have shape (N, 3)")
@@ -256,12 +339,15 @@ def _run_frames(topo, grid, scaled, begin, end, stride, order, sigma, dq, qcut, 
                 print(f"Error loading frame data: {exc}", file=sys.stderr)
                 break
             print(f"--> Frame: {fnum:<7}  Time Step: {ftime:.2f} ps")
-            try:
-                if ensemble is not None:
-                    engine.forward_host(pos, box)
-                nframes += 1
-            except Exception as exc:
-                print(f"Error processing frame {fnum}: {exc}", file=sys.stderr)
+            if ensemble is None:
+                continue
+            problem = _frame_problem(pos, box, natoms)
+            if problem:
+                print(f"Error processing frame {fnum}: {problem}", file=sys.stderr)
+                continue
+            batches.add(fnum, pos, box)
+        if ensemble is not None:
+            batches.flush()
         rows = engine.profile() if ensemble is not None else []
         engine.close()
         try:

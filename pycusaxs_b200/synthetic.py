@@ -159,12 +159,16 @@ def uneven_systems(n_systems: int = 64, frames: int = 8, seed: int = 0, nmin: in
 class SyntheticTopology:
     """Topology duck type over a ``System`` (the reference's callback contract)."""
 
-    def __init__(self, system: System, dt_ps: float = 1.0, fail_at_frame: int | None = None):
+    def __init__(self, system: System, dt_ps: float = 1.0, fail_at_frame: int | None = None,
+                 frames=None):
+        """``frames``: the positions of every frame, precomputed ((F, N, 3)
+        float32); default: each frame generated from the seed when it is read."""
         self.system = system
-        self.n_frames = system.nframes
+        self.n_frames = system.nframes if frames is None else len(frames)
         self.dt = dt_ps
         self.ts = None
         self.fail_at_frame = fail_at_frame
+        self.frames = frames
 
     def get_atom_index(self):
         return self.system.atom_index()
@@ -184,5 +188,6 @@ class SyntheticTopology:
         for k in range(start, min(stop, self.n_frames), step):
             if self.fail_at_frame is not None and k == self.fail_at_frame:
                 raise RuntimeError(f"synthetic read failure at frame {k}")
-            yield {"frame": k, "time": k * self.dt, "positions": self.system.frame(k),
+            pos = self.system.frame(k) if self.frames is None else self.frames[k]
+            yield {"frame": k, "time": k * self.dt, "positions": pos,
                    "box": self.system.box.astype(np.float32)}

@@ -125,3 +125,24 @@ def test_run_saxs_calculation_checks_frames_against_topology(tmp_path):
            "grid_size": [16], "initial_frame": 0, "last_frame": 5}
     with pytest.raises(ValueError, match="Last frame 5 exceeds available frames"):
         core.run_saxs_calculation(req, {}, topology_factory=lambda a, b: Topo())
+
+
+def test_batch_size_of_run():
+    # up to 32 frames, at most 64 MB of positions, at most the frames requested
+    assert pycusaxs_cuda._batch_frames(100_000, 100) == 32
+    assert pycusaxs_cuda._batch_frames(1_000_000, 20) == 5
+    assert pycusaxs_cuda._batch_frames(100_000, 3) == 3
+    assert pycusaxs_cuda._batch_frames(50_000_000, 10) == 1
+
+
+def test_frame_checks_before_batching():
+    import numpy as np
+
+    pos = np.zeros((10, 3), np.float32)
+    box = np.diag([30.0, 30.0, 30.0]).astype(np.float32)
+    assert pycusaxs_cuda._frame_problem(pos, box, 10) == ""
+    assert "indexes 11" in pycusaxs_cuda._frame_problem(pos, box, 11)
+    assert "positive" in pycusaxs_cuda._frame_problem(pos, np.zeros((3, 3), np.float32), 10)
+    bad = box.copy()
+    bad[0, 1] = np.nan
+    assert "non-finite" in pycusaxs_cuda._frame_problem(pos, bad, 10)

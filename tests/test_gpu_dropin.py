@@ -101,3 +101,29 @@ def test_default_pybind_arguments_give_an_empty_profile(cuda, tmp_path):
     out = tmp_path / "empty.dat"
     pycusaxs_cuda.run(SyntheticTopology(s), "t", "x", [16], output=str(out))
     assert out.read_text() == ""
+
+
+def test_frames_beyond_one_batch_with_a_bad_frame_in_between(cuda, tmp_path, capsys):
+    # 40 frames of 2000 atoms fill more than one 32-frame pinned batch; frame 5's
+    # box is unusable, so it is reported and skipped (RunSaxs.cu:195-199) and
+    # the profile is that of the other 39 frames
+    s = cubic_system(2000, 30.0, seed=28, jitter=0.3, nframes=40)
+
+    class OneBadBox(SyntheticTopology):
+        def iter_frames_stream(self, start, stop, step=1, **kw):
+            for fr in super().iter_frames_stream(start, stop, step):
+                if fr["frame"] == 5:
+                    fr = dict(fr, box=np.zeros((3, 3), np.float32))
+                yield fr
+
+    out = tmp_path / "skip.dat"
+    pycusaxs_cuda.run(OneBadBox(s), "t", "x", [16], end=39, output=str(out), scale_factor=2.0,
+                      qcut=0.8)
+    assert "Error processing frame 5" in capsys.readouterr().err
+    frames = [s.frame(k) for k in range(40) if k != 5]
+    h, n, plan = oracle_hist(s, (16, 16, 16), frames, sigma=2.0, qcut=0.8)
+    want = O.profile_rows(h, n, plan.dq)
+    got = _read_rows(out)
+    assert [r[0] for r in got] == [f"{q:10.5f}" for q, _ in want]
+    for (_, gi), (_, wi) in zip(got, want):
+        assert abs(gi - wi) <= max(RTOL_PROFILE, 6e-6) * abs(wi)

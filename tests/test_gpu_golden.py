@@ -1,14 +1,16 @@
 """The drop-in run() against the reference's own output files (GPU).
 
 Same seeded inputs as tests/golden/make_golden.py fed to the reference
-cudaSAXS; the profile files must agree row by row: identical q text and
+cudaSAXS (small and large cases); the profile files must agree row by row: identical q text and
 intensities within GOLDEN_RTOL (the reference's FP32 noise and 6 printed
 significant digits on both sides).
 """
+import json
+
 import numpy as np
 import pytest
 
-from golden.make_golden import CASES, build_system
+from golden.make_golden import ALL_CASES, CASES, LARGE_OUT, build_system
 from test_golden import GOLDEN_RTOL, golden
 from pycusaxs_b200 import pycusaxs_cuda
 from pycusaxs_b200.synthetic import SyntheticTopology
@@ -16,16 +18,22 @@ from pycusaxs_b200.synthetic import SyntheticTopology
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("name", sorted(CASES))
+def _golden_rows(name):
+    if name in CASES:
+        return golden()[name]["rows"]
+    return json.loads(LARGE_OUT.read_text())[name]["rows"]
+
+
+@pytest.mark.parametrize("name", sorted(ALL_CASES))
 def test_dropin_file_matches_reference_file(cuda, tmp_path, name):
-    c = CASES[name]
+    c = ALL_CASES[name]
     out = tmp_path / f"{name}.dat"
     pycusaxs_cuda.run(SyntheticTopology(build_system(c)), "synthetic.tpr", "synthetic.xtc",
                       c["grid"], scaled_grid=c.get("scaled", []), begin=0, end=c["frames"] - 1,
                       stride=1, output=str(out), order=c.get("order", 4), scale_factor=c["sigma"],
                       bin_size=c["bin_size"], qcut=c["qcut"], simulation=c.get("simulation", ""))
     got = [(line[:10], float(line[10:])) for line in open(out)]
-    ref = golden()[name]["rows"]
+    ref = _golden_rows(name)
     assert [g[0] for g in got] == [r[0] for r in ref]
     gi = np.array([g[1] for g in got])
     ri = np.array([float(r[1]) for r in ref])

@@ -6,8 +6,12 @@ the allocator) run a frame through ``saxs_forward_noalloc`` with buffers they
 already own.  These tests call it through the C ABI twice in a row on two
 different frames and compare each result with the regular path
 (``saxs_forward`` + ``saxs_histogram`` on a reset plan): bin counts exactly,
-intensities within the suite's tolerance.  The file is named so that pytest
-collects it last; it also passes on its own in a fresh process.
+intensities within the suite's tolerance.  They also run it first on a fresh
+plan against the FP64 oracle, with the free device memory compared across that
+first call, and check that NaN positions give a NaN histogram (the call is
+asynchronous and has no other way to report a kernel's error).  The file is
+named so that pytest collects it last; it also passes on its own in a fresh
+process.
 """
 import ctypes
 
@@ -89,4 +93,46 @@ def test_oversized_plan_is_refused_with_a_clear_error(cuda):
     assert rc == _native.SAXS_E_RANGE
     msg = eng.lib.saxs_last_error().decode()
     assert "bytes of scratch" in msg and str(_native.SAXS_NOALLOC_SCRATCH_BYTES) in msg
+    eng.close()
+
+
+def test_first_call_on_a_fresh_plan_matches_the_oracle_and_allocates_nothing(cuda):
+    import torch
+
+    from helpers import assert_profiles_close, oracle_hist
+
+    s = cubic_system(20_000, 60.0, seed=43)
+    eng = SaxsEngine((64, 64, 64), s.atom_index(), s.natoms, s.box, scale_factor=2.0,
+                     bin_size=0.002, qcut=0.5, max_frames=1)
+    nb = eng.info.num_bins
+    hist_dev = torch.full((nb,), -1.0, dtype=torch.float64, device=eng.device)
+    nhist_dev = torch.full((nb,), -1.0, dtype=torch.float64, device=eng.device)
+    x = torch.from_numpy(s.positions).to(eng.device)
+    torch.cuda.synchronize()
+    free_before = torch.cuda.mem_get_info(eng.device)[0]
+    h, n = _noalloc(eng, x, s.box, hist_dev, nhist_dev)   # the plan's first frame
+    assert torch.cuda.mem_get_info(eng.device)[0] == free_before
+    ho, no, _ = oracle_hist(s, (64, 64, 64), [s.positions], sigma=2.0, bin_size=0.002, qcut=0.5)
+    assert_profiles_close(h, n, ho, no)
+    assert eng.frames == 0
+    eng.close()
+
+
+def test_nan_positions_give_a_nan_histogram(cuda):
+    import torch
+
+    s = cubic_system(5_000, 40.0, seed=44)
+    eng = SaxsEngine((32, 32, 32), s.atom_index(), s.natoms, s.box, scale_factor=2.0, qcut=0.6,
+                     max_frames=1)
+    nb = eng.info.num_bins
+    hist_dev = torch.zeros(nb, dtype=torch.float64, device=eng.device)
+    nhist_dev = torch.zeros(nb, dtype=torch.float64, device=eng.device)
+    bad = s.positions.copy()
+    bad[7, 1] = np.nan
+    h, n = _noalloc(eng, torch.from_numpy(bad).to(eng.device), s.box, hist_dev, nhist_dev)
+    assert np.isnan(h).all() and np.isnan(n).all()
+    # the next call, on good positions, is valid again; the plan's status is untouched
+    h, n = _noalloc(eng, torch.from_numpy(s.positions).to(eng.device), s.box, hist_dev, nhist_dev)
+    assert np.isfinite(h).all() and n.sum() > 0
+    assert eng.counters()["status"] == 0
     eng.close()
