@@ -452,22 +452,29 @@ def refinement(steps: int = 100) -> dict:
     dev = eng.device
     with torch.no_grad():
         target = saxs_profile(torch.tensor(moved, device=dev), eng, s.box)
-    sel = target > 0
+    # reported bins as an index tensor (a boolean mask would make every step
+    # wait for the device to count it)
+    idx = torch.nonzero(target > 0).squeeze(1)
+    log_target = torch.log(target.index_select(0, idx))
     x = torch.tensor(s.positions, device=dev, requires_grad=True)
 
     def loss_fn():
         prof = saxs_profile(x, eng, s.box)
-        return ((torch.log(prof[sel]) - torch.log(target[sel])) ** 2).sum()
+        return ((torch.log(prof.index_select(0, idx)) - log_target) ** 2).sum()
 
     def timed(fn, n):
+        """ms per call: CUDA events on the current stream around n calls that
+        never wait for the host."""
         for _ in range(3):
             fn()
         torch.cuda.synchronize()
-        t0 = time.perf_counter()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
         for _ in range(n):
             fn()
-        torch.cuda.synchronize()
-        return (time.perf_counter() - t0) * 1e3 / n
+        b.record()
+        b.synchronize()
+        return a.elapsed_time(b) / n
 
     def fwd():
         with torch.no_grad():
@@ -477,8 +484,8 @@ def refinement(steps: int = 100) -> dict:
         x.grad = None
         loss_fn().backward()
 
-    fwd_ms = timed(fwd, 10)
-    fb_ms = timed(fwd_bwd, 10)
+    fwd_ms = timed(fwd, 20)
+    fb_ms = timed(fwd_bwd, 20)
     opt = torch.optim.Adam([x], lr=3e-4)
     l0 = float(loss_fn().detach())
     torch.cuda.synchronize()
@@ -493,6 +500,7 @@ def refinement(steps: int = 100) -> dict:
     l1 = float(loss_fn().detach())
     eng.close()
     return {"workload": "50k atoms, 10 nm box, grid 128, scale 2 (256^3), log-profile loss",
+            "timing": "CUDA events on the current stream around 20 steps (no host waits inside)",
             "forward_ms": round(fwd_ms, 3), "forward_adjoint_ms": round(fb_ms, 3),
             "adjoint_over_forward": round(fb_ms / fwd_ms, 2),
             "adam_steps": steps, "adam_s": round(adam_s, 3), "loss_start": l0, "loss_end": l1}

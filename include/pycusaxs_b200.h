@@ -184,6 +184,16 @@ int saxs_debug_wait_probe(SaxsPlan *plan, double limit_seconds, void *stream);
 int saxs_backward(SaxsPlan *plan, const float *xyz_dev, const float *box_host,
                   const double *dl_dhist_host, float *grad_xyz_dev, void *stream);
 
+/* Device-resident forms for optimisation loops that must not wait for the host
+ * (no reference counterpart).  saxs_histogram_device enqueues on `stream` the
+ * accumulated FP64 histogram and counts into device buffers (num_bins each; nvt
+ * bins the intensity sum first) and returns without waiting; a kernel error is
+ * left in the status word for saxs_histogram / saxs_debug_counters to report.
+ * saxs_backward_device is saxs_backward with dL/dhist read from device memory. */
+int saxs_histogram_device(SaxsPlan *plan, double *hist_dev, double *nhist_dev, void *stream);
+int saxs_backward_device(SaxsPlan *plan, const float *xyz_dev, const float *box_host,
+                         const double *dl_dhist_dev, float *grad_xyz_dev, void *stream);
+
 /* ---- batched form: many systems and frames per CUDA graph launch (no counterpart
  * in the reference, which processes one frame of one system per call) ---- */
 
@@ -249,13 +259,14 @@ int saxs_profile_read(SaxsPlan *plan, double *ms_out, int *launches_out);
 /* ---- trajectory readers without MDAnalysis ----
  * The reference reads every frame through MDAnalysis (pycusaxs/topology.py:52-75
  * Universe(tpr, xtc), 536-577 read_frame/get_box, 621-737 iter_frames_stream),
- * converting GROMACS nanometres to Angstrom.  These read GROMACS TRR and
- * CHARMM/NAMD DCD files natively into caller buffers: positions (natoms x 3,
+ * converting GROMACS nanometres to Angstrom.  These read GROMACS TRR and XTC
+ * and CHARMM/NAMD DCD files natively into caller buffers: positions (natoms x 3,
  * Angstrom) and the box as three row vectors (Angstrom; zeros when the file has
  * no box).  Errors go to saxs_last_error(). */
-#define SAXS_TRAJ_AUTO 0 /* by file extension (.trr / .dcd) */
+#define SAXS_TRAJ_AUTO 0 /* by file extension (.trr / .dcd / .xtc) */
 #define SAXS_TRAJ_TRR 1
 #define SAXS_TRAJ_DCD 2
+#define SAXS_TRAJ_XTC 3 /* GROMACS compressed coordinates (xdr3dfcoord) */
 typedef struct SaxsTraj SaxsTraj;
 
 /* Open and index a trajectory (frame byte offsets, atom count). */

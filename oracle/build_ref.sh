@@ -13,10 +13,14 @@
 # compilation, --expt-relaxed-constexpr, --expt-extended-lambda, C++17; fmt is
 # the header-only copy that ships with torch.
 #
-# usage: oracle/build_ref.sh [reference-root]     (default /root/reference)
+# usage: oracle/build_ref.sh <reference-root>
 set -euo pipefail
 
-REF=${1:-/root/reference}
+if [ $# -lt 1 ]; then
+  echo "usage: oracle/build_ref.sh <reference-root>" >&2
+  exit 2
+fi
+REF=$1
 HERE=$(cd "$(dirname "$0")" && pwd)
 OUT="$HERE/_ref"
 SRC="$REF/cpp-src"

@@ -26,7 +26,7 @@ EXPORTED = (
     "saxs_plan_create", "saxs_plan_destroy", "saxs_plan_info", "saxs_plan_config",
     "saxs_plan_set_config", "saxs_forward", "saxs_histogram",
     "saxs_reset", "saxs_debug_kbox_intensity", "saxs_debug_border_sums", "saxs_debug_counters",
-    "saxs_debug_wait_probe", "saxs_backward",
+    "saxs_debug_wait_probe", "saxs_backward", "saxs_histogram_device", "saxs_backward_device",
     "saxs_graph_create", "saxs_graph_launch", "saxs_graph_destroy",
     "saxs_forward_noalloc", "saxs_profile_stages", "saxs_profile_stage_name", "saxs_profile_enable", "saxs_profile_read",
     "saxs_traj_open", "saxs_traj_info", "saxs_traj_read", "saxs_traj_close",
@@ -136,6 +136,10 @@ def load(path: os.PathLike | str | None = None) -> ctypes.CDLL:
     lib.saxs_debug_wait_probe.restype = ctypes.c_int
     lib.saxs_backward.argtypes = [vp, vp, c_float_p, c_double_p, vp, vp]
     lib.saxs_backward.restype = ctypes.c_int
+    lib.saxs_histogram_device.argtypes = [vp, vp, vp, vp]
+    lib.saxs_histogram_device.restype = ctypes.c_int
+    lib.saxs_backward_device.argtypes = [vp, vp, c_float_p, vp, vp, vp]
+    lib.saxs_backward_device.restype = ctypes.c_int
     lib.saxs_graph_create.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(vp),
                                       ctypes.POINTER(ctypes.c_int64), c_int_p, ctypes.c_int,
                                       ctypes.POINTER(vp)]

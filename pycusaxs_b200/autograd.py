@@ -3,13 +3,18 @@
 ``saxs_profile(xyz, engine, box)`` returns the frame's FP64 profile over all
 histogram bins (0 in bin 0 and in bins with no k-point, which the reference
 does not report).  Its backward is the hand-written adjoint of the CUDA path
-(``saxs_backward``): dL/dI(bin) is spread onto the k-points of each bin and
-their mirror partners, carried through the form factors, the complex type sum
-and |F|^2, taken back through the three pruned DFT passes with conjugated
+(``saxs_backward_device``): dL/dI(bin) is spread onto the k-points of each bin
+and their mirror partners, carried through the form factors, the complex type
+sum and |F|^2, taken back through the three pruned DFT passes with conjugated
 twiddles, through the z-border padding mean, and gathered at the atoms with the
 B-spline derivative weights.  The per-type grids are recomputed in the backward
-pass instead of being stored.  No reference counterpart: the reference has no
-derivative.
+pass instead of being stored.
+
+Forward and backward stay on the device: the histogram is read into device
+tensors and dL/dhist is handed over as one, so an optimisation loop never waits
+for the host.  A kernel error is left in the plan's status word; the next
+``engine.histogram()`` or ``engine.counters()`` reports it.  No reference
+counterpart: the reference has no derivative.
 """
 from __future__ import annotations
 
@@ -17,32 +22,39 @@ import numpy as np
 import torch
 
 
+def _profile_of(h, n):
+    prof = torch.where(n > 0, h / torch.where(n > 0, n, torch.ones_like(n)), torch.zeros_like(h))
+    prof[0] = 0.0
+    return prof
+
+
 class _SaxsProfile(torch.autograd.Function):
     @staticmethod
     def forward(ctx, xyz, engine, box):
         x = xyz.detach().to(engine.device, torch.float32).contiguous()
+        cur = torch.cuda.current_stream(engine.device)
+        engine.stream.wait_stream(cur)
         engine.reset()
         engine.forward(x, box)
-        h, n = engine.histogram()
+        h, n = engine.histogram_device()
         engine.reset()
-        prof = np.where(n > 0, h / np.where(n > 0, n, 1.0), 0.0)
-        prof[0] = 0.0
+        x.record_stream(engine.stream)
         ctx.engine = engine
         ctx.nhist = n
         ctx.box = np.asarray(box, dtype=np.float32)
         ctx.save_for_backward(xyz)
-        return torch.from_numpy(prof).to(xyz.device)
+        return _profile_of(h, n).to(xyz.device)
 
     @staticmethod
     def backward(ctx, grad_out):
         (xyz,) = ctx.saved_tensors
-        dprof = grad_out.detach().to(torch.float64).cpu().numpy()
+        eng = ctx.engine
         n = ctx.nhist
-        dl = np.where(n > 0, dprof / np.where(n > 0, n, 1.0), 0.0)
+        g = grad_out.detach().to(eng.device, torch.float64)
+        dl = torch.where(n > 0, g / torch.where(n > 0, n, torch.ones_like(n)), torch.zeros_like(g))
         dl[0] = 0.0
-        g = ctx.engine.backward(xyz.detach().to(ctx.engine.device, torch.float32).contiguous(),
-                                ctx.box, dl)
-        return g.to(device=xyz.device, dtype=xyz.dtype), None, None
+        grad = eng.backward_device(xyz.detach().to(eng.device, torch.float32).contiguous(), ctx.box, dl)
+        return grad.to(device=xyz.device, dtype=xyz.dtype), None, None
 
 
 def saxs_profile(xyz: torch.Tensor, engine, box) -> torch.Tensor:

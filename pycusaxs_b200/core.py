@@ -85,12 +85,12 @@ def invoke_cuda_backend(required_params: Dict[str, Any], advanced_params: Dict[s
 
 # topology / trajectory formats read without MDAnalysis (pycusaxs_b200.trajectory)
 NATIVE_TOPOLOGY = (".gro", ".pdb")
-NATIVE_TRAJECTORY = (".trr", ".dcd", ".gro")
+NATIVE_TRAJECTORY = (".xtc", ".trr", ".dcd", ".gro")
 
 
 def _default_topology_factory(topology_path: str, trajectory_path: str):
-    """GRO/PDB topology with a TRR/DCD/GRO trajectory: the native readers; anything
-    else (TPR, XTC, ...): the reference's MDAnalysis-backed Topology."""
+    """GRO/PDB topology with an XTC/TRR/DCD/GRO trajectory: the native readers;
+    anything else (a TPR topology, ...): the reference's MDAnalysis-backed Topology."""
     if (Path(topology_path).suffix.lower() in NATIVE_TOPOLOGY
             and Path(trajectory_path).suffix.lower() in NATIVE_TRAJECTORY):
         from .trajectory import FileTopology

@@ -1502,6 +1502,30 @@ int histogram(SaxsPlan *pl, double *hist, double *nhist, cudaStream_t st) {
 }
 
 
+// The accumulated histogram into device buffers, enqueued on `st` without a
+// wait: npt copies the FP64 accumulators, nvt bins the intensity sum with the
+// first frame's box.  The status word is left for saxs_histogram /
+// saxs_debug_counters to report.
+int histogram_device(SaxsPlan *pl, double *hist, double *nhist, cudaStream_t st) {
+  if (!pl || !hist || !nhist) return fail(SAXS_E_INVALID, "null argument");
+  const DevArgs &a = pl->a;
+  const size_t nb = static_cast<size_t>(a.num_bins);
+  if (pl->ensemble == SAXS_NVT) {
+    CUDA_TRY(cudaMemsetAsync(hist, 0, nb * sizeof(double), st));
+    CUDA_TRY(cudaMemsetAsync(nhist, 0, nb * sizeof(double), st));
+    if (pl->frames > 0) {
+      const float fact = static_cast<float>(1.0 / static_cast<float>(pl->frames));
+      k_hist<double><<<dim3(a.nkz, 1), kThreads, pl->smem_hist, st>>>(a, a.iacc, pl->d_geom0, kGeom,
+                                                                     static_cast<double>(fact), hist, nhist);
+      if (int rc = launch_check("k_hist(nvt)")) return rc;
+    }
+  } else {
+    CUDA_TRY(cudaMemcpyAsync(hist, a.hist, nb * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(nhist, a.nhist, nb * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  }
+  return SAXS_OK;
+}
+
 int ensure_adjoint(SaxsPlan *pl) {
   if (pl->d_adj_G) return SAXS_OK;
   const DevArgs &a = pl->a;
@@ -1549,7 +1573,7 @@ int ensure_adjoint(SaxsPlan *pl) {
 }
 
 int backward(SaxsPlan *pl, const float *xyz, const float *box, const double *dl, float *grad,
-             cudaStream_t st) {
+             cudaStream_t st, bool dl_on_device) {
   if (!pl || !box || !dl || !grad || (!xyz && pl->a.M > 0)) return fail(SAXS_E_INVALID, "null argument");
   if (int rc = fit_kbox(pl, box, 1, st, true)) return rc;
   if (int rc = ensure_adjoint(pl)) return rc;
@@ -1579,7 +1603,8 @@ int backward(SaxsPlan *pl, const float *xyz, const float *box, const double *dl,
   CUDA_TRY(cudaMemcpyAsync(const_cast<float *>(a.geom), g, sizeof(float) * kGeom,
                            cudaMemcpyHostToDevice, st));
   CUDA_TRY(cudaEventRecord(ring.ev[slot], st));
-  CUDA_TRY(cudaMemcpyAsync(pl->d_adj_dl, dl, sizeof(double) * a.num_bins, cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaMemcpyAsync(pl->d_adj_dl, dl, sizeof(double) * a.num_bins,
+                           dl_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
   CUDA_TRY(cudaMemsetAsync(pl->d_adj_S, 0, sizeof(double) * a.T, st));
   CUDA_TRY(cudaMemsetAsync(grad, 0, sizeof(float) * 3 * static_cast<size_t>(pl->p.natoms), st));
   // recompute the frame's y-transformed planes (nothing is kept from the forward)
@@ -1871,7 +1896,29 @@ int saxs_backward(SaxsPlan *plan, const float *xyz_dev, const float *box_host,
   cudaGetDevice(&prev);
   if (plan && prev != plan->device) cudaSetDevice(plan->device);
   const int rc = backward(plan, xyz_dev, box_host, dl_dprofile_host, grad_xyz_dev,
-                          static_cast<cudaStream_t>(stream));
+                          static_cast<cudaStream_t>(stream), false);
+  if (plan && prev != plan->device) cudaSetDevice(prev);
+  return rc;
+}
+
+int saxs_histogram_device(SaxsPlan *plan, double *hist_dev, double *nhist_dev, void *stream) {
+  g_err.clear();
+  int prev = 0;
+  cudaGetDevice(&prev);
+  if (plan && prev != plan->device) cudaSetDevice(plan->device);
+  const int rc = histogram_device(plan, hist_dev, nhist_dev, static_cast<cudaStream_t>(stream));
+  if (plan && prev != plan->device) cudaSetDevice(prev);
+  return rc;
+}
+
+int saxs_backward_device(SaxsPlan *plan, const float *xyz_dev, const float *box_host,
+                         const double *dl_dhist_dev, float *grad_xyz_dev, void *stream) {
+  g_err.clear();
+  int prev = 0;
+  cudaGetDevice(&prev);
+  if (plan && prev != plan->device) cudaSetDevice(plan->device);
+  const int rc = backward(plan, xyz_dev, box_host, dl_dhist_dev, grad_xyz_dev,
+                          static_cast<cudaStream_t>(stream), true);
   if (plan && prev != plan->device) cudaSetDevice(prev);
   return rc;
 }

@@ -6,7 +6,7 @@ The reference evaluates atomic form factors from a 9-coefficient table
 same coefficients, so this script parses that table as text and writes it as
 JSON; it is run once, by hand, where the reference sources are available:
 
-    python pycusaxs_b200/data/extract_form_factors.py /root/reference
+    python pycusaxs_b200/data/extract_form_factors.py <reference-root>
 
 The JSON maps element symbol -> [a1, a2, a3, a4, b1, b2, b3, b4, c] and keeps
 the reference's key order.  Values are kept as the decimal strings of the
@@ -42,7 +42,10 @@ def parse(text: str) -> dict[str, list[str]]:
 
 
 def main(argv: list[str]) -> int:
-    root = Path(argv[1] if len(argv) > 1 else "/root/reference")
+    if len(argv) < 2:
+        print("usage: extract_form_factors.py <reference-root>", file=sys.stderr)
+        return 2
+    root = Path(argv[1])
     src = root / "cpp-src" / "Utilities" / "Scattering.cpp"
     table = parse(src.read_text())
     dest = Path(__file__).with_name("it1992.json")

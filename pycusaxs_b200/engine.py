@@ -365,19 +365,24 @@ class SaxsEngine:
 
     # -- results ----------------------------------------------------------
     def run_trajectory(self, traj, begin: int = 0, end: int | None = None, stride: int = 1,
-                       batch: int | None = None) -> int:
+                       batch: int | None = None, shard: tuple | None = None) -> int:
         """Frames begin, begin+stride, ... < end of `traj` (a reader from
         pycusaxs_b200.trajectory: n_frames, n_atoms, read(k, out)) through the plan.
 
         A reader thread fills two pinned host batches of up to `batch` frames
         (default max_frames) while the previous batch is copied to the device and
-        processed; returns the number of frames processed.
+        processed; returns the number of frames processed.  ``shard=(rank,
+        world)`` keeps this rank's round-robin share of those frames (one
+        process per GPU; combine with pycusaxs_b200.distributed.sharded_histogram).
         """
+        from .distributed import shard as shard_frames
         from .trajectory import BatchStream
 
         torch = self._torch
         end = traj.n_frames if end is None else min(int(end), traj.n_frames)
         frames = range(max(0, int(begin)), end, max(1, int(stride)))
+        if shard is not None:
+            frames = shard_frames(frames, int(shard[0]), int(shard[1]))
         B = self.max_frames if batch is None else max(1, min(int(batch), self.max_frames))
         bufs = [torch.empty((B, traj.n_atoms, 3), dtype=torch.float32).pin_memory() for _ in range(2)]
         stream = BatchStream(traj, frames, B, bufs)
@@ -401,6 +406,23 @@ class SaxsEngine:
         _native.check(self.lib.saxs_histogram(self._plan, h.ctypes.data_as(_native.c_double_p),
                                               n.ctypes.data_as(_native.c_double_p),
                                               ctypes.c_void_p(self.stream.cuda_stream)))
+        return h, n
+
+    def histogram_device(self):
+        """(hist, nhist) as FP64 CUDA tensors, without waiting for the device:
+        ordered after the engine's queued work and before anything the caller's
+        current stream does next.  A kernel error stays in the plan's status
+        word (the next ``histogram()`` or ``counters()`` reports it)."""
+        torch = self._torch
+        nb = self.info.num_bins
+        cur = torch.cuda.current_stream(self.device)
+        h = torch.empty(nb, dtype=torch.float64, device=self.device)
+        n = torch.empty(nb, dtype=torch.float64, device=self.device)
+        self.stream.wait_stream(cur)
+        _native.check(self.lib.saxs_histogram_device(self._plan, ctypes.c_void_p(h.data_ptr()),
+                                                     ctypes.c_void_p(n.data_ptr()),
+                                                     ctypes.c_void_p(self.stream.cuda_stream)))
+        cur.wait_stream(self.stream)
         return h, n
 
     def profile(self):
@@ -465,11 +487,44 @@ class SaxsEngine:
         grad = torch.empty((x.shape[0], 3), dtype=torch.float32, device=self.device)
         if x.shape[0] > self.natoms:
             grad.zero_()
+        cur = torch.cuda.current_stream(self.device)
+        self.stream.wait_stream(cur)
         _native.check(self.lib.saxs_backward(
             self._plan, ctypes.c_void_p(x.data_ptr()), b.ctypes.data_as(_native.c_float_p),
             dl.ctypes.data_as(_native.c_double_p), ctypes.c_void_p(grad.data_ptr()),
             ctypes.c_void_p(self.stream.cuda_stream)))
-        torch.cuda.current_stream(self.device).wait_stream(self.stream)
+        cur.wait_stream(self.stream)
+        x.record_stream(self.stream)
+        return grad
+
+    def backward_device(self, xyz, box, dl_dhist):
+        """``backward`` with dL/dhist an FP64 CUDA tensor (num_bins,): nothing
+        waits for the host; the work is ordered after the caller's current
+        stream and before what it does next."""
+        torch = self._torch
+        x = xyz.detach()
+        if x.dim() == 3:
+            x = x[0]
+        if x.dtype != torch.float32 or x.device != self.device or not x.is_contiguous():
+            x = x.to(self.device, torch.float32).contiguous()
+        if x.shape[0] < self.natoms:
+            raise ValueError("xyz must have natoms rows")
+        dl = dl_dhist.detach().to(self.device, torch.float64).contiguous().reshape(-1)
+        if dl.numel() != self.info.num_bins:
+            raise ValueError(f"dl_dhist must have {self.info.num_bins} entries")
+        b = np.ascontiguousarray(np.asarray(box, dtype=np.float32).reshape(9))
+        grad = torch.empty((x.shape[0], 3), dtype=torch.float32, device=self.device)
+        if x.shape[0] > self.natoms:
+            grad.zero_()
+        cur = torch.cuda.current_stream(self.device)
+        self.stream.wait_stream(cur)
+        _native.check(self.lib.saxs_backward_device(
+            self._plan, ctypes.c_void_p(x.data_ptr()), b.ctypes.data_as(_native.c_float_p),
+            ctypes.c_void_p(dl.data_ptr()), ctypes.c_void_p(grad.data_ptr()),
+            ctypes.c_void_p(self.stream.cuda_stream)))
+        cur.wait_stream(self.stream)
+        for t in (x, dl):
+            t.record_stream(self.stream)
         return grad
 
     def profile_enable(self, on: bool = True) -> None:

@@ -5,8 +5,9 @@ The reference reads its topology and frames through MDAnalysis
 from ``atom.element``, 536-577 ``read_frame`` / ``get_box``, 621-737
 ``iter_frames_stream``).  This module replaces that with:
 
-* ``NativeTrajectory``: GROMACS TRR and CHARMM/NAMD DCD read by the library's
-  native readers (``saxs_traj_*``; ctypes releases the GIL during reads);
+* ``NativeTrajectory``: GROMACS TRR and XTC (compressed coordinates) and
+  CHARMM/NAMD DCD read by the library's native readers (``saxs_traj_*``;
+  ctypes releases the GIL during reads);
 * ``NpyTrajectory``: coordinates memory-mapped from a ``.npy`` file of shape
   (frames, natoms, 3) float32 Angstrom, boxes from a (3, 3) or (frames, 3, 3)
   array;
@@ -20,8 +21,8 @@ from ``atom.element``, 536-577 ``read_frame`` / ``get_box``, 621-737
   (``SaxsEngine.run_trajectory``).
 
 Units: Angstrom for positions and box rows, picoseconds for time, as the
-reference's frame dicts carry them.  GRO and TRR store nanometres and are
-converted.  Not read: XTC (compressed coordinates) and TPR (binary run input).
+reference's frame dicts carry them.  GRO, TRR and XTC store nanometres and are
+converted.  Not read: TPR (binary run input).
 """
 from __future__ import annotations
 
@@ -176,7 +177,7 @@ def read_pdb(path) -> dict:
 
 
 class NativeTrajectory:
-    """GROMACS TRR or CHARMM/NAMD DCD through the library's native readers."""
+    """GROMACS TRR or XTC, or CHARMM/NAMD DCD, through the library's native readers."""
 
     def __init__(self, path, fmt: int = 0):
         self.lib = _native.load()
@@ -239,9 +240,9 @@ class NpyTrajectory:
 
 
 def open_trajectory(path, box=None):
-    """A reader for `path` by extension: .trr/.dcd native, .gro text, .npy memory-mapped."""
+    """A reader for `path` by extension: .trr/.xtc/.dcd native, .gro text, .npy memory-mapped."""
     ext = Path(path).suffix.lower()
-    if ext in (".trr", ".dcd"):
+    if ext in (".trr", ".xtc", ".dcd"):
         return NativeTrajectory(path)
     if ext == ".gro":
         return GroTrajectory(path)
@@ -249,7 +250,7 @@ def open_trajectory(path, box=None):
         if box is None:
             raise ValueError("a .npy trajectory needs a box")
         return NpyTrajectory(path, box)
-    raise ValueError(f"unsupported trajectory format {ext!r} (supported: .trr .dcd .gro .npy)")
+    raise ValueError(f"unsupported trajectory format {ext!r} (supported: .trr .xtc .dcd .gro .npy)")
 
 
 def read_topology(path) -> dict:

@@ -91,6 +91,60 @@ def test_failed_rank_surfaces_as_error_not_hang(tmp_path):
     assert not (tmp_path / "r0.npy").exists()
 
 
+def _nvt_worker(rank, world, port, outdir):
+    sys.path.insert(0, str(REPO))
+    import torch.distributed as dist
+
+    from oracle import saxs_oracle as O
+    from pycusaxs_b200 import distributed as D
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=10))
+    try:
+        s = _system()
+        plan, names = _plan(s)
+        plan.ensemble = "nvt"
+        toa = s.type_of_atom(names)
+        mine = D.shard(D.frame_range(0, 4, 1), rank, world)   # 3 and 2 frames: uneven shares
+        # (1) each rank bins its own intensity sum, as its plan does, and the
+        # binned histograms are combined
+        h, n = O.run_frames(plan, [(s.frame(k), s.box) for k in mine], toa)
+        h, n = D.combine_histogram(h, n, len(mine), "nvt")
+        # (2) the raw intensity sums are reduced and binned once
+        total = sum(O.frame_intensity(plan, s.frame(k), toa, s.box)[0] for k in mine)
+        total, frames = D.reduce_intensity(total, len(mine))
+        _, bins0 = O.kpoint_bins(plan.nn, plan.scaled_oc(plan.oc0), plan.dq, plan.kcut,
+                                 plan.num_bins, plan.contraction)
+        h2, n2 = O.histogram(total, bins0, plan.num_bins, 1.0 / frames)
+        np.save(os.path.join(outdir, f"nvt{rank}.npy"), np.stack([h, n, h2, n2]))
+    except Exception as exc:
+        Path(outdir, f"err{rank}.txt").write_text(f"{type(exc).__name__}: {exc}")
+    finally:
+        try:
+            dist.destroy_process_group()
+        except Exception:
+            pass
+
+
+def test_sharded_nvt_equals_single_process(tmp_path):
+    from oracle import saxs_oracle as O
+
+    mp.start_processes(_nvt_worker, args=(2, _free_port(), str(tmp_path)), nprocs=2,
+                       start_method="spawn", join=True)
+    assert not list(tmp_path.glob("err*.txt")), [p.read_text() for p in tmp_path.glob("err*.txt")]
+    s = _system()
+    plan, names = _plan(s)
+    plan.ensemble = "nvt"
+    h, n = O.run_frames(plan, [(s.frame(k), s.box) for k in range(5)], s.type_of_atom(names))
+    for r in range(2):
+        hb, nb, hr, nr = np.load(tmp_path / f"nvt{r}.npy")
+        np.testing.assert_array_equal(nb, n)
+        np.testing.assert_allclose(hb, h, rtol=1e-12)
+        np.testing.assert_array_equal(nr, n)
+        np.testing.assert_allclose(hr, h, rtol=1e-12)
+
+
 def test_shard_is_a_partition():
     from pycusaxs_b200 import distributed as D
 

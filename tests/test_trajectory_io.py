@@ -1,5 +1,10 @@
-"""Frame ingestion without MDAnalysis (CPU): native TRR/DCD readers, GRO/PDB topologies,
-the FileTopology callback contract and the read-ahead streams."""
+"""Frame ingestion without MDAnalysis (CPU): native TRR/XTC/DCD readers, GRO/PDB topologies,
+the FileTopology callback contract and the read-ahead streams.
+
+The XTC reader is checked by round trips through the test-side compressor
+(tests/trajfiles.py): positions must equal the written integer coordinates
+times 1/precision, converted to Angstrom, bit for bit.  No file written by
+GROMACS exists here, so parity with GROMACS-written files is unpinned."""
 import numpy as np
 import pytest
 
@@ -7,7 +12,7 @@ from pycusaxs_b200 import _native
 from pycusaxs_b200.trajectory import (BatchStream, FileTopology, GroTrajectory, NativeTrajectory,
                                       NpyTrajectory, box_from_lengths, guess_element, read_gro,
                                       read_pdb)
-from trajfiles import write_dcd, write_gro, write_pdb, write_trr
+from trajfiles import write_dcd, write_gro, write_pdb, write_trr, write_xtc
 
 
 def _frames(F=5, N=7, seed=0):
@@ -79,7 +84,7 @@ def test_dcd_without_cell_and_short_file(tmp_path):
 
 
 def test_unknown_extension_is_refused(tmp_path):
-    p = tmp_path / "x.xtc"
+    p = tmp_path / "x.xyz"
     p.write_bytes(b"\x00" * 16)
     with pytest.raises(_native.SaxsError, match="unsupported trajectory format"):
         NativeTrajectory(p)
@@ -197,3 +202,66 @@ def test_batch_stream_refills_only_released_buffers(tmp_path):
         st.release(slot, None)
     st.close()
     np.testing.assert_allclose(np.stack(seen), (x * 10).astype(np.float32), rtol=1e-5)
+
+
+def _waters(nmol, box_nm, seed):
+    """Water-like triples (O then two H 0.1 nm away) spread over a box: the
+    pairs and runs the compressor takes apart."""
+    rng = np.random.default_rng(seed)
+    o = rng.uniform(0.0, box_nm, (nmol, 3))
+    h1 = o + rng.normal(0, 0.06, (nmol, 3))
+    h2 = o + rng.normal(0, 0.06, (nmol, 3))
+    return np.stack([o, h1, h2], axis=1).reshape(-1, 3)
+
+
+def _expected(ints, precision):
+    inv = np.float32(1.0 / np.float64(np.float32(precision)))
+    return (ints.astype(np.float32) * inv) * np.float32(10.0)
+
+
+@pytest.mark.parametrize("large", [False, True])
+@pytest.mark.parametrize("precision", [1000.0, 100.0])
+def test_xtc_roundtrip(tmp_path, large, precision):
+    frames = [_waters(700, 4.0, seed=k) for k in range(4)]
+    frames[2] = np.random.default_rng(9).uniform(-1.0, 4.0, (2100, 3))   # no neighbours: lone atoms
+    boxes = [np.diag([4.0, 4.1, 4.2]) for _ in range(4)]
+    boxes[1][1, 0] = 0.7
+    p = tmp_path / "w.xtc"
+    written = write_xtc(p, frames, boxes, [0.5 * k for k in range(4)], precision=precision,
+                        large=large, seed=3)
+    tr = NativeTrajectory(p)
+    assert (tr.n_atoms, tr.n_frames) == (2100, 4)
+    for k in (3, 0, 2, 1):
+        pos, box, t = tr.read(k)
+        np.testing.assert_array_equal(pos, _expected(written[k], precision))
+        np.testing.assert_array_equal(box, np.asarray(boxes[k], np.float32) * np.float32(10.0))
+        assert t == pytest.approx(0.5 * k)
+        # and the positions are the frame's to the written precision
+        np.testing.assert_allclose(pos, frames[k] * 10.0, atol=10.0 * 0.5 / precision * 1.001 + 1e-4)
+    tr.close()
+
+
+def test_xtc_small_frames_are_plain_floats(tmp_path):
+    x = [np.random.default_rng(1).uniform(0, 2, (5, 3)) for _ in range(2)]
+    p = tmp_path / "s.xtc"
+    write_xtc(p, x, [np.eye(3) * 2.0] * 2, [0.0, 1.0])
+    tr = NativeTrajectory(p)
+    pos, box, _ = tr.read(1)
+    np.testing.assert_array_equal(pos, np.asarray(x[1], np.float32) * np.float32(10.0))
+    tr.close()
+
+
+def test_xtc_corrupt_stream_is_an_error_not_a_crash(tmp_path):
+    frames = [_waters(400, 3.0, seed=5)]
+    p = tmp_path / "c.xtc"
+    write_xtc(p, frames, [np.eye(3) * 3.0], [0.0])
+    raw = bytearray(p.read_bytes())
+    # keep the header's byte count, zero the stream's second half: the decoder
+    # must stop at the end of the stream or at a run past the last atom
+    nbytes = int.from_bytes(raw[88:92], "big")
+    raw[92 + nbytes // 2: 92 + nbytes] = b"\xff" * (nbytes - nbytes // 2)
+    p.write_bytes(bytes(raw))
+    tr = NativeTrajectory(p)
+    with pytest.raises(_native.SaxsError):
+        tr.read(0)
+    tr.close()
