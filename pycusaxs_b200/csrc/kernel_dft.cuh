@@ -121,12 +121,40 @@ constexpr int kDtcMaxStages = 4;
 // columns).  A k step is then two MMAs, D += Ah [Bh|Bl] and D += Al [Bh|Bl] (a
 // tf32 MMA costs about the same up to N = 192), instead of three; the epilogue
 // adds the two halves of D.
+//
+// With `f16` the pass runs in f16 instead of 3xTF32: the producers scale A by
+// a power of two per type (dtc_f16_scale), split it into an f16 head and the
+// rounded f16 remainder (both in tensor memory, two K values per column, the
+// even one in the low half: 16 columns each per chunk), B' holds the twiddles'
+// f16 head and remainder, and the MMAs are kind::f16 with K = 16, so a chunk
+// (K' = 32) takes two k steps instead of four.  With `side` the two halves of B'
+// sit side by side ([Bh | Bl], N = 2N') and a k step is two MMAs, D += Ah B' and
+// D += Al B', whose halves the epilogue adds; otherwise three, D += Al Bh + Ah Bl
+// + Ah Bh.  Head and remainder keep 22 bits of each operand, the precision of
+// 3xTF32, and an MMA costs about the same either way, so f16 halves the y and x
+// passes' MMA issue (which bounds them).
 struct DtcShape {
   int N, chunks, S, cols;
   int lo_smem;
+  int f16, side;
   const float *B;  // [chunk]: head block then remainder block (N' x 2*kDtcChunk
-                   // each), or one block of 2N' x 2*kDtcChunk with lo_smem
+                   // each), or one block of 2N' x 2*kDtcChunk with lo_smem or
+                   // side (f16: the same blocks in halves, packed two per float)
 };
+
+// Power-of-two scale of type t's rows in an f16 pass, from bounds that need no
+// look at the data: a z-transformed column |Z| <= M_t + ez * mean_t (the type's
+// M_t atoms carry weight 1 each; the average padding mean is at most M_t over
+// the nx * ny voxels of a border plane), a y-transformed row |Y| <= ey * max|Z|.
+// The scaled values stay below 2^14, well inside f16's range.
+__device__ __forceinline__ float dtc_f16_scale(const DevArgs &a, int t, bool x_pass) {
+  const float m = static_cast<float>(a.type_start[t + 1] - a.type_start[t]);
+  const float pad = a.pad_val ? a.pad_val[t] * static_cast<float>(a.ext[2])
+                              : m * static_cast<float>(a.ext[2]) / (static_cast<float>(a.n[0]) * a.n[1]);
+  float bound = m + pad + 1.0f;
+  if (x_pass) bound *= static_cast<float>(a.ext[1]);
+  return exp2f(14.0f - ceilf(log2f(bound)));
+}
 
 // Tensor copy of chunk c of item w's 128 rows into `dst`, 1024-byte aligned
 // (128-byte swizzle: the 16-byte piece j of row r lands at piece j ^ (r % 8) of
@@ -181,10 +209,13 @@ __global__ void __launch_bounds__(dtc_threads<kX>(), 1)
   __shared__ uint32_t tmem_slot;
   __shared__ volatile int abort_flag;
   const int N = sh.N, NS = sh.S, NC = sh.chunks;
-  const int NM = sh.lo_smem ? 2 * N : N;             // MMA N, accumulator stage width
-  const int AW = sh.lo_smem ? 32 : 64;               // tensor-memory columns of an A stage
+  const bool F16 = sh.f16 != 0;
+  const bool halves = F16 ? sh.side != 0 : sh.lo_smem != 0;  // B' = [Bh | Bl]: D in two halves
+  const int NM = halves ? 2 * N : N;                 // MMA N, accumulator stage width
+  const int AW = (F16 || sh.lo_smem) ? 32 : 64;      // tensor-memory columns of an A stage
   const int KP = 2 * kDtcChunk;                      // K' per chunk
-  const int a_floats = 128 * KP, b_floats = N * KP;  // raw A tile; B' head or remainder
+  const int a_floats = 128 * KP;                     // raw A tile
+  const int b_floats = F16 ? N * KP / 2 : N * KP;    // B' head or remainder (f16: halves)
   const int stage_floats = a_floats + 2 * b_floats;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   // swizzled tensor copies need a 1024-byte aligned destination: the stages
@@ -236,12 +267,52 @@ __global__ void __launch_bounds__(dtc_threads<kX>(), 1)
     const uint32_t lane_off = static_cast<uint32_t>(32 * quarter) << 16;
     int g = 0;
     for (int w = blockIdx.x; w < items; w += gridDim.x) {
+      // f16: this row's scale (y pass: the item's type; x pass: row r's type)
+      float rs = 1.0f;
+      if (F16) {
+        const int xblocks = (a.ext[0] + 127) / 128;
+        const int t = kX ? r % a.T : (w / xblocks / a.nkz) % a.T;
+        rs = dtc_f16_scale(a, t, kX);
+      }
       for (int c = 0; c < NC; ++c, ++g) {
         const int st = g % NS;
         if (g >= NS) wait(&empty[st], g / NS - 1);  // the stage's MMAs have read its TMEM columns
         wait(&bfull[st], g / NS);
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         float *raw = stages + static_cast<size_t>(st) * stage_floats;
+        if (F16) {
+          // K' 16*half .. +15 of row r: scaled, f16 head and rounded remainder,
+          // two K values per column (the even one low), head then remainder
+          uint32_t hi[8], lo[8];
+#pragma unroll
+          for (int jj = 0; jj < 4; ++jj) {
+            const int j = 4 * half + jj;
+            const float4 v = *reinterpret_cast<const float4 *>(raw + r * KP + 4 * (j ^ (r & 7)));
+            const float vv[4] = {v.x * rs, v.y * rs, v.z * rs, v.w * rs};
+#pragma unroll
+            for (int e = 0; e < 4; e += 2) {
+              const __half2 hh = __floats2half2_rn(vv[e], vv[e + 1]);
+              const float2 hf = __half22float2(hh);
+              const __half2 ll = __floats2half2_rn(vv[e] - hf.x, vv[e + 1] - hf.y);
+              hi[2 * jj + e / 2] = *reinterpret_cast<const uint32_t *>(&hh);
+              lo[2 * jj + e / 2] = *reinterpret_cast<const uint32_t *>(&ll);
+            }
+          }
+          const uint32_t col = tmem + lane_off + static_cast<uint32_t>(2 * NM + AW * st + 8 * half);
+          asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"r"(col),
+                       "r"(hi[0]), "r"(hi[1]), "r"(hi[2]), "r"(hi[3]), "r"(hi[4]), "r"(hi[5]), "r"(hi[6]),
+                       "r"(hi[7])
+                       : "memory");
+          asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"r"(col + 16),
+                       "r"(lo[0]), "r"(lo[1]), "r"(lo[2]), "r"(lo[3]), "r"(lo[4]), "r"(lo[5]), "r"(lo[6]),
+                       "r"(lo[7])
+                       : "memory");
+          asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+          asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+          __syncwarp();
+          if (lane == 0) mbar_arrive(smem_addr(&afull[st]));
+          continue;
+        }
         uint32_t hi[16], lo[16];
 #pragma unroll
         for (int jj = 0; jj < 4; ++jj) {
@@ -323,7 +394,22 @@ __global__ void __launch_bounds__(dtc_threads<kX>(), 1)
           asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
           const float *sb = stages + static_cast<size_t>(st) * stage_floats;
           const uint32_t ah0 = tmem + static_cast<uint32_t>(2 * NM + AW * st);
-          if (sh.lo_smem) {
+          if (F16) {
+            // kind::f16 (f16 A and B), D f32, N = NM, M = 128; B' K-major, 16-byte
+            // K blocks of N2 rows; a k step of 16 K advances two blocks
+            const uint32_t idesc16 = (1u << 4) | (static_cast<uint32_t>(NM >> 3) << 17) |
+                                     (static_cast<uint32_t>(128 >> 4) << 24);
+            const int N2 = sh.side ? 2 * N : N;
+            const uint64_t dbh0 = umma_desc(smem_addr(sb + a_floats), N2 * 16, 128);
+            const uint64_t dbl0 = umma_desc(smem_addr(sb + a_floats + b_floats), N * 16, 128);
+            for (int kk = 0; kk < KP / 16; ++kk) {
+              const uint32_t ah = ah0 + 8 * kk, al = ah + 16;
+              const uint64_t dbh = dbh0 + static_cast<uint64_t>(kk * 2 * N2);
+              umma_f16_ts(dcol, al, dbh, idesc16, (c > 0 || kk > 0) ? 1u : 0u);
+              if (!sh.side) umma_f16_ts(dcol, ah, dbl0 + static_cast<uint64_t>(kk * 2 * N), idesc16, 1u);
+              umma_f16_ts(dcol, ah, dbh, idesc16, 1u);
+            }
+          } else if (sh.lo_smem) {
             // B' = [Bh | Bl] (2N' columns); Al is the swizzled tile itself: a K-major
             // SWIZZLE_128B descriptor (layout type 2, 8-row groups 1024 B apart) whose
             // start advances 32 B per k step of 8 floats within the 128-byte rows
@@ -377,6 +463,13 @@ __global__ void __launch_bounds__(dtc_threads<kX>(), 1)
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const uint32_t lane_base = tmem + (static_cast<uint32_t>(32 * quarter) << 16) + static_cast<uint32_t>(d * NM);
       // 16 accumulator columns from c0 (with lo_smem: the sum of the two halves)
+      // f16: the row's scale is undone here (y pass: the item's type; x pass: row r's)
+      float unscale = 1.0f;
+      if (F16) {
+        const int xblocks = (a.ext[0] + 127) / 128;
+        const int t = kX ? r % a.T : (w / xblocks / a.nkz) % a.T;
+        unscale = 1.0f / dtc_f16_scale(a, t, kX);
+      }
       auto load16 = [&](int c0, uint32_t v[16]) {
         asm volatile(
             "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
@@ -384,7 +477,7 @@ __global__ void __launch_bounds__(dtc_threads<kX>(), 1)
             : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
               "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
             : "r"(lane_base + c0));
-        if (sh.lo_smem) {
+        if (halves) {
           uint32_t u[16];
           asm volatile(
               "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
@@ -397,6 +490,10 @@ __global__ void __launch_bounds__(dtc_threads<kX>(), 1)
           for (int q = 0; q < 16; ++q) v[q] = __float_as_uint(__uint_as_float(v[q]) + __uint_as_float(u[q]));
         } else {
           asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        }
+        if (F16) {
+#pragma unroll
+          for (int q = 0; q < 16; ++q) v[q] = __float_as_uint(__uint_as_float(v[q]) * unscale);
         }
       };
       if (!kX) {

@@ -295,6 +295,31 @@ bool dtc_shape(int nk, int extent, size_t avail, DtcShape *sh, size_t *smem, boo
   // then reads twice the accumulator columns, 0.34 against 0.33 ms, so it keeps
   // the first form.
   const char *mode = std::getenv("PYCUSAXS_DTC");
+  sh->f16 = sh->side = 0;
+  // f16 (the default; PYCUSAXS_DTC=tf32 or =split keep 3xTF32): per stage the
+  // raw A tile and B' in halves; tensor memory: two accumulators of 2N' columns
+  // ([Bh | Bl] side by side) or of N' columns, and 32 columns per stage
+  if (!(mode && (std::strcmp(mode, "tf32") == 0 || std::strcmp(mode, "split") == 0))) {
+    const size_t stage16 = (128 * sizeof(float) + 2 * static_cast<size_t>(N) * sizeof(uint16_t)) * 2 * kDtcChunk;
+    const int S16 = static_cast<int>((avail - 1024) / stage16);
+    int S = std::min({kDtcMaxStages, S16, (512 - 4 * N) / 32});
+    int side = 1;
+    if (S < 2 || 2 * N > 256) {
+      S = std::min({kDtcMaxStages, S16, (512 - 2 * N) / 32});
+      side = 0;
+    }
+    if (S >= 2 && N <= 256) {
+      sh->f16 = 1;
+      sh->side = side;
+      sh->lo_smem = 0;
+      sh->N = N;
+      sh->chunks = (extent + kDtcChunk - 1) / kDtcChunk;
+      sh->S = S;
+      sh->cols = 512;
+      *smem = S * stage16 + 1024;
+      return true;
+    }
+  }
   int S = std::min({kDtcMaxStages, S_smem, (512 - 2 * N) / 64});
   sh->lo_smem = 0;
   if (allow_lo_smem && !(mode && std::strcmp(mode, "split") == 0) && 2 * N <= 256) {
@@ -350,6 +375,43 @@ std::vector<float> dtc_bprime(const std::vector<float2> &tw, int stride, int ext
       }
     }
   return out;
+}
+
+// The same B' for an f16 pass: head = the twiddle rounded to f16, remainder =
+// the rounded difference, in K-major blocks of 16-byte K groups (element (n',
+// k') at half ((k' / 8) * N2 + n') * 8 + k' % 8, N2 the block's columns), head
+// and remainder side by side (one block of 2N' columns) or one after the other;
+// packed two halves per float.
+std::vector<float> dtc_bprime16(const std::vector<float2> &tw, int stride, int extent, int nk,
+                                const DtcShape &sh) {
+  const int KP = 2 * kDtcChunk, Np = sh.N, N2 = sh.side ? 2 * Np : Np;
+  const size_t blk = static_cast<size_t>(Np) * KP;  // halves of a head or remainder block
+  std::vector<__half> out(static_cast<size_t>(sh.chunks) * 2 * blk, __float2half_rn(0.0f));
+  auto at = [&](int c, int part, int np, int kp) {
+    const int n2 = sh.side ? np + part * Np : np;
+    const size_t off = static_cast<size_t>(c) * 2 * blk + (sh.side ? 0 : part * blk);
+    return off + (static_cast<size_t>(kp / 8) * N2 + n2) * 8 + kp % 8;
+  };
+  for (int c = 0; c < sh.chunks; ++c)
+    for (int uu = 0; uu < kDtcChunk; ++uu) {
+      const int u = c * kDtcChunk + uu;
+      if (u >= extent) continue;
+      for (int k = 0; k < nk; ++k) {
+        const float2 w = tw[static_cast<size_t>(u) * stride + k];
+        const float vals[2][2] = {{w.x, w.y}, {-w.y, w.x}};
+        for (int cz = 0; cz < 2; ++cz)
+          for (int d = 0; d < 2; ++d) {
+            const int kp = 2 * uu + cz, np = 2 * k + d;
+            const float v = vals[cz][d];
+            const __half h = __float2half_rn(v);
+            out[at(c, 0, np, kp)] = h;
+            out[at(c, 1, np, kp)] = __float2half_rn(v - __half2float(h));
+          }
+      }
+    }
+  std::vector<float> packed(out.size() / 2);
+  std::memcpy(packed.data(), out.data(), packed.size() * sizeof(float));
+  return packed;
 }
 
 // `min_half`, when given, is the smallest k-box half-width per axis the plan
@@ -819,10 +881,11 @@ int create(const SaxsParams *prm, SaxsPlan **out, const long long *min_half = nu
   for (int x = 0; x < ex; ++x)
     for (int k = 0; k < a.nkx; ++k)
       saxs::twiddle(a.kx_lo + k, x, nn[0], &twx[x * a.nkxp + k].x, &twx[x * a.nkxp + k].y);
-  const std::vector<float> twytc =
-      pl->use_ytc ? dtc_bprime(twy, a.nkyp, ey, a.nky, pl->yshape) : std::vector<float>();
-  const std::vector<float> twxtc =
-      pl->use_xtc ? dtc_bprime(twx, a.nkxp, ex, a.nkx, pl->xshape) : std::vector<float>();
+  auto bprime = [&](const std::vector<float2> &tw, int stride, int extent, int nk, const DtcShape &sh) {
+    return sh.f16 ? dtc_bprime16(tw, stride, extent, nk, sh) : dtc_bprime(tw, stride, extent, nk, sh);
+  };
+  const std::vector<float> twytc = pl->use_ytc ? bprime(twy, a.nkyp, ey, a.nky, pl->yshape) : std::vector<float>();
+  const std::vector<float> twxtc = pl->use_xtc ? bprime(twx, a.nkxp, ex, a.nkx, pl->xshape) : std::vector<float>();
   const int ndim = std::max(nn[0], std::max(nn[1], nn[2]));
   std::vector<float> mx(nn[0]), my(nn[1]), mz(nn[2]);
   saxs::bspline_moduli(nn[0], ndim, mx.data());

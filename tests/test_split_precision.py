@@ -53,3 +53,60 @@ def test_f16_split_matches_3xtf32_precision():
     e32 = np.abs(z32 - exact).max() / top
     assert e16 < 5e-7 and e32 < 5e-7, (e16, e32)
     assert e16 <= 1.2 * e32, (e16, e32)
+
+
+def _f16_scale(m_t, ez, nx, ny, ey=None):
+    """The kernels' power-of-two row scale of an f16 y (ey None) or x pass
+    (dtc_f16_scale): bound = M_t + ez * M_t / (nx * ny) + 1, times ey for x."""
+    bound = np.float32(m_t + m_t * ez / (nx * ny) + 1.0)
+    if ey is not None:
+        bound *= np.float32(ey)
+    return np.float32(2.0 ** (14 - np.ceil(np.log2(bound))))
+
+
+def _complex_gemm_operands(rows, extent, nk, nn, rng, amp):
+    z = (rng.normal(0, amp, (rows, extent)) + 1j * rng.normal(0, amp, (rows, extent)))
+    z[rng.random((rows, extent)) < 0.01] *= 50.0   # a few large columns
+    u = np.arange(extent)
+    k = np.arange(-(nk // 2), nk // 2 + 1)
+    w = np.exp(-2j * np.pi * np.outer(u, k) / nn)
+    a = np.stack([z.real, z.imag], axis=2).reshape(rows, 2 * extent)           # [r][2u + c]
+    b = np.zeros((2 * extent, 2 * len(k)))                                    # {Wr, Wi; -Wi, Wr}
+    b[0::2, 0::2], b[0::2, 1::2] = w.real, w.imag
+    b[1::2, 0::2], b[1::2, 1::2] = -w.imag, w.real
+    return a, b
+
+
+def _split16(x):
+    h = x.astype(np.float16)
+    return h, (x - h.astype(np.float32)).astype(np.float16)
+
+
+def test_f16_y_and_x_passes_match_3xtf32_precision():
+    rng = np.random.default_rng(4)
+    m_t = 60_000
+    for name, ey, amp in (("y", None, 3.0), ("x", 128, 300.0)):
+        a, b = _complex_gemm_operands(128, 128, 41, 256, rng, amp)
+        exact = a @ b
+        s = _f16_scale(m_t, 128, 128, 128, ey)
+        a32 = _f32(a * s)
+        assert np.abs(a32).max() < 2.0 ** 14
+        ah, al = _split16(a32)
+        bh, bl = _split16(_f32(b))
+        f = lambda x: _f32(x)  # noqa: E731
+        side = (f(ah) @ f(bh) + f(ah) @ f(bl)) + (f(al) @ f(bh) + f(al) @ f(bl))   # [Bh | Bl]
+        three = f(al) @ f(bh) + f(ah) @ f(bl) + f(ah) @ f(bh)                   # separate blocks
+        d_side = side.astype(np.float64) / s
+        d_three = three.astype(np.float64) / s
+        a2h = _tf32(_f32(a))
+        a2l = _tf32(_f32(_f32(a) - a2h))
+        b2h = _tf32(_f32(b))
+        b2l = _tf32(_f32(_f32(b) - b2h))
+        d32 = (a2h @ b2h + a2h @ b2l + a2l @ b2h).astype(np.float64)
+        top = np.abs(exact).max()
+        e_side = np.abs(d_side - exact).max() / top
+        e_three = np.abs(d_three - exact).max() / top
+        e32 = np.abs(d32 - exact).max() / top
+        # (K' = 256 terms accumulated in FP32 bound all three forms near 1e-6)
+        assert e_side < 2e-6 and e_three < 2e-6, (name, e_side, e_three, e32)
+        assert max(e_side, e_three) <= 1.5 * e32 + 1e-8, (name, e_side, e_three, e32)
