@@ -319,8 +319,8 @@ def bench_ours(args):
     # the kernel that ran for each stage: plan path bits 0/1/2 = z/y/x DFT on tcgen05,
     # bit 3 = wide z tiles
     path = info.path
-    kernel_of = {"k_spread_zdft": ("k_spread_zdft_tcw" if path & 8 else "k_spread_zdft_tc") if path & 1
-                 else "k_spread_zdft",
+    kernel_of = {"k_spread_zdft": ("k_spread_zdft_ag" if path & 16 else "k_spread_zdft_tcw" if path & 8
+                                   else "k_spread_zdft_tc") if path & 1 else "k_spread_zdft",
                  "k_ydft": "k_dft_tc<y>" if path & 2 else "k_ydft",
                  "k_xdft_post": "k_dft_tc<x>" if path & 4 else "k_xdft_post"}
     tensor = bool({"k_spread_zdft": 1, "k_ydft": 2, "k_xdft_post": 4}.get(dom, 0) & path)
@@ -333,7 +333,11 @@ def bench_ours(args):
                 "peak_source": "measured" if peaks else "fallback"}
     if dom in algo_flops:
         useful = algo_flops[dom] * frames_per_launch / per_launch_s / 1e12
-        if tensor and dom == "k_spread_zdft" and path & 8:
+        if tensor and dom == "k_spread_zdft" and path & 16:
+            # atom GEMM: the tensor cores also do the spreading (K = reaching atoms), so
+            # the dense z-DFT FLOP count is no measure of their work
+            roofline["tensor"] = {"mma_kind": "f16", "note": "spreading and z DFT as one GEMM over atoms"}
+        elif tensor and dom == "k_spread_zdft" and path & 8:
             # wide z kernel: f16 head/remainder of both operands, two kind::f16 MMAs per
             # 16 z against [Bh | Bl], so four f16 products issued per useful one; the
             # dense f16 rate equals the bf16 one

@@ -90,7 +90,8 @@ typedef struct SaxsPlanInfo {
   int kbox[3];          /* k-points evaluated per axis (x, y: signed range; z: 0..)*/
   int kz_count;
   int path;             /* pruned separable DFT; bits 0, 1, 2: z-, y-, x-axis DFT   */
-                        /* on tcgen05 (3xTF32); a clear bit: that pass in FP32 SIMT */
+                        /* on tcgen05; a clear bit: that pass in FP32 SIMT; bit 3:  */
+                        /* 128-column z tiles, bit 4: the atom-GEMM z pass          */
   size_t device_bytes;  /* device memory held by the plan                          */
   int frames_accumulated;
 } SaxsPlanInfo;
@@ -124,6 +125,10 @@ typedef struct SaxsPlanConfig {
   int z_narrow_tiles_available, z_wide_tiles_available;
   int z_producer_groups_max;       /* 64-column tiles  */
   int z_wide_producer_groups_max;  /* 128-column tiles */
+  int z_atom_gemm;        /* 1: spreading + z-axis DFT as one tensor-core GEMM over the
+                             atoms (128-column tiles, k_spread_zdft_ag); with it the
+                             z_wide_tiles and z_producer_groups fields are not used   */
+  int z_atom_gemm_available;  /* read by saxs_plan_config only                          */
 } SaxsPlanConfig;
 
 int saxs_plan_config(const SaxsPlan *plan, SaxsPlanConfig *cfg);

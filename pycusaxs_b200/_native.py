@@ -69,7 +69,7 @@ class SaxsPlanConfig(ctypes.Structure):
         "z_tensor_cores", "y_tensor_cores", "x_tensor_cores", "z_wide_tiles", "z_producer_groups",
         "z_tensor_cores_available", "y_tensor_cores_available", "x_tensor_cores_available",
         "z_narrow_tiles_available", "z_wide_tiles_available", "z_producer_groups_max",
-        "z_wide_producer_groups_max")]
+        "z_wide_producer_groups_max", "z_atom_gemm", "z_atom_gemm_available")]
 
 
 class SaxsPlanInfo(ctypes.Structure):

@@ -60,6 +60,9 @@ struct DevArgs {
   // wide-tile variant (k_spread_zdft_tcw): tile row stride (floats), record buffer,
   // atom table entries, producer groups; y tiles of 16 rows
   int twN, twRS, twRB, twCap, twG, stw;
+  // atom-GEMM variant (k_spread_zdft_ag): B' half width (N2 = 2 * agNB), atom
+  // table entries, record buffer
+  int agNB, agCap, agRB;
   int xtcKyb;  // tensor-core x-axis DFT: ky values per item (rows (ky, type), T per ky)
   int nf[3];
   int dz;

@@ -56,6 +56,7 @@ namespace {
 #include "kernel_spread_simt.cuh"
 #include "kernel_spread_tc.cuh"
 #include "kernel_spread_tcw.cuh"
+#include "kernel_spread_ag.cuh"
 #include "kernel_dft.cuh"
 #include "kernel_adjoint.cuh"
 
@@ -120,6 +121,9 @@ struct SaxsPlan {
   int tw_cap[2] = {0, 0}, tw_rb[2] = {0, 0};  // wide kernel atom table / record buffer, 1 or 2 groups
   size_t tw_smem[2] = {0, 0};
   bool tc_ok = false, ytc_ok = false, xtc_ok = false;  // tensor-core kernels the plan can run
+  bool ag_ok = false, use_ag = false;  // atom-GEMM spreading (k_spread_zdft_ag): runnable, in use
+  size_t smem_spread_ag = 0;
+  int ag_ctas = 1;
   bool use_ytc = false;  // y-axis DFT on the tensor cores (k_dft_tc<false>)
   bool use_xtc = false;  // x-axis DFT + post on the tensor cores (k_dft_tc<true>)
   DtcShape yshape{}, xshape{};
@@ -637,9 +641,33 @@ int create(const SaxsParams *prm, SaxsPlan **out, const long long *min_half = nu
             GW = g;
           }
     }
+    // atom-GEMM tiles: B' = [Sh | Sl] of 2 * NB columns (NB = 2 * nkz padded to
+    // 16, N2 <= 256 and two accumulator stages in 512 columns), kAgSlots chunk
+    // slots, then the largest atom table and record buffer beside them
+    {
+      const int NB = round_up(2 * a.nkz, 16);
+      const char *agm = std::getenv("PYCUSAXS_ZAG");  // PYCUSAXS_ZAG=0: not available
+      if (a.stw > 0 && 2 * NB <= 256 && !simt_only && !(agm && std::strcmp(agm, "0") == 0)) {
+        const size_t avail_ag = optin - static_smem(k_spread_zdft_ag);
+        const size_t fixed = 128 + kAgSlots * (2 * kAgWBytes + static_cast<size_t>(kAgK) * 2 * NB * 2) +
+                             static_cast<size_t>(a.stiles[0] + 2 * a.stw) * sizeof(int4);
+        static const int cand[][2] = {{1024, 1024}, {1024, 512}, {512, 1024}, {512, 512}, {1024, 256},
+                                      {512, 256},   {256, 512},  {256, 256},  {128, 256}, {128, 128}};
+        for (const auto &c : cand)
+          if (!pl->ag_ok && fixed + 2 * static_cast<size_t>(c[1]) * 16 + static_cast<size_t>(c[0]) * kAgAtomBytes <=
+                                avail_ag) {
+            pl->ag_ok = true;
+            a.agNB = NB;
+            a.agCap = c[0];
+            a.agRB = c[1];
+            pl->smem_spread_ag = fixed + 2 * static_cast<size_t>(c[1]) * 16 + static_cast<size_t>(c[0]) * kAgAtomBytes;
+          }
+      }
+    }
     pl->tcn_ok = !simt_only && N <= 256 && S > 0;
     pl->tcw_ok = !simt_only && !narrow_only && GW > 0;
-    if (pl->tcn_ok || pl->tcw_ok) {
+    if (pl->ag_ok) pl->use_ag = mode && std::strcmp(mode, "atoms") == 0;  // PYCUSAXS_ZDFT=atoms
+    if (pl->tcn_ok || pl->tcw_ok || pl->ag_ok) {
       pl->use_tc = true;
       pl->use_tcw = pl->tcw_ok;
       a.tcN = N;
@@ -943,6 +971,7 @@ int create(const SaxsParams *prm, SaxsPlan **out, const long long *min_half = nu
   if (e == cudaSuccess) e = raise_smem_limit(k_hist<double>);
   if (e == cudaSuccess) e = raise_smem_limit(k_spread_zdft_tc);
   if (e == cudaSuccess) e = raise_smem_limit(k_spread_zdft_tcw);
+  if (e == cudaSuccess) e = raise_smem_limit(k_spread_zdft_ag);
   if (e == cudaSuccess) e = raise_smem_limit(k_dft_tc<false>);
   if (e == cudaSuccess) e = raise_smem_limit(k_dft_tc<true>);
   // load the allocation-free forward's last kernel now (under lazy module
@@ -984,6 +1013,7 @@ int create(const SaxsParams *prm, SaxsPlan **out, const long long *min_half = nu
       cudaGetLastError();  // a size the device cannot schedule is not an error of the plan
     }
     if (e == cudaSuccess && pl->tcw_ok) pl->tcw_ctas = std::max(1, sms);  // 512 TMEM columns: one per SM
+    if (e == cudaSuccess && pl->ag_ok) pl->ag_ctas = std::max(1, sms);    // its shared memory: one per SM
     if (e == cudaSuccess && pl->tcn_ok) {
       // resident CTAs whose tensor-memory allocations fit the SM's 512 columns together
       int tc_per_sm = 0;
@@ -1114,6 +1144,11 @@ int launch_sort(const SaxsPlan *pl, const DevArgs &a, int nframes, cudaStream_t 
 // Spreading + z-axis DFT of `nframes` frames: the wide-tile or 64-column
 // tensor-core kernel the plan is configured for, else the FP32 SIMT kernel.
 int launch_spread(const SaxsPlan *pl, const DevArgs &a, int nframes, cudaStream_t st) {
+  if (pl->use_tc && pl->use_ag) {
+    const int items = a.stiles[0] * a.stw * a.T * nframes;
+    return launch_pdl("k_spread_zdft_ag", k_spread_zdft_ag, dim3(std::max(1, std::min(items, pl->ag_ctas))),
+                      dim3(kAgThreads), pl->smem_spread_ag, st, a, items);
+  }
   if (pl->use_tc && pl->use_tcw) {
     const int items = a.stiles[0] * a.stw * a.T * nframes;
     return launch_pdl("k_spread_zdft_tcw", k_spread_zdft_tcw, dim3(std::max(1, std::min(items, pl->tcw_ctas))),
@@ -1302,9 +1337,10 @@ int regrow(SaxsPlan *pl, const long long need[3], cudaStream_t st) {
     return rc;
   }
   // the kernel configuration in use (an autotuned choice), where it still fits
-  if ((!pl->use_tc || (pl->use_tcw ? np->tcw_ok : np->tcn_ok)) && (!pl->use_ytc || np->ytc_ok) &&
-      (!pl->use_xtc || np->xtc_ok)) {
+  if ((!pl->use_tc || (pl->use_ag ? np->ag_ok : pl->use_tcw ? np->tcw_ok : np->tcn_ok)) &&
+      (!pl->use_ytc || np->ytc_ok) && (!pl->use_xtc || np->xtc_ok)) {
     np->use_tc = pl->use_tc;
+    np->use_ag = pl->use_ag;
     np->use_tcw = pl->use_tcw;
     np->use_ytc = pl->use_ytc;
     np->use_xtc = pl->use_xtc;
@@ -1834,7 +1870,7 @@ int saxs_plan_info(const SaxsPlan *pl, SaxsPlanInfo *info) {
   info->kbox[2] = a.nkz;
   info->kz_count = a.nkz;
   info->path = (pl->use_tc ? 1 : 0) | (pl->use_ytc ? 2 : 0) | (pl->use_xtc ? 4 : 0) |
-               (pl->use_tc && pl->use_tcw ? 8 : 0);
+               (pl->use_tc && !pl->use_ag && pl->use_tcw ? 8 : 0) | (pl->use_tc && pl->use_ag ? 16 : 0);
   info->device_bytes = pl->bytes;
   info->frames_accumulated = pl->frames;
   return SAXS_OK;
@@ -1854,11 +1890,24 @@ int saxs_plan_config(const SaxsPlan *pl, SaxsPlanConfig *cfg) {
   cfg->z_wide_tiles_available = pl->tcw_ok ? 1 : 0;
   cfg->z_producer_groups_max = (pl->tcn_ok && pl->a.tcS == 2) ? 2 : 1;
   cfg->z_wide_producer_groups_max = pl->tcw_ok ? pl->twG_max : 1;
+  cfg->z_atom_gemm = pl->use_tc && pl->use_ag ? 1 : 0;
+  cfg->z_atom_gemm_available = pl->ag_ok ? 1 : 0;
   return SAXS_OK;
 }
 
 int saxs_plan_set_config(SaxsPlan *pl, const SaxsPlanConfig *cfg) {
   if (!pl || !cfg) return fail(SAXS_E_INVALID, "null argument");
+  if (cfg->z_atom_gemm) {
+    if (!pl->ag_ok || !cfg->z_tensor_cores)
+      return fail(SAXS_E_INVALID, "the atom-GEMM spreading was requested but the plan cannot run it");
+    if ((cfg->y_tensor_cores && !pl->ytc_ok) || (cfg->x_tensor_cores && !pl->xtc_ok))
+      return fail(SAXS_E_INVALID, "a tensor-core pass the plan cannot run was requested");
+    pl->use_tc = true;
+    pl->use_ag = true;
+    pl->use_ytc = cfg->y_tensor_cores != 0;
+    pl->use_xtc = cfg->x_tensor_cores != 0;
+    return SAXS_OK;
+  }
   const bool z = cfg->z_tensor_cores != 0, wide = z && cfg->z_wide_tiles != 0;
   if ((z && !(wide ? pl->tcw_ok : pl->tcn_ok)) || (cfg->y_tensor_cores && !pl->ytc_ok) ||
       (cfg->x_tensor_cores && !pl->xtc_ok))
@@ -1868,6 +1917,7 @@ int saxs_plan_set_config(SaxsPlan *pl, const SaxsPlanConfig *cfg) {
     return fail(SAXS_E_INVALID, "z_producer_groups must be 1.." + std::to_string(gmax));
   pl->use_tc = z;
   pl->use_tcw = wide;
+  pl->use_ag = false;
   pl->use_ytc = cfg->y_tensor_cores != 0;
   pl->use_xtc = cfg->x_tensor_cores != 0;
   if (wide)

@@ -45,7 +45,8 @@ class PlanInfo:
     path: int = 0  # bits 1, 2, 4: the z-, y-, x-axis DFT on the tensor cores (tcgen05); 8: wide z tiles
 
 
-CONFIG_KEYS = ("z_tensor_cores", "y_tensor_cores", "x_tensor_cores", "z_wide_tiles", "z_producer_groups")
+CONFIG_KEYS = ("z_tensor_cores", "y_tensor_cores", "x_tensor_cores", "z_wide_tiles", "z_producer_groups",
+               "z_atom_gemm")
 
 
 def entries_from_index(atom_index: dict, natoms: int | None = None):
@@ -171,22 +172,27 @@ class SaxsEngine:
     def config(self) -> dict:
         """The kernel configuration in use: tensor cores (1) or FP32 SIMT (0) for
         the z, y and x passes, 128- (1) or 64-column (0) tiles and the producer
-        groups of the tensor-core spreading."""
+        groups of the tensor-core spreading, and whether the spreading runs as
+        one tensor-core GEMM over the atoms (``z_atom_gemm``, 128-column tiles;
+        the tile and group fields then do not apply)."""
         c = self._config_struct()
         return {k: int(getattr(c, k)) for k in CONFIG_KEYS}
 
     def config_candidates(self) -> list:
         """Every configuration the plan can run (its resources cover them all)."""
         c = self._config_struct()
-        zk = [(0, 0, 1)]  # (tensor cores, wide tiles, producer groups)
+        zk = [(0, 0, 1, 0)]  # (tensor cores, wide tiles, producer groups, atom GEMM)
         if c.z_narrow_tiles_available:
-            zk += [(1, 0, g) for g in range(1, c.z_producer_groups_max + 1)]
+            zk += [(1, 0, g, 0) for g in range(1, c.z_producer_groups_max + 1)]
         if c.z_wide_tiles_available:
-            zk += [(1, 1, g) for g in range(1, c.z_wide_producer_groups_max + 1)]
+            zk += [(1, 1, g, 0) for g in range(1, c.z_wide_producer_groups_max + 1)]
+        if c.z_atom_gemm_available:
+            zk += [(1, 1, 1, 1)]
         ys = [0, 1] if c.y_tensor_cores_available else [0]
         xs = [0, 1] if c.x_tensor_cores_available else [0]
         return [{"z_tensor_cores": z, "y_tensor_cores": y, "x_tensor_cores": x, "z_wide_tiles": w,
-                 "z_producer_groups": g} for (z, w, g), y, x in itertools.product(zk, ys, xs)]
+                 "z_producer_groups": g, "z_atom_gemm": ag}
+                for (z, w, g, ag), y, x in itertools.product(zk, ys, xs)]
 
     def set_config(self, cfg: dict) -> None:
         """Select one of ``config_candidates()``; work already queued keeps the

@@ -56,3 +56,40 @@ def assert_profiles_close(h, n, ho, no, rtol=RTOL_PROFILE):
     err = np.abs(got - want) / np.abs(want)
     assert err.max() <= rtol, f"max rel err {err.max():.3e} at bins {np.nonzero(sel)[0][err > rtol]}"
     return float(err.max())
+
+
+_CASE_ORACLE = {}
+
+
+def oracle_case(name, case, system):
+    """FP64 oracle (hist, nhist, plan) of a golden case over all its frames,
+    computed once per test session."""
+    if name not in _CASE_ORACLE:
+        g = case["grid"]
+        grid = tuple(g * 3 if len(g) == 1 else g)
+        sg = case.get("scaled", [0, 0, 0])
+        _CASE_ORACLE[name] = oracle_hist(
+            system, grid, [system.frame(k) for k in range(case["frames"])],
+            scaled_grid=tuple(sg * 3 if len(sg) == 1 else sg), order=case.get("order", 4),
+            sigma=case["sigma"], bin_size=case["bin_size"], qcut=case["qcut"],
+            ensemble=case.get("simulation") or "npt")
+    return _CASE_ORACLE[name]
+
+
+def check_against_reference_file(got, oracle_rows, ref_rows, rtol):
+    """Rows (q, I) of the CUDA path against the reference's file, where the
+    reference's own FP32 error can exceed `rtol`: the q text must be identical,
+    and per bin the CUDA path may differ from the reference by no more than the
+    FP64 oracle of the same method does, plus rtol.  Returns (max relative
+    difference CUDA - reference, max relative difference oracle - reference)."""
+    qs = [r[0] for r in ref_rows]
+    assert [f"{q:10.5f}" for q, _ in got] == qs
+    assert [f"{q:10.5f}" for q, _ in oracle_rows] == qs
+    c = np.array([i for _, i in got])
+    o = np.array([i for _, i in oracle_rows])
+    r = np.array([float(x[1]) for x in ref_rows])
+    dc = np.abs(c - r) / np.abs(r)
+    do = np.abs(o - r) / np.abs(r)
+    bad = np.nonzero(dc > do + rtol)[0]
+    assert bad.size == 0, f"bins {bad}: cuda-ref {dc[bad]}, oracle-ref {do[bad]}"
+    return float(dc.max()), float(do.max())

@@ -5,7 +5,8 @@ Plans take a tensor-core kernel whenever its operands fit shared memory
 pass runs the 128-column wide-tile kernel);
 ``PYCUSAXS_ZDFT=simt`` / ``PYCUSAXS_YDFT=simt`` / ``PYCUSAXS_XDFT=simt`` at plan
 creation keep the SIMT kernel, ``PYCUSAXS_ZDFT=narrow`` the 64-column
-tensor-core z kernel.  Every z case runs with both z kernels.  Both must give identical bin counts and profiles within the 1e-4
+tensor-core z kernel, ``PYCUSAXS_ZDFT=atoms`` the atom-GEMM z kernel (path bit
+4).  Every z case runs with each of the three z kernels.  Both must give identical bin counts and profiles within the 1e-4
 tolerance of the FP64 oracle; the 3xTF32 products are accurate to ~2^-19, and
 TC_VS_SIMT_RTOL (2e-5 per bin) bounds the difference between the two kernels.
 """
@@ -42,14 +43,15 @@ def dft_mode(var, mode):
 _AXES = {"z": ("PYCUSAXS_ZDFT", 1), "y": ("PYCUSAXS_YDFT", 2), "x": ("PYCUSAXS_XDFT", 4)}
 
 
-@pytest.fixture(params=["wide", "narrow"])
+@pytest.fixture(params=["wide", "narrow", "atoms"])
 def zmode(request):
     return request.param
 
 
 def _both(system, grid, frames, expect_tc=True, axis="z", zmode="wide", expect_wide=None, **kw):
     var, bit = _AXES[axis]
-    with dft_mode(var, "narrow" if (axis == "z" and zmode == "narrow") else None):
+    zenv = {"narrow": "narrow", "atoms": "atoms"}.get(zmode) if axis == "z" else None
+    with dft_mode(var, zenv):
         h_tc, n_tc, e_tc = engine_hist(system, grid, frames, **kw)
         path_tc = e_tc.info.path
         e_tc.close()
@@ -61,6 +63,9 @@ def _both(system, grid, frames, expect_tc=True, axis="z", zmode="wide", expect_w
     assert (path_tc & bit) == (bit if expect_tc else 0)
     if axis == "z" and zmode == "narrow":
         assert path_tc & 8 == 0
+    elif axis == "z" and zmode == "atoms":
+        if expect_wide:  # every plan that can run the wide tiles can run the atom GEMM
+            assert path_tc & 16 == 16, path_tc
     elif axis == "z" and expect_wide is not None:
         assert (path_tc & 8) == (8 if expect_wide else 0), path_tc
     np.testing.assert_array_equal(n_tc, n_s)
