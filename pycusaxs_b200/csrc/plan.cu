@@ -1892,6 +1892,10 @@ int saxs_plan_config(const SaxsPlan *pl, SaxsPlanConfig *cfg) {
   cfg->z_wide_producer_groups_max = pl->tcw_ok ? pl->twG_max : 1;
   cfg->z_atom_gemm = pl->use_tc && pl->use_ag ? 1 : 0;
   cfg->z_atom_gemm_available = pl->ag_ok ? 1 : 0;
+  if (cfg->z_atom_gemm) {  // its tiles are the wide ones; it has no producer groups
+    cfg->z_wide_tiles = 1;
+    cfg->z_producer_groups = 1;
+  }
   return SAXS_OK;
 }
 

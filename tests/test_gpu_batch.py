@@ -2,11 +2,13 @@
 
 Each system's histogram after the batched launches must equal the one its own
 engine gives for the same frames (exact counts, 1e-6 relative intensities),
-across two launches (the two alternating graph copies) and two buckets.
+across two launches (the two alternating graph copies) and two buckets, and
+the FP64 oracle's for those frames (exact counts, RTOL_PROFILE per bin).
 """
 import numpy as np
 import pytest
 
+from helpers import assert_profiles_close, oracle_hist
 from pycusaxs_b200 import SaxsEngine
 from pycusaxs_b200.batch import BatchedSaxs
 from pycusaxs_b200.synthetic import uneven_systems
@@ -42,6 +44,9 @@ def test_batched_graph_equals_per_system_engines(cuda):
         np.testing.assert_array_equal(n, nr)
         sel = nr > 0
         np.testing.assert_allclose(h[sel], hr[sel], rtol=1e-6)
+        frames = [s.frame(k) for k in range(6)]
+        ho, no, _ = oracle_hist(s, (g,) * 3, frames, sigma=2.0, bin_size=0.002, qcut=0.5)
+        assert_profiles_close(h, n, ho, no)
     batch.close()
 
 
