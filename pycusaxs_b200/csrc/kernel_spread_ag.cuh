@@ -140,9 +140,11 @@ __device__ __forceinline__ void ag_prepass(const DevArgs &a, const TileAtomsW &t
 // The operands of table atoms [k0, k0 + kc) in one chunk slot: W (head, Wh, and
 // remainder, Wl; zeroed beforehand) and B' = [Sh | Sl].  W: two atoms per warp
 // pass, a lane per (x tap, y tap).  S: a warp per atom, a lane per kz (and
-// kz + 32), so the twiddle loads of a tap are one coalesced row of tw[z][*].
-__device__ __forceinline__ void ag_operands(const DevArgs &a, const AgTab &tab, int k0, int kc, uint16_t *Wh,
-                                            uint16_t *Wl, uint16_t *Bp, int NB, int tid, int nthreads) {
+// kz + 32), reading the z twiddles tws[z][kz] from shared memory (the kernel's
+// shared memory leaves too little L1 to keep them cached).
+__device__ __forceinline__ void ag_operands(const DevArgs &a, const AgTab &tab, const float2 *tws, int k0, int kc,
+                                            uint16_t *Wh, uint16_t *Wl, uint16_t *Bp, int NB, int tid,
+                                            int nthreads) {
   const int N2 = 2 * NB;
   const int lane = tid & 31, warp = tid >> 5, nwarps = nthreads >> 5;
   for (int p = warp; 2 * p < kc; p += nwarps) {
@@ -174,7 +176,7 @@ __device__ __forceinline__ void ag_operands(const DevArgs &a, const AgTab &tab, 
 #pragma unroll
       for (int o = 0; o < 4; ++o) {
         if (zo[o] < ez && wz[o] != 0.0f) {
-          const float2 tw = __ldg(a.twz + static_cast<int64_t>(zo[o]) * a.nkzp + kz);
+          const float2 tw = tws[zo[o] * nkz + kz];
           sr = fmaf(wz[o], tw.x, sr);
           si = fmaf(wz[o], tw.y, si);
         }
@@ -211,8 +213,8 @@ __device__ __forceinline__ void ag_operands(const DevArgs &a, const AgTab &tab, 
 //   acc_full[d] / acc_empty[d]   MMA -> epilogue -> MMA, accumulator stage d
 // Dynamic shared memory (128-byte aligned): kAgSlots chunk slots {Wh, Wl, B'},
 // two record buffers of agRB float4, the home-bin tables (stiles[0] + 2*stw
-// int4) and an atom table of agCap entries.  Tensor memory: two accumulator
-// stages of N2 columns.
+// int4), the z twiddles (ez x nkz float2) and an atom table of agCap entries.
+// Tensor memory: two accumulator stages of N2 columns.
 __global__ void __launch_bounds__(kAgThreads, 1) k_spread_zdft_ag(DevArgs a, int items) {
   pdl_release();
   extern __shared__ __align__(16) unsigned char smem[];
@@ -232,8 +234,9 @@ __global__ void __launch_bounds__(kAgThreads, 1) k_spread_zdft_ag(DevArgs a, int
   float4 *recs = reinterpret_cast<float4 *>(base + kAgSlots * slot_bytes);
   int4 *home_x = reinterpret_cast<int4 *>(recs + 2 * RB);
   int4 *home_y = home_x + a.stiles[0];
+  float2 *tws = reinterpret_cast<float2 *>(home_y + 2 * a.stw);
   AgTab tab;
-  tab.wx = reinterpret_cast<float4 *>(home_y + 2 * a.stw);
+  tab.wx = reinterpret_cast<float4 *>(tws + ((a.ext[2] * a.nkz + 1) & ~1));  // 16-byte aligned
   tab.wy = tab.wx + cap;
   tab.wz = tab.wy + cap;
   tab.zo = reinterpret_cast<int4 *>(tab.wz + cap);
@@ -248,6 +251,7 @@ __global__ void __launch_bounds__(kAgThreads, 1) k_spread_zdft_ag(DevArgs a, int
     for (int i = tid; i < n16; i += blockDim.x) z[i] = make_int4(0, 0, 0, 0);
     for (int i = tid; i < a.stiles[0]; i += blockDim.x) home_x[i] = a.home_x[i];
     for (int i = tid; i < 2 * a.stw; i += blockDim.x) home_y[i] = a.home_yw[i];
+    for (int i = tid; i < a.ext[2] * a.nkz; i += blockDim.x) tws[i] = a.twz[(i / a.nkz) * a.nkzp + i % a.nkz];
   }
   const uint32_t tcols = 2 * N2 <= 32 ? 32 : 2 * N2 <= 64 ? 64 : 2 * N2 <= 128 ? 128 : 2 * N2 <= 256 ? 256 : 512;
   if (warp == kAgMmaWarp) {
@@ -316,7 +320,7 @@ __global__ void __launch_bounds__(kAgThreads, 1) k_spread_zdft_ag(DevArgs a, int
               wz[i] = make_int4(0, 0, 0, 0);
           }
           producers_sync(kAgBar, kAgProducers);
-          ag_operands(a, tab, k0, kc, wh_of(s), wl_of(s), bp_of(s), NB, ptid, kAgProducers);
+          ag_operands(a, tab, tws, k0, kc, wh_of(s), wl_of(s), bp_of(s), NB, ptid, kAgProducers);
           asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // generic writes -> tensor core reads
           producers_sync(kAgBar, kAgProducers);
           if (ptid == 0) {

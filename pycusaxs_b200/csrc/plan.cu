@@ -650,7 +650,8 @@ int create(const SaxsParams *prm, SaxsPlan **out, const long long *min_half = nu
       if (a.stw > 0 && 2 * NB <= 256 && !simt_only && !(agm && std::strcmp(agm, "0") == 0)) {
         const size_t avail_ag = optin - static_smem(k_spread_zdft_ag);
         const size_t fixed = 128 + kAgSlots * (2 * kAgWBytes + static_cast<size_t>(kAgK) * 2 * NB * 2) +
-                             static_cast<size_t>(a.stiles[0] + 2 * a.stw) * sizeof(int4);
+                             static_cast<size_t>(a.stiles[0] + 2 * a.stw) * sizeof(int4) +
+                             static_cast<size_t>(round_up(a.ext[2] * a.nkz, 2)) * sizeof(float2);
         static const int cand[][2] = {{1024, 1024}, {1024, 512}, {512, 1024}, {512, 512}, {1024, 256},
                                       {512, 256},   {256, 512},  {256, 256},  {128, 256}, {128, 128}};
         for (const auto &c : cand)
