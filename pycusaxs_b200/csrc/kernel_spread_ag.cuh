@@ -315,9 +315,12 @@ __global__ void __launch_bounds__(kAgThreads, 1) k_spread_zdft_ag(DevArgs a, int
           if (skip) break;
           const int k0 = c * kAgK, kc = max(0, min(kAgK, n - k0));
           {
-            int4 *wz = reinterpret_cast<int4 *>(wh_of(s));  // Wh and Wl are contiguous
-            for (int i = ptid; i < static_cast<int>(2 * kAgWBytes / 16); i += kAgProducers)
-              wz[i] = make_int4(0, 0, 0, 0);
+            // the K columns the chunk's MMAs read (whole 16-atom k steps, at least
+            // one): (zk / 8) core-matrix groups of 128 rows x 16 bytes per operand
+            const int zk = max(16, (kc + 15) & ~15), n16 = zk * 16;
+            int4 *zh = reinterpret_cast<int4 *>(wh_of(s)), *zl = reinterpret_cast<int4 *>(wl_of(s));
+            for (int i = ptid; i < 2 * n16; i += kAgProducers)
+              (i < n16 ? zh : zl)[i < n16 ? i : i - n16] = make_int4(0, 0, 0, 0);
           }
           producers_sync(kAgBar, kAgProducers);
           ag_operands(a, tab, tws, k0, kc, wh_of(s), wl_of(s), bp_of(s), NB, ptid, kAgProducers);
