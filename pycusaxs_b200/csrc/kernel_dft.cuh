@@ -456,6 +456,20 @@ __global__ void __launch_bounds__(dtc_threads<kX>(), 1)
     int i = 0;
     for (int w = blockIdx.x; w < items; w += gridDim.x, ++i) {
       const int d = i & 1;
+      // x pass: the item's geometry, form factors and padding mean, loaded before
+      // the wait so that their latency overlaps it
+      float ocs[9], ff[9], mean = 0.0f;
+      if (kX) {
+        const int T = a.T, kyb = a.xtcKyb;
+        const int nblk = (a.nky + kyb - 1) / kyb;
+        const int f = w / (a.nkz * nblk);
+        const int kyl = r / T, t = r % T, ky = (w % nblk) * kyb + kyl;
+#pragma unroll
+        for (int q = 0; q < 9; ++q) ocs[q] = a.geom[f * kGeom + 9 + q];
+#pragma unroll
+        for (int q = 0; q < 9; ++q) ff[q] = a.ff[9 * t + q];
+        if (r < T * kyb && ky < a.nky) mean = padding_mean(a, f, t);
+      }
       wait(&dfull[d], i >> 1);
       // x pass: the four warps of a slot meet at named barriers, so they decide together
       if (kX ? producers_sync_or(abort_flag != 0, 1 + eslot, 128) : __any_sync(0xffffffffu, abort_flag != 0))
@@ -523,17 +537,16 @@ __global__ void __launch_bounds__(dtc_threads<kX>(), 1)
         const int nblk = (a.nky + kyb - 1) / kyb;
         const int f = w / (a.nkz * nblk), kz = (w / nblk) % a.nkz;
         const int ky0 = (w % nblk) * kyb;
-        const int kyl = r / T, t = r % T, ky = ky0 + kyl;
+        const int kyl = r / T, ky = ky0 + kyl;
         const bool row_ok = r < T * kyb && ky < a.nky;
-        float ocs[9];
-#pragma unroll
-        for (int q = 0; q < 9; ++q) ocs[q] = a.geom[f * kGeom + 9 + q];
         const int ka = signed_k(kz, a.nn[2], a.nf[2]);
         const int ja = a.ky_lo + min(ky, a.nky - 1);
-        const float mean = row_ok ? padding_mean(a, f, t) : 0.0f;
-        float ff[9];
-#pragma unroll
-        for (int q = 0; q < 9; ++q) ff[q] = a.ff[9 * t + q];
+        // the per-row form factors use the float |q|; their cut-off test is made
+        // inclusive by 1e-6 relative (kpoint_q_f32 is within a few ulp of the
+        // reference's expression), and the reference's expression itself decides
+        // below which outputs are kept
+        const float qcut_incl = a.qcut * (1.0f + 1e-6f);
+        const float inv4pi = static_cast<float>(1.0 / (4.0 * M_PI));
         float2 *red = xsum + eslot * 128 * 8;  // [row][8 kx]
         const int rid = 32 * quarter + lane;    // 0..127 over the slot's four warps
         const uint32_t bar_id = 1 + eslot;
@@ -544,15 +557,15 @@ __global__ void __launch_bounds__(dtc_threads<kX>(), 1)
           for (int jj = 0; jj < 8; ++jj) {
             const int kx = c0 / 2 + jj;
             const int ia = a.kx_lo + min(kx, a.nkx - 1);
-            const float mw = kpoint_q(ocs, ia, ja, ka);
-            const bool inside = row_ok && kx < a.nkx && !(mw > a.qcut);
+            const float mw = kpoint_q_f32(ocs, ia, ja, ka);
+            const bool inside = row_ok && kx < a.nkx && !(mw > qcut_incl);
             float2 F = make_float2(__uint_as_float(v[2 * jj]), __uint_as_float(v[2 * jj + 1]));
             // the padding mean's constant over the whole supercell lands at k = 0
             if (ka == 0 && ja == 0 && ia == 0)
               F.x += static_cast<float>(static_cast<double>(mean) * a.nn3);
             float2 A = make_float2(0.f, 0.f);
             if (inside) {
-              const float q = mw / (4.0 * M_PI);
+              const float q = mw * inv4pi;
               const float ft = form_factor(ff, q * q);
               A.x = ft * F.x;
               A.y = ft * F.y;

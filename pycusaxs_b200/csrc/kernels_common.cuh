@@ -137,6 +137,19 @@ __device__ __forceinline__ float kpoint_q(const float *oc, int ia, int ja, int k
   return mw;
 }
 
+// |q| of the same k-point in float arithmetic only (the 2*pi factor in float):
+// within a few ulp of kpoint_q, for uses that tolerate that - the form factor's
+// argument, and a cut-off test made slightly inclusive - where kpoint_q's three
+// double-precision multiplies per point would dominate.
+__device__ __forceinline__ float kpoint_q_f32(const float *oc, int ia, int ja, int ka) {
+  const float tp = 6.28318530717958647692f;
+  const float fa = static_cast<float>(ia), fb = static_cast<float>(ja), fc = static_cast<float>(ka);
+  const float m1 = tp * (oc[0] * fa + oc[1] * fb + oc[2] * fc);
+  const float m2 = tp * (oc[3] * fa + oc[4] * fb + oc[5] * fc);
+  const float m3 = tp * (oc[6] * fa + oc[7] * fb + oc[8] * fc);
+  return sqrtf(m1 * m1 + m2 * m2 + m3 * m3);
+}
+
 // Cubic (order-4) cardinal B-spline weights of the four taps at fractional
 // offset u in [0, 1]: tap 0 is the farthest-left grid point.
 __device__ __forceinline__ void cubic_weights(float u, float w[4]) {
