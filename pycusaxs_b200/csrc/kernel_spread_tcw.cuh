@@ -288,7 +288,11 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
   __shared__ volatile int released;
   __shared__ int tab_count[2][2][2];  // reaching atoms in the table: [group][item parity][chunk parity]
   const int NB = a.twN, N = 2 * a.twN, KT = a.tcK, R = a.tcR, RB = a.twRB, RS = a.twRS, G = a.twG;
-  const int SR = 2;  // split warps per lane quarter (16 z of a chunk each); 4 measured no faster
+  // split warps per lane quarter: the item's 16-z units u = 2c + h (chunk c,
+  // half h) go to rank u mod SR, and the other ranks pre-pass the next item
+  // meanwhile (SR = 4 split faster but left the dense types' pre-pass too few
+  // warps: 2.42 against 2.32 ms per 100 frames of the 100k-atom workload)
+  constexpr int SR = 2;
   const int CH = (KT + kTwChunk - 1) / kTwChunk;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   float *bh = reinterpret_cast<float *>(smem);  // B' = [Bh | Bl], f16, K-major, N columns
@@ -328,7 +332,7 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
   if (tid == 0) {
     for (int i = 0; i < 4 + 2 * kTwRing + 4; ++i) {
       int cnt = 1;
-      if (i >= 4 && i < 4 + kTwRing) cnt = 4 * SR;  // a_full: 4 lane quarters x SR split warps
+      if (i >= 4 && i < 4 + kTwRing) cnt = 8;  // a_full: 4 lane quarters x 2 units of 16 z
       if (i >= 4 + 2 * kTwRing + 2) cnt = 4;   // acc_empty: 4 epilogue warps
       asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&bars[i])), "r"(cnt));
     }
@@ -426,17 +430,24 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
         const int mm = i / ((R - KT) / 4), zq = i % ((R - KT) / 4);
         reinterpret_cast<float4 *>(A + static_cast<size_t>(mm) * RS + KT)[zq] = make_float4(0.f, 0.f, 0.f, 0.f);
       }
-      // split, chunk by chunk through the A ring
-      for (int c = 0; c < CH; ++c) {
-        const int q = j * CH + c, s = q % kTwRing;
-        if (q >= kTwRing) wait_released(q - kTwRing + 1);
+      // split, in batches of up to kTwRing chunks through the A ring: one bounded
+      // wait until the batch's ring slots are free (the release counter is
+      // monotonic), the tensor-memory stores of this warp's units of the batch,
+      // one wait for their completion, then the units' chunks handed to the MMA
+      // warp (a_full counts the 8 units of a chunk, 2 per lane quarter)
+      const float mz0 = -mean_fx * 0x1p-17f;
+      for (int cb = 0; cb < CH; cb += kTwRing) {
+        const int ce = min(CH, cb + kTwRing);
+        const int q_last = j * CH + ce - 1;
+        if (q_last >= kTwRing) wait_released(q_last - kTwRing + 1);
         __syncwarp();  // converged for the .sync.aligned tensor-memory stores
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const int h = rq;
-        // 16 z per split warp: (tile - mean) * 2^-17 in fixed-point units, split
-        // into an f16 head and remainder; two halves per tensor-memory column,
-        // head to the slot's first 16 columns, remainder to the next 16
-        {
+        for (int u = 2 * cb + rq; u < 2 * ce; u += SR) {
+          const int c = u >> 1, h = u & 1;
+          const int s = (j * CH + c) % kTwRing;
+          // 16 z: (tile - mean) * 2^-17 in fixed-point units, split into an f16
+          // head and remainder; two halves per tensor-memory column, head to the
+          // slot's columns 8h.., remainder to 16 + 8h..
           const int z0 = kTwChunk * c + 16 * h;
           uint32_t hi[8], lo[8];
           // all four loads, then the zeroing stores, then the arithmetic
@@ -448,11 +459,13 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
 #pragma unroll
           for (int k4 = 0; k4 < 4; ++k4)
             if (k4 < nq) p[k4] = make_int4(0, 0, 0, 0);
-          const float mz = z0 < KT ? mean_fx : 0.0f;
+          // (v - mean) * 2^-17 as one FMA: scaling by a power of two is exact, so
+          // v * 2^-17 - mean * 2^-17 rounds to the same value
+          const float mz = z0 < KT ? mz0 : 0.0f;
 #pragma unroll
           for (int k4 = 0; k4 < 4; ++k4) {
-            const float v[4] = {(__int2float_rn(iv[k4].x) - mz) * 0x1p-17f, (__int2float_rn(iv[k4].y) - mz) * 0x1p-17f,
-                                (__int2float_rn(iv[k4].z) - mz) * 0x1p-17f, (__int2float_rn(iv[k4].w) - mz) * 0x1p-17f};
+            const float v[4] = {fmaf(__int2float_rn(iv[k4].x), 0x1p-17f, mz), fmaf(__int2float_rn(iv[k4].y), 0x1p-17f, mz),
+                                fmaf(__int2float_rn(iv[k4].z), 0x1p-17f, mz), fmaf(__int2float_rn(iv[k4].w), 0x1p-17f, mz)};
 #pragma unroll
             for (int e = 0; e < 4; e += 2) {
               const __half2 hh = __floats2half2_rn(v[e], v[e + 1]);
@@ -476,7 +489,8 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
         asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         __syncwarp();
-        if (lane == 0) mbar_arrive(smem_addr(&a_full[s]));
+        if (lane == 0)
+          for (int u = 2 * cb + rq; u < 2 * ce; u += SR) mbar_arrive(smem_addr(&a_full[(j * CH + (u >> 1)) % kTwRing]));
       }
     }
   } else if (warp == kTwMmaWarp) {

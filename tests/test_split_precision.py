@@ -7,7 +7,8 @@ the low 13 mantissa bits cleared plus the FP32 remainder, three products).  This
 model of one item's GEMM (128 z x 21 kz, sparse tile values around the padding
 mean, in the kernel's fixed-point units and 2^-17 scaling) checks that both
 stay within 5e-7 of the largest FP64 result and that the f16 form is no less
-accurate than 3xTF32.
+accurate than 3xTF32; a box-wide model checks the lowest-q amplitude, for which
+the mean must be subtracted inside the tile.
 """
 import numpy as np
 
@@ -53,6 +54,45 @@ def test_f16_split_matches_3xtf32_precision():
     e32 = np.abs(z32 - exact).max() / top
     assert e16 < 5e-7 and e32 < 5e-7, (e16, e32)
     assert e16 <= 1.2 * e32, (e16, e32)
+
+
+def _gemm16(a, tw):
+    """f16 head + rounded remainder of both operands, four products, FP32."""
+    ah = a.astype(np.float16)
+    al = (a - ah.astype(np.float32)).astype(np.float16)
+    b = _f32(tw)
+    bh = b.astype(np.float16)
+    bl = (b - bh.astype(np.float32)).astype(np.float16)
+    return _f32((_f32(ah) @ _f32(bh) + _f32(ah) @ _f32(bl)) + (_f32(al) @ _f32(bh) + _f32(al) @ _f32(bl)))
+
+
+def test_mean_inside_the_tile_keeps_lowest_q_amplitude():
+    # The lowest-q amplitude sums Z over every column of the box.  With the
+    # padding mean subtracted inside the tile (as the wide z kernel does) the FP32
+    # accumulation works on rho - mean and its rounding averages out over the
+    # columns; subtracting mean * sum_z tw after the transform instead leaves each
+    # column's FP32 sum of the positive density ~mean * |sum_z tw| large, and the
+    # box-wide sum several times less accurate.  A uniform 64-z system of 4096
+    # columns, kz = 1 of a 128 supercell.
+    errs_in, errs_after = [], []
+    for seed in range(3):
+        rng = np.random.default_rng(11 + seed)
+        scale, ez, nz = 2.0 ** 23, 64, 128
+        rho = rng.poisson(0.11 * 8, size=(4096, ez)) / 8.0
+        mean = np.float32(rho.mean())
+        i = np.rint(rho * scale).astype(np.int64)
+        z = np.arange(ez)
+        tw = np.stack([np.cos(2 * np.pi * z / nz), -np.sin(2 * np.pi * z / nz)], axis=1)
+        exact = ((i / scale - np.float64(mean)) @ tw).sum(axis=0)
+        top = np.abs(exact).max()
+        x_in = _f32((i.astype(np.float32) - np.float32(mean * scale)) * np.float32(2.0 ** -17))
+        z_in = _gemm16(x_in, tw).astype(np.float64) * 2.0 ** 17 / scale
+        x_pos = _f32(i.astype(np.float32) * np.float32(2.0 ** -17))
+        z_after = _gemm16(x_pos, tw).astype(np.float64) * 2.0 ** 17 / scale - np.float64(mean) * tw.sum(axis=0)
+        errs_in.append(np.abs(z_in.sum(axis=0) - exact).max() / top)
+        errs_after.append(np.abs(z_after.sum(axis=0) - exact).max() / top)
+    assert max(errs_in) < 2e-6, errs_in
+    assert min(e / f for e, f in zip(errs_after, errs_in)) > 3, (errs_after, errs_in)
 
 
 def _f16_scale(m_t, ez, nx, ny, ey=None):
