@@ -621,10 +621,12 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
       float2 *Zft = a.Z + (static_cast<int64_t>(it.f) * a.T + it.t) * a.nkz * zplane;
       const int m = 32 * quarter + lane, lx = m >> 4, ly = m & 15;
       const bool valid = lx < min(kTwX, a.ext[0] - x0) && ly < min(kTwY, a.ext[1] - y0);
-      const int64_t cell = static_cast<int64_t>(x0 + lx) * a.ext[1] + (y0 + ly);
+      // offsets within the (frame, type) block of nkz planes fit in 32 bits
+      const int zp32 = static_cast<int>(zplane);
+      int off = (x0 + lx) * a.ext[1] + (y0 + ly);
       const uint32_t lane_base = tmem + (static_cast<uint32_t>(32 * quarter) << 16) + 256u +
                                  static_cast<uint32_t>(128 * d);
-      for (int c0 = 0; c0 < NB; c0 += 8) {
+      for (int c0 = 0; c0 < NB; c0 += 8, off += 4 * zp32) {
         uint32_t r[8], t[8];
         asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
                      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
@@ -636,14 +638,14 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
                      : "r"(lane_base + NB + c0));
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
         if (valid) {
+          // columns past 2*nkz (NB pads it to 16) only in the last groups
+          const int nk = min(4, a.nkz - c0 / 2);
 #pragma unroll
-          for (int jj = 0; jj < 4; ++jj) {
-            const int kz = c0 / 2 + jj;
-            if (kz < a.nkz)
-              Zft[kz * zplane + cell] =
+          for (int jj = 0; jj < 4; ++jj)
+            if (jj < nk)
+              Zft[off + jj * zp32] =
                   make_float2((__uint_as_float(r[2 * jj]) + __uint_as_float(t[2 * jj])) * unscale,
                               (__uint_as_float(r[2 * jj + 1]) + __uint_as_float(t[2 * jj + 1])) * unscale);
-          }
         }
       }
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");

@@ -666,7 +666,9 @@ int create(const SaxsParams *prm, SaxsPlan **out, const long long *min_half = nu
       }
     }
     pl->tcn_ok = !simt_only && N <= 256 && S > 0;
-    pl->tcw_ok = !simt_only && !narrow_only && GW > 0;
+    // (the wide kernel's epilogue indexes a (frame, type) block of Z in 32 bits)
+    pl->tcw_ok = !simt_only && !narrow_only && GW > 0 &&
+                 static_cast<int64_t>(a.nkz) * a.ext[0] * a.ext[1] < (int64_t{1} << 31);
     if (pl->ag_ok) pl->use_ag = mode && std::strcmp(mode, "atoms") == 0;  // PYCUSAXS_ZDFT=atoms
     if (pl->tcn_ok || pl->tcw_ok || pl->ag_ok) {
       pl->use_tc = true;
