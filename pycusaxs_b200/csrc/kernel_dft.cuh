@@ -111,7 +111,7 @@ template <bool kX>
 __host__ __device__ constexpr int dtc_epi_warps() { return kX ? 12 : 4; }
 template <bool kX>
 __host__ __device__ constexpr int dtc_threads() { return 32 * (kDtcProducerWarps + 2 + dtc_epi_warps<kX>()); }
-constexpr int kDtcMaxStages = 4;
+constexpr int kDtcMaxStages = 8;
 
 // One pass's GEMM shape: N', K chunks, stages, TMEM columns, B' table.
 // With `lo_smem` (when 2N' <= 256): only A's TF32 head goes to tensor memory (32

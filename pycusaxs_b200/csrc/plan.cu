@@ -306,10 +306,15 @@ bool dtc_shape(int nk, int extent, size_t avail, DtcShape *sh, size_t *smem, boo
   if (!(mode && (std::strcmp(mode, "tf32") == 0 || std::strcmp(mode, "split") == 0))) {
     const size_t stage16 = (128 * sizeof(float) + 2 * static_cast<size_t>(N) * sizeof(uint16_t)) * 2 * kDtcChunk;
     const int S16 = static_cast<int>((avail - 1024) / stage16);
-    int S = std::min({kDtcMaxStages, S16, (512 - 4 * N) / 32});
-    int side = 1;
-    if (S < 2 || 2 * N > 256) {
-      S = std::min({kDtcMaxStages, S16, (512 - 2 * N) / 32});
+    // [Bh | Bl] side by side (two MMAs per k step) needs accumulators of 2N'
+    // columns; the three-MMA form leaves tensor memory for more A stages, and is
+    // taken when it gets more: at N' = 96 seven stages against four, y pass 0.574
+    // -> 0.567 and x pass 0.249 -> 0.245 ms per 100 frames of the 100k-atom workload
+    const int S_side = 2 * N <= 256 ? std::min({kDtcMaxStages, S16, (512 - 4 * N) / 32}) : 0;
+    const int S_three = std::min({kDtcMaxStages, S16, (512 - 2 * N) / 32});
+    int S = S_side, side = 1;
+    if (S_three > S_side) {
+      S = S_three;
       side = 0;
     }
     if (S >= 2 && N <= 256) {
