@@ -27,7 +27,9 @@
 //               the first 16 columns of a slot, remainder in the next 16
 //   [256, 512)  two accumulator stages of 2*twN <= 128 columns
 constexpr int kTwX = 8, kTwY = 16;  // wide tile: x-columns, y-rows (M = 128)
-constexpr int kTwProducerWarps = 24;
+// 20 producer warps: 864 threads leave 72 registers a thread, which the taps'
+// 32-bit shared addressing needs without spills (24 warps: 64 registers)
+constexpr int kTwProducerWarps = 20;
 constexpr int kTwMmaWarp = kTwProducerWarps;
 constexpr int kTwLoaderWarp = kTwProducerWarps + 1;
 constexpr int kTwReleaseWarp = kTwProducerWarps + 6;
@@ -204,14 +206,14 @@ __device__ __forceinline__ void spread_prepass_w(const DevArgs &a, const TileAto
 // takes two units per round and reads both units' table entries before either
 // unit's atomics, so the shared-memory loads of one overlap the other.
 struct TapUnit {
-  int *col;  // tile row start of the unit's (y tap, z tap), or null when outside
-  int i;     // the atom's table entry
-  float w;   // wy * wz
+  uint32_t col;  // shared-window byte address of the unit's (y tap, z tap) row start
+  int i;         // the atom's table entry, or -1 when the unit is outside
+  float w;       // wy * wz
 };
 
-__device__ __forceinline__ TapUnit tap_unit(const AtomTabW &tab, int u, int nu, int *A, int rs) {
+__device__ __forceinline__ TapUnit tap_unit(const AtomTabW &tab, int u, int nu, uint32_t A, int rs) {
   TapUnit t;
-  t.col = nullptr;
+  t.i = -1;
   if (u >= nu) return t;
   const int i = u >> 4, p = (u >> 2) & 3, r = u & 3;
   const int ly = reinterpret_cast<const unsigned char *>(&tab.ly[i])[p];  // byte p
@@ -221,27 +223,31 @@ __device__ __forceinline__ TapUnit tap_unit(const AtomTabW &tab, int u, int nu, 
   const int zo = reinterpret_cast<const int *>(&tab.zo[i])[r];
   t.i = i;
   t.w = wy * wz;
-  t.col = A + zo + ly * rs;
+  t.col = A + 4u * static_cast<uint32_t>(zo + ly * rs);
   return t;
 }
 
 __device__ __forceinline__ void tap_apply(const AtomTabW &tab, const TapUnit &t) {
-  if (!t.col) return;
+  if (t.i < 0) return;
   const float4 w4 = tab.wxs[t.i];
   const int4 x4 = tab.xo[t.i];
   const float wx[4] = {w4.x, w4.y, w4.z, w4.w};
   const int xo[4] = {x4.x, x4.y, x4.z, x4.w};
 #pragma unroll
   for (int o = 0; o < 4; ++o)
-    if (xo[o] >= 0) atomicAdd(t.col + xo[o], tap_fixed(wx[o], t.w));
+    if (xo[o] >= 0)
+      asm volatile("red.shared.add.u32 [%0], %1;" ::"r"(t.col + 4u * static_cast<uint32_t>(xo[o])),
+                   "r"(tap_fixed(wx[o], t.w))
+                   : "memory");
 }
 
 __device__ __forceinline__ void spread_taps_w(const AtomTabW &tab, int nv, int *A, int rs, int tid,
                                               int nthreads) {
   const int nu = nv * 16;
+  const uint32_t a32 = smem_addr(A);
   for (int u = tid; u < nu; u += 2 * nthreads) {
-    const TapUnit t0 = tap_unit(tab, u, nu, A, rs);
-    const TapUnit t1 = tap_unit(tab, u + nthreads, nu, A, rs);
+    const TapUnit t0 = tap_unit(tab, u, nu, a32, rs);
+    const TapUnit t1 = tap_unit(tab, u + nthreads, nu, a32, rs);
     tap_apply(tab, t0);
     tap_apply(tab, t1);
   }

@@ -299,14 +299,14 @@ class SaxsEngine:
         copied straight to the device; anything else goes through a pinned
         staging buffer first.  Host-to-device copies run on a copy stream,
         double-buffered against the compute stream, in sub-batches (default:
-        4, 8, 16, ... frames, see ``_host_batches``; ``chunk`` frames each if
+        6, 10, 15, ... frames, see ``_host_batches``; ``chunk`` frames each if
         given) so that the copy of one sub-batch overlaps the kernels of the
         previous one.  The first sub-batch is small because its copy is not
         overlapped; the later ones grow because every sub-batch pays its
-        launches' ramp-up and tail.  On a B200 (55 GB/s pinned host-to-device)
-        with 100 frames of 100k atoms per call, 4/8/16/32/40 measured 4.6 ms
-        per call against 5.2 ms for tenths, 5.0 ms for fifths and 5.2 ms for
-        halves.
+        launches' ramp-up and tail.  On a B200 (52-55 GB/s pinned host-to-device
+        once warm) with 100 frames of 100k atoms per call, 6/10/15/25/44
+        measured 4.00 ms per call against 4.04 ms for 4/8/16/32/40 and 4.15-4.22
+        ms for schedules of eight or nine sub-batches growing 1.3-1.4-fold.
         """
         torch = self._torch
         pinned = isinstance(xyz, torch.Tensor) and xyz.device.type == "cpu" and xyz.is_pinned()
@@ -576,18 +576,22 @@ class SaxsEngine:
 def _host_batches(nf: int, cap: int, chunk=None):
     """(start, stop) frame ranges of forward_host's sub-batches of an nf-frame call.
 
-    ``chunk`` None: sizes doubling from 4 (4, 8, 16, ...), the last sub-batch
-    taking the rest when the rest is at most 1.5 times the next size; an int:
+    ``chunk`` None: sizes growing 1.6-fold from 6 (6, 10, 15, 25, ...), the last
+    sub-batch taking the rest when the rest is at most 1.5 times the next size
+    (each copy, at ~22 us per 1.2 MB frame, then mostly hides behind the previous
+    sub-batch's ~34 us per frame of kernels, and each sub-batch's fixed ~60 us of
+    launch ramp and tail is paid only five times per 100 frames); an int:
     that many frames per sub-batch; a sequence of ints: those sizes in order,
     the last one repeated.  Every size is clamped to [1, cap].
     """
     if chunk is None:
-        sizes, left, n = [], nf, 4
+        sizes, left, g = [], nf, 6.0
         while left > 0:
+            n = int(round(g))
             take = left if left <= 1.5 * n else n
             sizes.append(take)
             left -= take
-            n *= 2
+            g *= 1.6
     elif isinstance(chunk, (int, np.integer)):
         sizes = [int(chunk)]
     else:

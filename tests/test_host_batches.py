@@ -1,8 +1,8 @@
 """forward_host's sub-batch schedule (CPU) and its result on the GPU.
 
 The schedule must cover every frame exactly once, in order, with no sub-batch
-above the plan's max_frames; by default its sizes double from 4 so that the
-first (unoverlapped) copy is small.  On the GPU, frames fed from host memory in
+above the plan's max_frames; by default its sizes grow 1.6-fold from 6 so that
+the first (unoverlapped) copy is small.  On the GPU, frames fed from host memory in
 that schedule, in single frames, and from device memory in one batch (more than
 the 128 frames the sort kernel takes per launch in its parameters) must give the
 same histogram: exact bin counts and intensities within 1e-6 relative (the
@@ -24,9 +24,10 @@ def test_schedule_covers_every_frame_once(nf, cap, chunk):
     assert all(1 <= e - s <= cap for s, e in b)
 
 
-def test_default_schedule_doubles_from_four():
-    assert [e - s for s, e in _host_batches(100, 100)] == [4, 8, 16, 32, 40]
-    assert [e - s for s, e in _host_batches(10, 10)] == [4, 6]
+def test_default_schedule_grows_from_six():
+    assert [e - s for s, e in _host_batches(100, 100)] == [6, 10, 15, 25, 44]
+    assert [e - s for s, e in _host_batches(10, 10)] == [6, 4]
+    assert [e - s for s, e in _host_batches(20, 20)] == [6, 14]
     assert [e - s for s, e in _host_batches(20, 20, [3, 7])] == [3, 7, 7, 3]
 
 
