@@ -91,7 +91,8 @@ typedef struct SaxsPlanInfo {
   int kz_count;
   int path;             /* pruned separable DFT; bits 0, 1, 2: z-, y-, x-axis DFT   */
                         /* on tcgen05; a clear bit: that pass in FP32 SIMT; bit 3:  */
-                        /* 128-column z tiles, bit 4: the atom-GEMM z pass          */
+                        /* 128-column z tiles, bit 4: the atom-GEMM z pass, bit 5:  */
+                        /* sparse element types on the direct SIMT z kernel         */
   size_t device_bytes;  /* device memory held by the plan                          */
   int frames_accumulated;
 } SaxsPlanInfo;

@@ -254,7 +254,9 @@ __device__ __forceinline__ void spread_taps_w(const AtomTabW &tab, int nv, int *
 }
 
 // Persistent, warp-specialized like k_spread_zdft_tc; grid = min(work items,
-// SMs), block kTwThreads.  Work items w = ((f*T + t)*stw + ty)*stiles[0] + tx.
+// SMs), block kTwThreads.  Work items w = ((f*tw_nd + i)*stw + ty)*stiles[0] + tx
+// over the dense element types t = tw_types[i] (all types unless the plan sends
+// the sparse ones to k_spread_zdft_sparse).
 //   producer warps: twG groups on alternate items, each with its own fixed-point
 //               tile and atom table: pre-pass and shared-memory taps into the
 //               tile, then the split, chunk by chunk of kTwChunk z: chunk q
@@ -540,24 +542,25 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
     }
   } else if (warp == kTwLoaderWarp) {
     ItemIter it;
-    it.init_dims(blockIdx.x, gridDim.x, a.stiles[0], a.stw, a.T);
+    it.init_dims(blockIdx.x, gridDim.x, a.stiles[0], a.stw, a.tw_nd);  // it.t: index into tw_types
     int j = 0;
     for (int w = blockIdx.x; w < items; w += gridDim.x, ++j, it.next()) {
       const int b = j & 1;
       const int x0 = it.tx * kTwX, y0 = it.ty * kTwY;
       int s0, cnt;
       bool valid;
-      home_ranges_load_w(a, home_x, home_y, it.f, it.t, it.tx, it.ty, s0, cnt, valid);
+      const int tt = a.tw_types[it.t];
+      home_ranges_load_w(a, home_x, home_y, it.f, tt, it.tx, it.ty, s0, cnt, valid);
       const int most = __reduce_max_sync(0xffffffffu, static_cast<unsigned>(valid ? cnt : 0));
       const int nall = __reduce_add_sync(0xffffffffu, static_cast<unsigned>(valid ? cnt : 0));
-      const float mean = tw_item_mean(a, it.f, it.t);
+      const float mean = tw_item_mean(a, it.f, tt);
       if (j >= 2) wait(&rec_empty[b], (j - 2) >> 1);
       if (__any_sync(0xffffffffu, abort_flag != 0)) break;
       TwSlot &sl = slot[b];
       home_ranges_publish_w(sl.ta, s0, cnt, valid);
       if (lane == 0) {
         sl.f = it.f;
-        sl.t = it.t;
+        sl.t = tt;
         sl.x0 = x0;
         sl.y0 = y0;
         sl.cw = min(kTwX, a.ext[0] - x0);
@@ -604,27 +607,28 @@ __global__ void __launch_bounds__(kTwThreads, 1) k_spread_zdft_tcw(DevArgs a, in
   } else {
     const int quarter = warp & 3;
     ItemIter it;
-    it.init_dims(blockIdx.x, gridDim.x, a.stiles[0], a.stw, a.T);
+    it.init_dims(blockIdx.x, gridDim.x, a.stiles[0], a.stw, a.tw_nd);  // it.t: index into tw_types
     const int64_t zplane = static_cast<int64_t>(a.ext[0]) * a.ext[1];
     int j = 0;
     for (int w = blockIdx.x; w < items; w += gridDim.x, ++j, it.next()) {
       const int d = j & 1;
+      const int tt = a.tw_types[it.t];
       // the item's fixed-point scale, as the loader computed it (before the wait,
       // so that its loads overlap it): Z = D * 2^17 / scale
       float unscale;
       {
         int s0, cnt;
         bool valid;
-        home_ranges_load_w(a, home_x, home_y, it.f, it.t, it.tx, it.ty, s0, cnt, valid);
+        home_ranges_load_w(a, home_x, home_y, it.f, tt, it.tx, it.ty, s0, cnt, valid);
         const int most = __reduce_max_sync(0xffffffffu, static_cast<unsigned>(valid ? cnt : 0));
         const int nall = __reduce_add_sync(0xffffffffu, static_cast<unsigned>(valid ? cnt : 0));
-        unscale = 131072.0f / tw_scale(nall, most, tw_item_mean(a, it.f, it.t), a.ntaps);
+        unscale = 131072.0f / tw_scale(nall, most, tw_item_mean(a, it.f, tt), a.ntaps);
       }
       wait(&acc_full[d], j >> 1);
       if (__any_sync(0xffffffffu, abort_flag != 0)) break;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const int x0 = it.tx * kTwX, y0 = it.ty * kTwY;
-      float2 *Zft = a.Z + (static_cast<int64_t>(it.f) * a.T + it.t) * a.nkz * zplane;
+      float2 *Zft = a.Z + (static_cast<int64_t>(it.f) * a.T + tt) * a.nkz * zplane;
       const int m = 32 * quarter + lane, lx = m >> 4, ly = m & 15;
       const bool valid = lx < min(kTwX, a.ext[0] - x0) && ly < min(kTwY, a.ext[1] - y0);
       // offsets within the (frame, type) block of nkz planes fit in 32 bits

@@ -98,6 +98,11 @@ struct DevArgs {
   double *hist, *nhist;
   double *iacc;
   int *status;
+  // element types of the wide z kernel (tw_types[0, tw_nd)) and of the direct
+  // kernel for types too sparse for a dense tile (tw_types[tw_nd, tw_nd + tw_ns));
+  // tw_ns = 0: every type in the wide kernel, in order
+  const int *tw_types;
+  int tw_nd, tw_ns;
 };
 
 // ---------------------------------------------------------------------------

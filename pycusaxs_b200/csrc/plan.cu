@@ -56,6 +56,7 @@ namespace {
 #include "kernel_spread_simt.cuh"
 #include "kernel_spread_tc.cuh"
 #include "kernel_spread_tcw.cuh"
+#include "kernel_spread_sparse.cuh"
 #include "kernel_spread_ag.cuh"
 #include "kernel_dft.cuh"
 #include "kernel_adjoint.cuh"
@@ -115,6 +116,7 @@ struct SaxsPlan {
   bool use_tc = false;   // z-axis DFT on the tensor cores
   bool use_tcw = false;  // ... with the wide-tile kernel (k_spread_zdft_tcw), else k_spread_zdft_tc
   size_t smem_spread_tc = 0, smem_spread_tcw = 0;
+  size_t smem_sparse = 0;  // k_spread_zdft_sparse's accumulator (0: no sparse types)
   int tc_ctas = 1, tcw_ctas = 1;
   bool tcn_ok = false, tcw_ok = false;  // z kernels the plan can run: 64- and 128-column tiles
   int twG_max = 1;                      // producer groups the wide kernel's shared memory allows
@@ -811,6 +813,34 @@ int create(const SaxsParams *prm, SaxsPlan **out, const long long *min_half = nu
   if (pl->tcn_ok) ALLOC(d_twztc, 2 * static_cast<size_t>(a.tcK) * a.tcN);
   if (pl->tcw_ok) ALLOC(d_twztcw, 2 * static_cast<size_t>(a.tcK) * a.twN);
   if (pl->tcw_ok) ALLOC(d_hyw, 2 * static_cast<size_t>(a.stw));
+  // PYCUSAXS_SPARSE_REACH=r: element types whose wide items would see fewer than r
+  // atoms on average (expected atoms reaching an 8 x 16 column tile) go to
+  // k_spread_zdft_sparse, whose cost grows with the atoms rather than with the
+  // tile.  Off by default: at r = 24 on the 100k-atom workload (its two 1% types,
+  // ~13 atoms per tile) the two paths measured the same (2.31 ms per 100 frames),
+  // each item being a short chain of dependent loads either way.  The order of
+  // tw_types is the wide kernel's types, then the sparse ones.
+  std::vector<int> tw_types;
+  {
+    const char *sr = std::getenv("PYCUSAXS_SPARSE_REACH");
+    const double lim = sr ? std::atof(sr) : 0.0;
+    const size_t sp_smem = 2 * 128 * static_cast<size_t>(a.nkzp) * sizeof(float);
+    const bool can = pl->tcw_ok && lim > 0.0 && sp_smem + static_smem(k_spread_zdft_sparse) <= optin_smem();
+    const double cols = static_cast<double>(kTwX + a.ntaps - 1) * (kTwY + a.ntaps - 1) /
+                        (static_cast<double>(a.n[0]) * a.n[1]);
+    std::vector<int> sparse;
+    for (int t = 0; t < a.T; ++t) {
+      const double reach = (type_start[t + 1] - type_start[t]) * cols;
+      if (can && reach < lim) sparse.push_back(t);
+      else tw_types.push_back(t);
+    }
+    a.tw_nd = static_cast<int>(tw_types.size());
+    a.tw_ns = static_cast<int>(sparse.size());
+    tw_types.insert(tw_types.end(), sparse.begin(), sparse.end());
+    pl->smem_sparse = a.tw_ns > 0 ? sp_smem : 0;
+  }
+  int *d_twt = nullptr;
+  ALLOC(d_twt, a.T);
   if (pl->use_ytc) ALLOC(d_twytc, static_cast<size_t>(pl->yshape.chunks) * 4 * pl->yshape.N * kDtcChunk);
   if (pl->use_xtc) ALLOC(d_twxtc, static_cast<size_t>(pl->xshape.chunks) * 4 * pl->xshape.N * kDtcChunk);
   ALLOC(d_hx, a.stiles[0]);
@@ -849,6 +879,7 @@ int create(const SaxsParams *prm, SaxsPlan **out, const long long *min_half = nu
   a.home_x = d_hx;
   a.home_y = d_hy;
   a.home_yw = d_hyw;
+  a.tw_types = d_twt;
   a.geom = d_geom;
   a.status = d_status;
 
@@ -955,6 +986,7 @@ int create(const SaxsParams *prm, SaxsPlan **out, const long long *min_half = nu
       (rc = up(d_twxtc, twxtc.data(), sizeof(float) * twxtc.size())) ||
       (rc = up(d_hy, hyt.data(), sizeof(int4) * hyt.size())) ||
       (rc = up(d_hyw, hywt.data(), pl->tcw_ok ? sizeof(int4) * hywt.size() : 0)) ||
+      (rc = up(d_twt, tw_types.data(), sizeof(int) * tw_types.size())) ||
       (rc = up(pl->d_geom0, g0, sizeof(g0)))) {
     destroy(pl);
     return rc;
@@ -979,6 +1011,7 @@ int create(const SaxsParams *prm, SaxsPlan **out, const long long *min_half = nu
   if (e == cudaSuccess) e = raise_smem_limit(k_hist<double>);
   if (e == cudaSuccess) e = raise_smem_limit(k_spread_zdft_tc);
   if (e == cudaSuccess) e = raise_smem_limit(k_spread_zdft_tcw);
+  if (e == cudaSuccess) e = raise_smem_limit(k_spread_zdft_sparse);
   if (e == cudaSuccess) e = raise_smem_limit(k_spread_zdft_ag);
   if (e == cudaSuccess) e = raise_smem_limit(k_dft_tc<false>);
   if (e == cudaSuccess) e = raise_smem_limit(k_dft_tc<true>);
@@ -1158,9 +1191,18 @@ int launch_spread(const SaxsPlan *pl, const DevArgs &a, int nframes, cudaStream_
                       dim3(kAgThreads), pl->smem_spread_ag, st, a, items);
   }
   if (pl->use_tc && pl->use_tcw) {
-    const int items = a.stiles[0] * a.stw * a.T * nframes;
-    return launch_pdl("k_spread_zdft_tcw", k_spread_zdft_tcw, dim3(std::max(1, std::min(items, pl->tcw_ctas))),
-                      dim3(kTwThreads), pl->smem_spread_tcw, st, a, items);
+    // the dense types' items on the wide kernel, the sparse types' on the direct one
+    const int items = a.stiles[0] * a.stw * a.tw_nd * nframes;
+    if (items > 0)
+      if (int rc = launch_pdl("k_spread_zdft_tcw", k_spread_zdft_tcw,
+                              dim3(std::max(1, std::min(items, pl->tcw_ctas))), dim3(kTwThreads),
+                              pl->smem_spread_tcw, st, a, items))
+        return rc;
+    const int sitems = a.stiles[0] * a.stw * a.tw_ns * nframes;
+    if (sitems > 0)
+      return launch_pdl("k_spread_zdft_sparse", k_spread_zdft_sparse, dim3(sitems), dim3(kSpThreads),
+                        pl->smem_sparse, st, a);
+    return SAXS_OK;
   }
   const int items = a.stiles[0] * a.stiles[1] * a.T * nframes;
   if (pl->use_tc) {
@@ -1878,7 +1920,8 @@ int saxs_plan_info(const SaxsPlan *pl, SaxsPlanInfo *info) {
   info->kbox[2] = a.nkz;
   info->kz_count = a.nkz;
   info->path = (pl->use_tc ? 1 : 0) | (pl->use_ytc ? 2 : 0) | (pl->use_xtc ? 4 : 0) |
-               (pl->use_tc && !pl->use_ag && pl->use_tcw ? 8 : 0) | (pl->use_tc && pl->use_ag ? 16 : 0);
+               (pl->use_tc && !pl->use_ag && pl->use_tcw ? 8 : 0) | (pl->use_tc && pl->use_ag ? 16 : 0) |
+               (pl->use_tc && !pl->use_ag && pl->use_tcw && pl->a.tw_ns > 0 ? 32 : 0);
   info->device_bytes = pl->bytes;
   info->frames_accumulated = pl->frames;
   return SAXS_OK;
