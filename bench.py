@@ -317,7 +317,8 @@ def bench_ours(args):
     frames_per_launch = frames_timed / max(dom_launches, 1)
     achieved = algo_bytes.get(dom, 0) * frames_per_launch / per_launch_s / 1e9
     # the kernel that ran for each stage: plan path bits 0/1/2 = z/y/x DFT on tcgen05,
-    # bit 3 = wide z tiles
+    # bit 3 = wide z tiles, bit 5 = sparse element types on k_spread_zdft_sparse (the
+    # same stage, after the wide kernel)
     path = info.path
     kernel_of = {"k_spread_zdft": ("k_spread_zdft_ag" if path & 16 else "k_spread_zdft_tcw" if path & 8
                                    else "k_spread_zdft_tc") if path & 1 else "k_spread_zdft",
@@ -331,6 +332,9 @@ def bench_ours(args):
                                 "), scaled by frames per launch",
                 "algorithmic_bytes": round(algo_bytes.get(dom, 0) * frames_per_launch),
                 "peak_source": "measured" if peaks else "fallback"}
+    if dom == "k_spread_zdft" and path & 32:
+        roofline["stage_note"] = ("the stage runs k_spread_zdft_tcw for the dense element types and "
+                                  "k_spread_zdft_sparse for the sparse ones; achieved is the stage's")
     if dom in algo_flops:
         useful = algo_flops[dom] * frames_per_launch / per_launch_s / 1e12
         if tensor and dom == "k_spread_zdft" and path & 16:

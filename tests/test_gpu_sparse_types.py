@@ -1,11 +1,11 @@
 """Sparse element types on the direct z kernel (k_spread_zdft_sparse) vs the FP64 oracle (GPU).
 
-With the wide-tile z kernel and PYCUSAXS_SPARSE_REACH=r at plan creation (off
-by default), an element type whose 8 x 16 column tiles would see fewer than r
-atoms on average is spread and z-transformed by the direct kernel instead
+With the wide-tile z kernel, an element type whose 8 x 16 column tiles would
+see fewer than r atoms on average (r = PYCUSAXS_SPARSE_REACH at plan creation,
+default 24) is spread and z-transformed by the direct kernel instead
 (``info.path`` bit 5); the other types stay on the wide kernel.  Both must give
 the oracle's bin counts and profiles within RTOL_PROFILE, and the same profile
-as the default plan, which keeps every type on the wide kernel.  Sending every type to the
+as a plan that keeps every type on the wide kernel (r = 0).  Sending every type to the
 direct kernel (a limit above every type's count) checks it on dense types too,
 where many atoms add into the same shared-memory accumulators.
 """
@@ -53,11 +53,11 @@ def test_rare_types_on_the_direct_kernel_match_the_oracle_and_the_wide_kernel(cu
     # are sparse, the others stay on the wide kernel
     s = cubic_system(20_000, 60.0, seed=71, jitter=0.3, nframes=3)
     frames = s.frames(0, 3)
-    h, n, path = _run(s, (64, 64, 64), frames, "24")
+    h, n, path = _run(s, (64, 64, 64), frames, None)
     assert path & WIDE_BIT and path & SPARSE_BIT, path
     ho, no, _ = oracle_hist(s, (64, 64, 64), frames)
     assert_profiles_close(h, n, ho, no)
-    hw, nw, pw = _run(s, (64, 64, 64), frames, None)
+    hw, nw, pw = _run(s, (64, 64, 64), frames, "0")
     assert pw & WIDE_BIT and not pw & SPARSE_BIT, pw
     assert_profiles_close(h, n, hw, nw, rtol=1e-5)
 
@@ -77,7 +77,7 @@ def test_triclinic_box_with_sparse_types(cuda):
     box = np.array([[60.0, 0.0, 0.0], [12.0, 58.0, 0.0], [6.0, 9.0, 55.0]], dtype=np.float32)
     boxes = np.stack([box, box])
     frames = s.frames(0, 2)
-    h, n, path = _run(s, (64, 60, 56), frames, "24", boxes=boxes)
+    h, n, path = _run(s, (64, 60, 56), frames, None, boxes=boxes)
     assert path & SPARSE_BIT, path
     ho, no, _ = oracle_hist(s, (64, 60, 56), frames, boxes=boxes)
     assert_profiles_close(h, n, ho, no)
