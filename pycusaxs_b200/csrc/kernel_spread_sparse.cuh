@@ -17,8 +17,10 @@
 // over the data rows, as the wide kernel subtracts it inside its tile).
 // Work items are those of the wide kernel (frame, type, 8 x 16 column tile) for
 // the types tw_types[tw_nd + i]: w = ((f*tw_ns + i)*stw + ty)*stiles[0] + tx.
-// One CTA per item.  Dynamic shared memory: acc[128 columns][2][nkzp] ints
-// (real parts, then imaginary parts, of a column).
+// One CTA per item, 128 threads, eight per SM (26 KB of shared memory and 63
+// registers each; six per SM with 35 KB were 0.15 ms per 100 frames slower on the
+// 100k-atom workload).  Dynamic shared memory: acc[128 columns][2][nkz] ints (real
+// parts, then imaginary parts, of a column).
 constexpr int kSpThreads = 128;
 // Fixed-point scale of an item's accumulator (integer shared-memory atomics
 // issue about three times faster than FP32 ones).  A term wx*wy*T, T = sum_r
@@ -34,19 +36,19 @@ __device__ __forceinline__ float sp_scale(int nvis, int ntaps) {
   return exp2f(fminf(e, cap));
 }
 
-// One reaching atom, staged by its lane for the warp's broadcast reads.
+// One reaching atom, staged by its thread for the warps' broadcast reads.
 struct SpAtom {
   float4 wx, wy, wz;
-  int4 zr;          // z tap rows, -1 for none
-  uint32_t lx, ly;  // in-tile x and y tap positions, one byte each, 0xFF outside
-  uint32_t pad[2];
+  uint32_t z01, z23;  // z tap rows, 16 bits each (0xFFFF for none)
+  uint32_t lx, ly;    // in-tile x and y tap positions, one byte each, 0xFF outside
 };
+constexpr int kSpRound = 64;  // atoms staged per round
 
-__global__ void __launch_bounds__(kSpThreads, 6) k_spread_zdft_sparse(DevArgs a) {
+__global__ void __launch_bounds__(kSpThreads, 8) k_spread_zdft_sparse(DevArgs a) {
   pdl_release();
   extern __shared__ int acc[];  // fixed point, sp_scale units
   __shared__ TileAtomsW ta;
-  __shared__ SpAtom sp_stage[kSpThreads];  // a round's reaching atoms
+  __shared__ SpAtom sp_stage[kSpRound];  // a round's reaching atoms
   __shared__ int sp_count[2];
   const int nkz = a.nkz, nkzp = a.nkzp;
   const int w = blockIdx.x;
@@ -54,7 +56,7 @@ __global__ void __launch_bounds__(kSpThreads, 6) k_spread_zdft_sparse(DevArgs a)
   const int rest = w / (a.stiles[0] * a.stw);
   const int f = rest / a.tw_ns;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  for (int i = tid; i < 128 * 2 * nkzp; i += kSpThreads) acc[i] = 0;
+  for (int i = tid; i < 128 * 2 * nkz; i += kSpThreads) acc[i] = 0;
   if (tid == 0) sp_count[0] = sp_count[1] = 0;
   // plan constants before the wait for the sort: the type, and per lane of warp 0
   // one home bin (lane 4*iy + ix: home_x[tx] entry ix, home_yw entry iy) or -1
@@ -86,7 +88,7 @@ __global__ void __launch_bounds__(kSpThreads, 6) k_spread_zdft_sparse(DevArgs a)
   const float inv_scale = 1.0f / scale;  // exact: scale is a power of two
   const float4 *rec = a.rec + static_cast<int64_t>(f) * a.M;
   const int P = a.order, nt = a.ntaps, ez = a.ext[2];
-  for (int base = 0, round = 0; base < nvis; base += kSpThreads, ++round) {
+  for (int base = 0, round = 0; base < nvis; base += kSpRound, ++round) {
     // thread i stages atom base + i if it reaches the tile: its weights, in-tile
     // x/y tap positions (bytes, 0xFF outside) and z tap rows (-1 for a missing
     // tap or a row outside the data), compacted to sp_stage[0, count); rounds
@@ -95,7 +97,7 @@ __global__ void __launch_bounds__(kSpThreads, 6) k_spread_zdft_sparse(DevArgs a)
     const int v = base + tid;
     float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
     uint32_t lxb = 0xFFFFFFFFu, lyb = 0xFFFFFFFFu;
-    if (v < nvis) {
+    if (tid < kSpRound && v < nvis) {
       int j = 0;
       while (v >= ta.cum[j + 1]) ++j;
       q = rec[ta.start[j] + (v - ta.cum[j])];
@@ -125,18 +127,19 @@ __global__ void __launch_bounds__(kSpThreads, 6) k_spread_zdft_sparse(DevArgs a)
       cubic_weights(q.x - static_cast<float>(m0), wx);
       cubic_weights(q.y - static_cast<float>(m1), wy);
       cubic_weights(q.z - static_cast<float>(m2), wz);
-      int zr[4];
+      uint32_t zr[4];
 #pragma unroll
       for (int o = 0; o < 4; ++o) {
         int z = m2 - P + o;
         if (z < 0) z += a.n[2];
-        zr[o] = o < nt && z < ez ? z : -1;
+        zr[o] = o < nt && z < ez ? static_cast<uint32_t>(z) : 0xFFFFu;
       }
       SpAtom &e = sp_stage[pos];
       e.wx = make_float4(wx[0], wx[1], wx[2], wx[3]);
       e.wy = make_float4(wy[0], wy[1], wy[2], wy[3]);
       e.wz = make_float4(wz[0], wz[1], wz[2], wz[3]);
-      e.zr = make_int4(zr[0], zr[1], zr[2], zr[3]);
+      e.z01 = zr[0] | (zr[1] << 16);
+      e.z23 = zr[2] | (zr[3] << 16);
       e.lx = lxb;
       e.ly = lyb;
     }
@@ -147,17 +150,17 @@ __global__ void __launch_bounds__(kSpThreads, 6) k_spread_zdft_sparse(DevArgs a)
     for (int k = warp; k < nr; k += kSpThreads / 32) {
       const SpAtom &b = sp_stage[k];
       const float4 bz = b.wz;
-      const int4 br = b.zr;
+      const uint32_t z01 = b.z01, z23 = b.z23;
       const uint32_t lxb = b.lx, lyb = b.ly;
       for (int k0 = 0; k0 < nkz; k0 += 32) {
         const int kz = k0 + lane;
         if (kz >= nkz) continue;
         float tr = 0.f, ti = 0.f;
         const float wzv[4] = {bz.x, bz.y, bz.z, bz.w};
-        const int zrv[4] = {br.x, br.y, br.z, br.w};
+        const uint32_t zrv[4] = {z01 & 0xFFFFu, z01 >> 16, z23 & 0xFFFFu, z23 >> 16};
 #pragma unroll
         for (int r = 0; r < 4; ++r)
-          if (zrv[r] >= 0) {
+          if (zrv[r] != 0xFFFFu) {
             const float2 c = a.twz[static_cast<size_t>(zrv[r]) * nkzp + kz];
             tr = fmaf(wzv[r], c.x, tr);
             ti = fmaf(wzv[r], c.y, ti);
@@ -173,9 +176,9 @@ __global__ void __launch_bounds__(kSpThreads, 6) k_spread_zdft_sparse(DevArgs a)
             const uint32_t cy = (lyb >> (8 * p)) & 0xFFu;
             if (cy == 0xFFu) continue;
             const float wxy = wxv[o] * wyv[p] * scale;
-            int *col = acc + (16 * cx + cy) * 2 * nkzp;
+            int *col = acc + (16 * cx + cy) * 2 * nkz;
             atomicAdd(col + kz, tap_fixed(wxy, tr));
-            atomicAdd(col + nkzp + kz, tap_fixed(wxy, ti));
+            atomicAdd(col + nkz + kz, tap_fixed(wxy, ti));
           }
         }
       }
@@ -189,9 +192,9 @@ __global__ void __launch_bounds__(kSpThreads, 6) k_spread_zdft_sparse(DevArgs a)
   for (int i = tid; i < nkz * 128; i += kSpThreads) {
     const int kz = i >> 7, c = i & 127, cx = c >> 4, cy = c & 15;
     if (cx < cw && cy < ch) {
-      const int *col = acc + c * 2 * nkzp;
+      const int *col = acc + c * 2 * nkz;
       Zft[kz * zplane + static_cast<int64_t>(x0 + cx) * a.ext[1] + (y0 + cy)] =
-          make_float2(fmaf(-mean, a.twz_sum[2 * kz], static_cast<float>(col[kz]) * inv_scale), fmaf(-mean, a.twz_sum[2 * kz + 1], static_cast<float>(col[nkzp + kz]) * inv_scale));
+          make_float2(fmaf(-mean, a.twz_sum[2 * kz], static_cast<float>(col[kz]) * inv_scale), fmaf(-mean, a.twz_sum[2 * kz + 1], static_cast<float>(col[nkz + kz]) * inv_scale));
     }
   }
 }

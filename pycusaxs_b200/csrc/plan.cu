@@ -816,16 +816,16 @@ int create(const SaxsParams *prm, SaxsPlan **out, const long long *min_half = nu
   // Element types whose wide items would see fewer than r atoms on average
   // (expected atoms reaching an 8 x 16 column tile; r = PYCUSAXS_SPARSE_REACH,
   // default 24, 0 turns it off) go to k_spread_zdft_sparse, whose cost grows with
-  // the atoms (~3.7k + ~100 cycles per atom and item) where the wide kernel's
-  // hardly does (~6k + ~14).  On the 100k-atom workload r = 24 sends its two 1%
-  // types (~13 atoms per tile): 2.30 -> 2.20 ms per 100 frames; adding the 5% type
-  // (~64) was slower (2.33 ms).  The order of tw_types is the wide kernel's types,
-  // then the sparse ones.
+  // the atoms where the wide kernel's hardly does (~6k cycles per item + ~14 per
+  // atom).  On the 100k-atom workload r = 24 sends its two 1% types (~13 atoms per
+  // tile): 2.30 -> 2.06 ms per 100 frames; adding the 5% type (~64) was slower
+  // (2.15 ms).  The order of tw_types is the wide kernel's types, then the sparse
+  // ones.
   std::vector<int> tw_types;
   {
     const char *sr = std::getenv("PYCUSAXS_SPARSE_REACH");
     const double lim = sr ? std::atof(sr) : 24.0;
-    const size_t sp_smem = 2 * 128 * static_cast<size_t>(a.nkzp) * sizeof(float);
+    const size_t sp_smem = 2 * 128 * static_cast<size_t>(a.nkz) * sizeof(int);
     const bool can = pl->tcw_ok && lim > 0.0 && sp_smem + static_smem(k_spread_zdft_sparse) <= optin_smem();
     const double cols = static_cast<double>(kTwX + a.ntaps - 1) * (kTwY + a.ntaps - 1) /
                         (static_cast<double>(a.n[0]) * a.n[1]);
